@@ -1,0 +1,321 @@
+"""Python host mirror of the AVIONIC B200 reconstruction core.
+
+The product is ``libavionic_core.so`` (CUDA, sm_100a) behind the C ABI in
+``include/avionic.h``.  This module binds that ABI with ctypes and mirrors the
+reference's interface for the reconstruction path (``CartesianOperator``,
+``TV``/``TGV2``/``ICTGV2`` solvers, ``utils`` stencils), taking device buffers
+as torch CUDA tensors.  There is no CPU fallback: importing the package fails
+loudly when the library is missing, and every call raises on a non-zero
+status.
+"""
+
+import ctypes
+import os
+
+from . import _abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libavionic_core.so")
+
+TV, TVTEMP, TGV2, TGV2_3D, ICTV, ICTGV2 = 0, 1, 2, 3, 4, 5
+METHODS = {"TV": TV, "TGV2": TGV2, "ICTGV2": ICTGV2}
+P_OF = {TV: 1, TGV2: 4, ICTGV2: 8}
+D_OF = {TV: 3, TGV2: 9, ICTGV2: 18}
+
+
+class AvionicError(RuntimeError):
+    pass
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            "libavionic_core.so is not built (expected at %s); run "
+            "`python -c 'import __graft_entry__ as g; g.build()'` or `make -C avionic_b200/csrc`" % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    _abi.declare(lib)
+    return lib
+
+
+lib = _load()
+
+
+def check(status):
+    if status != 0:
+        msg = lib.avx_last_error().decode(errors="replace")
+        raise AvionicError("avionic status %d: %s" % (status, msg))
+
+
+PDParams = _abi.PDParams
+RunStats = _abi.RunStats
+
+
+def default_params(method):
+    p = PDParams()
+    check(lib.avx_default_params(method, ctypes.byref(p)))
+    return p
+
+
+# ---------------------------------------------------------------------------
+# device-buffer helpers (torch is only the allocator here)
+# ---------------------------------------------------------------------------
+
+def _torch():
+    import torch
+    return torch
+
+
+def _cptr(t):
+    """ctypes void pointer of a contiguous CUDA tensor."""
+    if not t.is_cuda:
+        raise AvionicError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise AvionicError("expected a contiguous tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _ptr_array(tensors):
+    arr = (ctypes.c_void_p * len(tensors))()
+    for i, t in enumerate(tensors):
+        arr[i] = _cptr(t).value
+    return arr
+
+
+def to_device(a, dtype=None):
+    """numpy array -> contiguous CUDA tensor (complex64 / float32)."""
+    import numpy as np
+    torch = _torch()
+    a = np.asarray(a)
+    if dtype is None:
+        dtype = np.complex64 if np.iscomplexobj(a) else np.float32
+    return torch.from_numpy(np.ascontiguousarray(a.astype(dtype))).cuda()
+
+
+class CartesianOperator:
+    """``CartesianOperator`` (CUDA/src/cartesian_operator.cpp:3-168).
+
+    ``mask`` is None (the reference's empty mask) or a float32 CUDA tensor of
+    shape (T, H, W)."""
+
+    def __init__(self, width, height, coils, frames, mask=None, centered=True):
+        self.W, self.H, self.C, self.T = width, height, coils, frames
+        self.handle = ctypes.c_void_p()
+        mptr = _cptr(mask) if mask is not None else None
+        check(lib.avx_cartesian_operator_create(width, height, coils, frames, mptr, int(centered),
+                                                ctypes.byref(self.handle)))
+
+    def backward(self, x, b1, out=None):
+        """image (T,H,W) -> k-space (T,C,H,W) (BackwardOperation)."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty((self.T, self.C, self.H, self.W), dtype=torch.complex64, device=x.device)
+        check(lib.avx_operator_backward(self.handle, _cptr(x), _cptr(out), _cptr(b1)))
+        return out
+
+    def forward(self, k, b1, out=None):
+        """k-space (T,C,H,W) -> image (T,H,W) (ForwardOperation; masks k in place)."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty((self.T, self.H, self.W), dtype=torch.complex64, device=k.device)
+        check(lib.avx_operator_forward(self.handle, _cptr(k), _cptr(out), _cptr(b1)))
+        return out
+
+    def adapt_lambda(self, k, d):
+        lam = ctypes.c_float()
+        check(lib.avx_operator_adapt_lambda(self.handle, ctypes.c_float(k), ctypes.c_float(d), ctypes.byref(lam)))
+        return lam.value
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and h.value:
+            lib.avx_operator_destroy(h)
+            self.handle = ctypes.c_void_p()
+
+
+class Solver:
+    """``TV`` / ``TGV2`` / ``ICTGV2`` (PDRecon, CUDA/include/pd_recon.h:88-185)."""
+
+    def __init__(self, method, op, params=None):
+        if isinstance(method, str):
+            method = METHODS[method.upper()]
+        self.method, self.op = method, op
+        self.handle = ctypes.c_void_p()
+        pp = ctypes.byref(params) if params is not None else None
+        check(lib.avx_solver_create(method, op.W, op.H, op.C, op.T, pp, op.handle, ctypes.byref(self.handle)))
+
+    @property
+    def params(self):
+        p = PDParams()
+        check(lib.avx_solver_get_params(self.handle, ctypes.byref(p)))
+        return p
+
+    @params.setter
+    def params(self, p):
+        check(lib.avx_solver_set_params(self.handle, ctypes.byref(p)))
+
+    def set_debug(self, debug, debugstep=1):
+        check(lib.avx_solver_set_debug(self.handle, int(debug), int(debugstep)))
+
+    def set_verbose(self, verbose):
+        check(lib.avx_solver_set_verbose(self.handle, int(verbose)))
+
+    def set_stream(self, stream):
+        check(lib.avx_solver_set_stream(self.handle, ctypes.c_void_p(stream)))
+
+    def run(self, data, x, b1):
+        """IterativeReconstruction(data, x, b1); x is updated in place."""
+        check(lib.avx_solver_run(self.handle, _cptr(data), _cptr(x), _cptr(b1)))
+        return x
+
+    def adapt_step_size(self, diffs, b1):
+        check(lib.avx_solver_adapt_step_size(self.handle, _ptr_array(diffs), _cptr(b1)))
+        p = self.params
+        return p.sigma, p.tau
+
+    def compute_gap(self, xs, ys, z, data, b1):
+        gs, gap = ctypes.c_double(), ctypes.c_double()
+        check(lib.avx_solver_compute_gap(self.handle, _ptr_array(xs), _ptr_array(ys), _cptr(z), _cptr(data),
+                                         _cptr(b1), ctypes.byref(gs), ctypes.byref(gap)))
+        return gs.value, gap.value
+
+    def set_timing(self, on):
+        check(lib.avx_solver_set_timing(self.handle, int(on)))
+
+    def kernel_times(self):
+        """Mean ms of the (dual, k-space, primal) kernels of the last timed run."""
+        arr = (ctypes.c_float * 3)()
+        n = ctypes.c_uint()
+        check(lib.avx_solver_kernel_times(self.handle, arr, ctypes.byref(n)))
+        return list(arr), n.value
+
+    def stats(self):
+        s = RunStats()
+        check(lib.avx_solver_get_stats(self.handle, ctypes.byref(s)))
+        return s
+
+    def export(self, output_dir=""):
+        """ExportAdditionalResults: returns {name: complex numpy array}."""
+        import numpy as np
+        out = {}
+
+        def cb(d, name, vals, n, user):
+            arr = np.ctypeslib.as_array(ctypes.cast(vals, ctypes.POINTER(ctypes.c_float)), shape=(2 * n,))
+            out[name.decode()] = (arr[0::2] + 1j * arr[1::2]).astype(np.complex64).copy()
+
+        cbf = _abi.EXPORT_CB(cb)
+        check(lib.avx_solver_export(self.handle, output_dir.encode(), cbf, None))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h and h.value:
+            lib.avx_solver_destroy(h)
+            self.handle = ctypes.c_void_p()
+
+
+# ---------------------------------------------------------------------------
+# utils
+# ---------------------------------------------------------------------------
+
+def _empty_like_n(u, n):
+    torch = _torch()
+    return [torch.empty_like(u) for _ in range(n)]
+
+
+def gradient(u, dx=1.0, dy=1.0, dt=1.0):
+    T, H, W = u.shape
+    g = _empty_like_n(u, 3)
+    check(lib.avx_gradient(_cptr(u), _ptr_array(g), W, H, T, dx, dy, dt))
+    return g
+
+
+def divergence(y, dx=1.0, dy=1.0, dt=1.0):
+    torch = _torch()
+    T, H, W = y[0].shape
+    out = torch.empty_like(y[0])
+    check(lib.avx_divergence(_ptr_array(y), _cptr(out), W, H, T, dx, dy, dt))
+    return out
+
+
+def sym_gradient(v, dx=1.0, dy=1.0, dt=1.0):
+    T, H, W = v[0].shape
+    e = _empty_like_n(v[0], 6)
+    check(lib.avx_sym_gradient(_ptr_array(v), _ptr_array(e), W, H, T, dx, dy, dt))
+    return e
+
+
+def sym_divergence(w, dx=1.0, dy=1.0, dt=1.0):
+    T, H, W = w[0].shape
+    d = _empty_like_n(w[0], 3)
+    check(lib.avx_sym_divergence(_ptr_array(w), _ptr_array(d), W, H, T, dx, dy, dt))
+    return d
+
+
+def prox(y, scale):
+    n = y[0].numel()
+    fn = lib.avx_prox3 if len(y) == 3 else lib.avx_prox6
+    check(fn(_ptr_array(y), n, ctypes.c_float(scale)))
+    return y
+
+
+def norm(g):
+    torch = _torch()
+    out = torch.empty(g[0].shape, dtype=torch.float32, device=g[0].device)
+    fn = lib.avx_norm3 if len(g) == 3 else lib.avx_norm6
+    check(fn(_ptr_array(g), _cptr(out), g[0].numel()))
+    return out
+
+
+def tv_norm(u, dx=1.0, dy=1.0, dt=1.0):
+    T, H, W = u.shape
+    v = ctypes.c_double()
+    check(lib.avx_tv_norm(_cptr(u), W, H, T, dx, dy, dt, ctypes.byref(v)))
+    return v.value
+
+
+def tgv2_norm(x1, x2, alpha0, alpha1, dx=1.0, dy=1.0, dt=1.0):
+    T, H, W = x1.shape
+    v = ctypes.c_double()
+    check(lib.avx_tgv2_norm(_cptr(x1), _ptr_array(x2), alpha0, alpha1, W, H, T, dx, dy, dt, ctypes.byref(v)))
+    return v.value
+
+
+def ictgv2_norm(x1, x2, x3, x4, alpha0, alpha1, alpha, w1, w2):
+    T, H, W = x1.shape
+    v = ctypes.c_double()
+    a1 = (ctypes.c_float * 3)(*w1)
+    a2 = (ctypes.c_float * 3)(*w2)
+    check(lib.avx_ictgv2_norm(_cptr(x1), _ptr_array(x2), _cptr(x3), _ptr_array(x4), alpha0, alpha1, alpha, W, H, T,
+                              a1, a2, ctypes.byref(v)))
+    return v.value
+
+
+def ellipke(m):
+    return lib.avx_ellipke(ctypes.c_float(m))
+
+
+def time_space_weights(tsw):
+    ds, dt = ctypes.c_float(), ctypes.c_float()
+    check(lib.avx_time_space_weights(ctypes.c_float(tsw), ctypes.byref(ds), ctypes.byref(dt)))
+    return ds.value, dt.value
+
+
+def reconstruct_host(method, kdata, mask, b1, u0=None, params=None, debugstep=0):
+    """Host-buffer reconstruction (the CLI path).  numpy in, numpy out."""
+    import numpy as np
+    if isinstance(method, str):
+        method = METHODS[method.upper()]
+    T, C, H, W = kdata.shape
+    k = np.ascontiguousarray(kdata, dtype=np.complex64)
+    b = np.ascontiguousarray(b1, dtype=np.complex64)
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.float32)
+    u = None if u0 is None else np.ascontiguousarray(u0, dtype=np.complex64)
+    x = np.empty((T, H, W), dtype=np.complex64)
+    st = RunStats()
+    pp = ctypes.byref(params) if params is not None else None
+    check(lib.avx_reconstruct_host(
+        method, W, H, C, T, pp, int(debugstep), k.ctypes.data_as(ctypes.c_void_p),
+        None if m is None else m.ctypes.data_as(ctypes.c_void_p), b.ctypes.data_as(ctypes.c_void_p),
+        None if u is None else u.ctypes.data_as(ctypes.c_void_p), x.ctypes.data_as(ctypes.c_void_p),
+        ctypes.byref(st)))
+    return x, st

@@ -1,0 +1,77 @@
+"""ctypes declarations of include/avionic.h (kept in step with the header;
+tests/test_abi.py checks that every declared function is exported and bound)."""
+
+import ctypes as C
+
+VP = C.c_void_p
+U = C.c_uint
+I = C.c_int
+F = C.c_float
+D = C.c_double
+
+
+class PDParams(C.Structure):
+    _fields_ = [
+        ("maxIt", U), ("stopPDGap", F), ("sigma", F), ("tau", F), ("sigmaTauRatio", F),
+        ("timeSpaceWeight", F), ("lambda_", F), ("dx", F), ("dy", F), ("dt", F),
+        ("alpha0", F), ("alpha1", F), ("alpha", F), ("timeSpaceWeight2", F),
+        ("dx2", F), ("dy2", F), ("dt2", F), ("adaptLambda", I), ("adaptK", F), ("adaptD", F),
+    ]
+
+
+class RunStats(C.Structure):
+    _fields_ = [
+        ("iterations", U), ("sigma", F), ("tau", F), ("gap_count", U), ("last_gap", D),
+        ("stopped_by_gap", I), ("elapsed_ms", F), ("kernel_launches", U),
+    ]
+
+
+EXPORT_CB = C.CFUNCTYPE(None, C.c_char_p, C.c_char_p, VP, C.c_size_t, VP)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "avx_version": (C.c_char_p, []),
+    "avx_last_error": (C.c_char_p, []),
+    "avx_cartesian_operator_create": (I, [U, U, U, U, VP, I, C.POINTER(VP)]),
+    "avx_operator_backward": (I, [VP, VP, VP, VP]),
+    "avx_operator_forward": (I, [VP, VP, VP, VP]),
+    "avx_operator_adapt_lambda": (I, [VP, F, F, C.POINTER(F)]),
+    "avx_operator_destroy": (None, [VP]),
+    "avx_default_params": (I, [I, C.POINTER(PDParams)]),
+    "avx_solver_create": (I, [I, U, U, U, U, C.POINTER(PDParams), VP, C.POINTER(VP)]),
+    "avx_solver_get_params": (I, [VP, C.POINTER(PDParams)]),
+    "avx_solver_set_params": (I, [VP, C.POINTER(PDParams)]),
+    "avx_solver_set_verbose": (I, [VP, I]),
+    "avx_solver_set_debug": (I, [VP, I, I]),
+    "avx_solver_set_stream": (I, [VP, VP]),
+    "avx_solver_run": (I, [VP, VP, VP, VP]),
+    "avx_solver_adapt_step_size": (I, [VP, C.POINTER(VP), VP]),
+    "avx_solver_compute_gap": (I, [VP, C.POINTER(VP), C.POINTER(VP), VP, VP, VP, C.POINTER(D), C.POINTER(D)]),
+    "avx_solver_export": (I, [VP, C.c_char_p, EXPORT_CB, VP]),
+    "avx_solver_get_stats": (I, [VP, C.POINTER(RunStats)]),
+    "avx_solver_destroy": (None, [VP]),
+    "avx_solver_set_timing": (I, [VP, I]),
+    "avx_solver_kernel_times": (I, [VP, C.POINTER(F), C.POINTER(U)]),
+    "avx_gradient": (I, [VP, C.POINTER(VP), U, U, U, F, F, F]),
+    "avx_divergence": (I, [C.POINTER(VP), VP, U, U, U, F, F, F]),
+    "avx_sym_gradient": (I, [C.POINTER(VP), C.POINTER(VP), U, U, U, F, F, F]),
+    "avx_sym_divergence": (I, [C.POINTER(VP), C.POINTER(VP), U, U, U, F, F, F]),
+    "avx_prox3": (I, [C.POINTER(VP), U, F]),
+    "avx_prox6": (I, [C.POINTER(VP), U, F]),
+    "avx_norm3": (I, [C.POINTER(VP), VP, U]),
+    "avx_norm6": (I, [C.POINTER(VP), VP, U]),
+    "avx_tv_norm": (I, [VP, U, U, U, F, F, F, C.POINTER(D)]),
+    "avx_tgv2_norm": (I, [VP, C.POINTER(VP), F, F, U, U, U, F, F, F, C.POINTER(D)]),
+    "avx_ictgv2_norm": (I, [VP, C.POINTER(VP), VP, C.POINTER(VP), F, F, F, U, U, U, C.POINTER(F), C.POINTER(F),
+                            C.POINTER(D)]),
+    "avx_ellipke": (F, [F]),
+    "avx_time_space_weights": (I, [F, C.POINTER(F), C.POINTER(F)]),
+    "avx_reconstruct_host": (I, [I, U, U, U, U, C.POINTER(PDParams), I, VP, VP, VP, VP, VP, C.POINTER(RunStats)]),
+}
+
+
+def declare(lib):
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args

@@ -1,0 +1,1025 @@
+// Host side of the AVIONIC B200 reconstruction core: the Cartesian operator,
+// the TV / TGV2 / ICTGV2 solvers and the C ABI declared in include/avionic.h.
+//
+// A solver run follows TV/TGV2/ICTGV2::IterativeReconstruction of the
+// reference (CUDA/src/tv.cpp:99-200, tgv2.cpp:180-338, ictgv2.cpp:294-492):
+// time-space weights, zeroed duals, x and xbar from the initial image, then
+// maxIt iterations with the step rule at k < 10 or k % 50 == 0 and the gap on
+// the verbose/debug/stop cadence.  All scalars that steer the loop (sigma,
+// tau, the gap, the stop flag) stay on the device, so iterations are
+// enqueued without host synchronisation; each of the four iteration shapes
+// (plain, +step, +gap, +step+gap) is captured once as a CUDA graph and
+// replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/avionic.h"
+#include "pd_kernels.cuh"
+#include "utils_kernels.cuh"
+
+
+
+namespace {
+
+thread_local std::string g_err;
+
+avx_status fail(avx_status s, const std::string& msg) {
+  g_err = msg;
+  return s;
+}
+
+#define AVX_CK(call)                                                                         \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(e_ == cudaErrorMemoryAllocation ? AVX_E_NOMEM : AVX_E_CUDA,                \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+  } while (0)
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    if (count <= n && p) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+    if (e == cudaSuccess) n = count;
+    return e;
+  }
+};
+
+// Complete elliptic integral of the second kind by the AGM
+// (utils::Ellipke, utils.cpp:18-47; Abramowitz & Stegun 17.6).
+double ellipke_d(double m) {
+  double a0 = 1.0, b0 = std::sqrt(1.0 - m), s0 = m, mm = 1.0, a1 = 1.0;
+  int i1 = 0;
+  while (mm > 1e-7) {
+    a1 = (a0 + b0) / 2.0;
+    const double b1 = std::sqrt(a0 * b0);
+    const double c1 = (a0 - b0) / 2.0;
+    ++i1;
+    const double w1 = std::pow(2.0, i1) * c1 * c1;
+    mm = w1;
+    s0 += w1;
+    a0 = a1;
+    b0 = b1;
+  }
+  const double k = M_PI / (2.0 * a1);
+  return k * (1.0 - s0 / 2.0);
+}
+
+// PDRecon::ComputeTimeSpaceWeights (pd_recon.cpp:72-98)
+bool time_space_weights(double tsw, double* ds, double* dt) {
+  double r = 1.0 / tsw, w1, w2;
+  if (r > 0.0 && r <= 1.0) {
+    w2 = M_PI / (2.0 * ellipke_d(1.0 - r * r));
+    w1 = r * w2;
+  } else if (r > 1.0) {
+    r = 1.0 / r;
+    w1 = M_PI / (2.0 * ellipke_d(1.0 - r * r));
+    w2 = r * w1;
+  } else {
+    return false;
+  }
+  *ds = 1.0 / w1;
+  *dt = 1.0 / w2;
+  return true;
+}
+
+Wts make_wts(float dx, float dy, float dt) {
+  Wts w;
+  w.ix = (float)(1.0 / (double)dx);
+  w.iy = (float)(1.0 / (double)dy);
+  w.it = (float)(1.0 / (double)dt);
+  w.hx = (float)(1.0 / (2.0 * (double)dx));
+  w.hy = (float)(1.0 / (2.0 * (double)dy));
+  w.ht = (float)(1.0 / (2.0 * (double)dt));
+  return w;
+}
+
+int method_P(int m) { return m == AVX_METHOD_TV ? 1 : m == AVX_METHOD_TGV2 ? 4 : 8; }
+int method_D(int m) { return m == AVX_METHOD_TV ? 3 : m == AVX_METHOD_TGV2 ? 9 : 18; }
+bool method_ok(int m) { return m == AVX_METHOD_TV || m == AVX_METHOD_TGV2 || m == AVX_METHOD_ICTGV2; }
+
+__global__ void sumsq_kernel(const float2* v, long long n, double* partial) {
+  __shared__ double red[32];
+  double acc[1] = {0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    acc[0] += (double)cabs2(v[i]);
+  block_sum<1>(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+}
+
+// FP64 sum of squared magnitudes (synchronous; used at set-up only)
+avx_status sum_sq(const float2* v, long long n, cudaStream_t s, double* out) {
+  DevBuf<double> part;
+  AVX_CK(part.alloc(256));
+  sumsq_kernel<<<256, 256, 0, s>>>(v, n, part.p);
+  AVX_CK(cudaGetLastError());
+  std::vector<double> h(256);
+  AVX_CK(cudaMemcpyAsync(h.data(), part.p, 256 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  AVX_CK(cudaStreamSynchronize(s));
+  double acc = 0.0;
+  for (double x : h) acc += x;
+  *out = acc;
+  return AVX_OK;
+}
+
+bool g_configured = false;
+
+avx_status configure_once() {
+  if (g_configured) return AVX_OK;
+  AVX_CK(avx::configure_kernels());
+  g_configured = true;
+  return AVX_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Cartesian operator
+// ===========================================================================
+
+struct avx_operator {
+  int W = 0, H = 0, C = 0, T = 0, centered = 0;
+  bool has_mask = false, binary = true;
+  std::vector<int> rows, row_off;
+  int R = 0;
+  double mask_norm2 = 0.0;
+  DevBuf<int> d_rows, d_row_off;
+  DevBuf<float> d_mrow, d_mask;
+  DevBuf<float2> d_twx, d_twy, d_qp;
+
+  CartGeomDev geom() const {
+    CartGeomDev g;
+    g.W = W; g.H = H; g.C = C; g.T = T;
+    g.sx = centered ? W / 2 : 0;
+    g.sy = centered ? H / 2 : 0;
+    g.rows = d_rows.p;
+    g.row_off = d_row_off.p;
+    g.mrow = d_mrow.p;
+    g.twx = d_twx.p;
+    g.twy = d_twy.p;
+    g.inv_sqrt_w = (float)(1.0 / std::sqrt((double)W));
+    g.inv_sqrt_h = (float)(1.0 / std::sqrt((double)H));
+    return g;
+  }
+};
+
+static avx_status build_operator(avx_operator* op, const float* h_mask) {
+  const int W = op->W, H = op->H, T = op->T;
+  op->has_mask = h_mask != nullptr;
+  op->rows.clear();
+  op->row_off.assign(T + 1, 0);
+  std::vector<float> mrow;
+  op->binary = true;
+  op->mask_norm2 = 0.0;
+  for (int t = 0; t < T; ++t) {
+    op->row_off[t] = (int)op->rows.size();
+    for (int y = 0; y < H; ++y) {
+      bool keep = !op->has_mask;
+      if (op->has_mask) {
+        const float* m = h_mask + ((size_t)t * H + y) * W;
+        for (int x = 0; x < W; ++x) {
+          const float v = m[x];
+          op->mask_norm2 += (double)v * v;
+          if (v != 0.f) keep = true;
+          if (v != 0.f && v != 1.f) op->binary = false;
+        }
+      }
+      if (!keep) continue;
+      op->rows.push_back(y);
+      for (int x = 0; x < W; ++x) mrow.push_back(op->has_mask ? h_mask[((size_t)t * H + y) * W + x] : 1.f);
+    }
+  }
+  op->row_off[T] = (int)op->rows.size();
+  op->R = (int)op->rows.size();
+  std::vector<float2> twx(W), twy(H);
+  for (int j = 0; j < W; ++j) twx[j] = make_float2((float)std::cos(2.0 * M_PI * j / W), (float)std::sin(2.0 * M_PI * j / W));
+  for (int j = 0; j < H; ++j) twy[j] = make_float2((float)std::cos(2.0 * M_PI * j / H), (float)std::sin(2.0 * M_PI * j / H));
+  AVX_CK(op->d_rows.alloc(std::max(op->R, 1)));
+  AVX_CK(op->d_row_off.alloc(T + 1));
+  AVX_CK(op->d_mrow.alloc(std::max<size_t>(mrow.size(), 1)));
+  AVX_CK(op->d_twx.alloc(W));
+  AVX_CK(op->d_twy.alloc(H));
+  AVX_CK(op->d_qp.alloc((size_t)op->C * std::max(op->R, 1) * W));
+  if (op->R) AVX_CK(cudaMemcpy(op->d_rows.p, op->rows.data(), op->R * sizeof(int), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(op->d_row_off.p, op->row_off.data(), (T + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  if (!mrow.empty()) AVX_CK(cudaMemcpy(op->d_mrow.p, mrow.data(), mrow.size() * sizeof(float), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(op->d_twx.p, twx.data(), W * sizeof(float2), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(op->d_twy.p, twy.data(), H * sizeof(float2), cudaMemcpyHostToDevice));
+  if (op->has_mask) {
+    AVX_CK(op->d_mask.alloc((size_t)T * H * W));
+    AVX_CK(cudaMemcpy(op->d_mask.p, h_mask, (size_t)T * H * W * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  return AVX_OK;
+}
+
+static avx_status check_dims(unsigned W, unsigned H, unsigned C, unsigned T) {
+  if (!W || !H || !C || !T) return fail(AVX_E_ARG, "dimensions must be positive");
+  if (avx::kspace_smem_bytes((int)W, (int)H) > 227 * 1024)
+    return fail(AVX_E_UNSUPPORTED, "image size exceeds the k-space kernel's shared-memory tile");
+  if ((double)W * H * T * C > 4.0e9) return fail(AVX_E_ARG, "problem too large for 32-bit row offsets");
+  return AVX_OK;
+}
+
+// ===========================================================================
+// Solver
+// ===========================================================================
+
+struct avx_solver {
+  int method = 0;
+  int W = 0, H = 0, C = 0, T = 0;
+  avx_pd_params p{};
+  avx_operator* op = nullptr;
+  bool verbose = false, debug = false;
+  int debugstep = 1;
+  cudaStream_t user_stream = 0;
+  cudaStream_t stream = 0;
+  // device state
+  DevBuf<float2> prim, ext, dual, escr, z, d;
+  DevBuf<DevState> st;
+  DevBuf<double> pimg, pk, hist;
+  int cap = 0;
+  double d_off_energy = 0.0;
+  avx_run_stats stats{};
+  DevState last{};
+  // graphs of the four iteration shapes
+  cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
+  size_t graph_key = 0;
+  // timing mode
+  bool timing = false;
+  std::vector<cudaEvent_t> events;
+  float kmean[3] = {0.f, 0.f, 0.f};
+  unsigned kcount = 0;
+
+  ~avx_solver() {
+    drop_graphs();
+    for (auto e : events) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  void drop_graphs() {
+    for (auto& g : gexec)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  }
+  long long N() const { return (long long)W * H * T; }
+  float2* primc(int c) { return prim.p + (size_t)c * N(); }
+  float2* extc(int c) { return ext.p + (size_t)c * N(); }
+  float2* dualc(int c) { return dual.p + (size_t)c * N(); }
+  float2* escrc(int c) { return escr.p + (size_t)c * N(); }
+};
+
+static avx_status solver_alloc(avx_solver* s) {
+  const int P = method_P(s->method), D = method_D(s->method);
+  const size_t N = (size_t)s->N();
+  const size_t K = (size_t)s->C * std::max(s->op->R, 1) * s->W;
+  AVX_CK(s->prim.alloc(P * N));
+  AVX_CK(s->ext.alloc(P * N));
+  AVX_CK(s->dual.alloc(D * N));
+  AVX_CK(s->escr.alloc(P * N));
+  AVX_CK(s->z.alloc(K));
+  AVX_CK(s->d.alloc(K));
+  AVX_CK(s->st.alloc(1));
+  AVX_CK(s->pimg.alloc((size_t)8 * std::max(AVX_RED_BLOCKS, avx::gap_img_blocks(s->W, s->H, s->T))));
+  AVX_CK(s->pk.alloc((size_t)3 * s->C * s->T));
+  s->cap = (int)s->p.maxIt + 2;
+  AVX_CK(s->hist.alloc((size_t)3 * (s->cap + 1)));
+  if (!s->stream) AVX_CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  return AVX_OK;
+}
+
+static void solver_weights(avx_solver* s, Wts* w1, Wts* w2) {
+  *w1 = make_wts(s->p.dx, s->p.dy, s->p.dt);
+  *w2 = make_wts(s->p.dx2, s->p.dy2, s->p.dt2);
+}
+
+static PDArgs make_pdargs(avx_solver* s) {
+  PDArgs a;
+  memset(&a, 0, sizeof(a));
+  a.W = s->W; a.H = s->H; a.T = s->T; a.N = s->N();
+  const int P = method_P(s->method), D = method_D(s->method);
+  for (int c = 0; c < P; ++c) {
+    a.x[c] = s->primc(c);
+    a.xb[c] = s->extc(c);
+  }
+  for (int c = 0; c < D; ++c) a.y[c] = s->dualc(c);
+  solver_weights(s, &a.w1, &a.w2);
+  const double alpha = s->p.alpha;
+  const double m = std::min(alpha, 1.0 - alpha);
+  if (s->method == AVX_METHOD_TV) {
+    a.r1 = 1.0f;  // ProximalMap3(y, 1.0) (tv.cpp:157)
+  } else if (s->method == AVX_METHOD_TGV2) {
+    a.r1 = (float)(1.0 / (double)s->p.alpha1);  // tgv2.cpp:258-259
+    a.r2 = (float)(1.0 / (double)s->p.alpha0);
+  } else {
+    // ictgv2.cpp:366-381
+    a.r1 = (float)(1.0 / ((double)s->p.alpha1 * (alpha / m)));
+    a.r2 = (float)(1.0 / ((double)s->p.alpha0 * (alpha / m)));
+    a.r3 = (float)(1.0 / ((double)s->p.alpha1 * ((1.0 - alpha) / m)));
+    a.r4 = (float)(1.0 / ((double)s->p.alpha0 * ((1.0 - alpha) / m)));
+  }
+  a.alpha0 = s->p.alpha0;
+  a.alpha1 = s->p.alpha1;
+  a.alpha = s->p.alpha;
+  a.ic_a = (float)(alpha / m);
+  a.ic_b = (float)((1.0 - alpha) / m);
+  a.st = s->st.p;
+  return a;
+}
+
+static KArgs make_kargs(avx_solver* s, const float2* b1, const float2* in, const float2* in2) {
+  KArgs k;
+  memset(&k, 0, sizeof(k));
+  k.g = s->op->geom();
+  k.b1 = b1;
+  k.in = in;
+  k.in2 = in2;
+  k.z = s->z.p;
+  k.d = s->d.p;
+  k.qp = s->op->d_qp.p;
+  k.lam = s->p.lambda;
+  k.binary_mask = s->op->binary ? 1 : 0;
+  k.st = s->st.p;
+  k.partial = s->pk.p;
+  return k;
+}
+
+static avx::GapConst make_gapconst(avx_solver* s) {
+  avx::GapConst gc;
+  const double alpha = s->p.alpha, m = std::min(alpha, 1.0 - alpha);
+  gc.lam = s->p.lambda;
+  gc.d_off_energy = s->d_off_energy;
+  gc.N = (double)s->N();
+  gc.stop_gap = s->p.stopPDGap;
+  gc.alpha0 = s->p.alpha0;
+  gc.alpha1 = s->p.alpha1;
+  gc.ic_a = alpha / m;
+  gc.ic_b = (1.0 - alpha) / m;
+  return gc;
+}
+
+static bool step_due(unsigned k) { return k < 10 || k % 50 == 0; }
+static bool gap_due(const avx_solver* s, unsigned k) {
+  return (s->verbose && (k < 10 || k % 50 == 0)) || (s->debug && s->debugstep > 0 && k % (unsigned)s->debugstep == 0) ||
+         (s->p.stopPDGap > 0 && k % 20 == 0);
+}
+
+static unsigned shape_launches(int shape) { return 3u + ((shape & 1) ? 4u : 0u) + ((shape & 2) ? 3u : 0u); }
+
+static void enqueue_shape(avx_solver* s, int shape, const float2* b1, cudaEvent_t* ev = nullptr) {
+  const PDArgs a = make_pdargs(s);
+  const KArgs ks = make_kargs(s, b1, s->extc(0), nullptr);
+  if (ev) {
+    cudaEventRecord(ev[0], s->stream);
+    avx::launch_dual(s->method, a, s->stream);
+    cudaEventRecord(ev[1], s->stream);
+    avx::launch_kspace(ks, 0, s->stream);
+    cudaEventRecord(ev[2], s->stream);
+    avx::launch_primal(s->method, a, ks, s->stream);
+    cudaEventRecord(ev[3], s->stream);
+  } else {
+    avx::launch_iteration(s->method, a, ks, s->stream);
+  }
+  if (shape & 1) {
+    avx::Ptr8 e;
+    const int P = method_P(s->method);
+    for (int c = 0; c < 8; ++c) e.p[c] = c < P ? s->escrc(c) : nullptr;
+    const KArgs ke = make_kargs(s, b1, s->escrc(0), nullptr);
+    avx::launch_step(s->method, a, ke, e, P, s->pimg.p, s->pk.p, s->p.sigmaTauRatio, s->stream);
+  }
+  if (shape & 2) {
+    const KArgs kx = make_kargs(s, b1, s->primc(0), nullptr);
+    double* h = s->hist.p;
+    const bool ic = s->method == AVX_METHOD_ICTGV2;
+    avx::launch_gap(s->method, a, kx, s->pimg.p, s->pk.p, make_gapconst(s), h, ic ? h + (s->cap + 1) : nullptr,
+                    ic ? h + 2 * (s->cap + 1) : nullptr, s->cap, 0, s->stream);
+  }
+}
+
+static avx_status prepare_run(avx_solver* s, const float2* data, const float2* x0) {
+  const int P = method_P(s->method), D = method_D(s->method);
+  const size_t N = (size_t)s->N();
+  AVX_CK(cudaMemsetAsync(s->dual.p, 0, D * N * sizeof(float2), s->stream));
+  AVX_CK(cudaMemsetAsync(s->z.p, 0, s->z.n * sizeof(float2), s->stream));
+  AVX_CK(cudaMemsetAsync(s->d.p, 0, s->d.n * sizeof(float2), s->stream));
+  if (P > 1) {
+    AVX_CK(cudaMemsetAsync(s->primc(1), 0, (P - 1) * N * sizeof(float2), s->stream));
+    AVX_CK(cudaMemsetAsync(s->extc(1), 0, (P - 1) * N * sizeof(float2), s->stream));
+  }
+  if (x0) {
+    AVX_CK(cudaMemcpyAsync(s->primc(0), x0, N * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
+    AVX_CK(cudaMemcpyAsync(s->extc(0), x0, N * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
+  }
+  if (data && s->op->R) {
+    avx::launch_gather_rows(s->op->geom(), data, s->d.p, 0, s->stream);
+    AVX_CK(cudaGetLastError());
+    // energy of the data rows the operator never samples enters g1 as a constant
+    double all = 0.0, kept = 0.0;
+    avx_status r = sum_sq(data, (long long)s->C * N, s->stream, &all);
+    if (r != AVX_OK) return r;
+    r = sum_sq(s->d.p, (long long)s->d.n, s->stream, &kept);
+    if (r != AVX_OK) return r;
+    s->d_off_energy = std::max(0.0, all - kept);
+  } else {
+    s->d_off_energy = 0.0;
+  }
+  DevState h{};
+  h.sigma = s->p.sigma;
+  h.tau = s->p.tau;
+  AVX_CK(cudaMemcpyAsync(s->st.p, &h, sizeof(h), cudaMemcpyHostToDevice, s->stream));
+  AVX_CK(cudaStreamSynchronize(s->stream));
+  return AVX_OK;
+}
+
+static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const float2* b1) {
+  avx_status r = solver_alloc(s);
+  if (r != AVX_OK) return r;
+  // the reference overwrites dx, dy, dt (and dx2..dt2) from the weights (tv.cpp:103-104)
+  double ds, dt;
+  if (!time_space_weights(s->p.timeSpaceWeight, &ds, &dt)) return fail(AVX_E_ARG, "ComputeTimeSpaceWeights: invalid ratio");
+  s->p.dx = (float)ds; s->p.dy = (float)ds; s->p.dt = (float)dt;
+  if (s->method == AVX_METHOD_ICTGV2) {
+    if (!time_space_weights(s->p.timeSpaceWeight2, &ds, &dt)) return fail(AVX_E_ARG, "ComputeTimeSpaceWeights: invalid ratio");
+    s->p.dx2 = (float)ds; s->p.dy2 = (float)ds; s->p.dt2 = (float)dt;
+  }
+  // order the internal stream after the caller's stream
+  cudaEvent_t ev0, ev1, evin;
+  AVX_CK(cudaEventCreate(&ev0));
+  AVX_CK(cudaEventCreate(&ev1));
+  AVX_CK(cudaEventCreateWithFlags(&evin, cudaEventDisableTiming));
+  AVX_CK(cudaEventRecord(evin, s->user_stream));
+  AVX_CK(cudaStreamWaitEvent(s->stream, evin, 0));
+  r = prepare_run(s, data, x);
+  if (r != AVX_OK) return r;
+  if (s->method == AVX_METHOD_ICTGV2 && s->debug) {
+    const PDArgs a = make_pdargs(s);
+    const KArgs kx = make_kargs(s, b1, s->primc(0), nullptr);
+    double* h = s->hist.p;
+    avx::launch_gap(s->method, a, kx, s->pimg.p, s->pk.p, make_gapconst(s), h, h + (s->cap + 1), h + 2 * (s->cap + 1),
+                    s->cap, 1, s->stream);
+    AVX_CK(cudaGetLastError());
+  }
+  // graphs depend on every pointer and scalar baked into the launches
+  const size_t key = (size_t)b1 ^ ((size_t)s->prim.p << 1) ^ ((size_t)s->op << 2) ^
+                     std::hash<std::string>()(std::string((const char*)&s->p, sizeof(s->p))) ^ (size_t)s->d_off_energy;
+  if (key != s->graph_key) {
+    s->drop_graphs();
+    s->graph_key = key;
+  }
+  if (s->timing && s->events.size() < (size_t)4 * s->p.maxIt) {
+    const size_t need = (size_t)4 * s->p.maxIt;
+    while (s->events.size() < need) {
+      cudaEvent_t e;
+      AVX_CK(cudaEventCreate(&e));
+      s->events.push_back(e);
+    }
+  }
+  unsigned launches = 0;
+  AVX_CK(cudaEventRecord(ev0, s->stream));
+  unsigned k = 0;
+  for (; k < s->p.maxIt; ++k) {
+    const int shape = (step_due(k) ? 1 : 0) | (gap_due(s, k) ? 2 : 0);
+    launches += shape_launches(shape);
+    if (s->timing) {
+      enqueue_shape(s, shape, b1, &s->events[(size_t)4 * k]);
+      AVX_CK(cudaGetLastError());
+      continue;
+    }
+    if (!s->gexec[shape]) {
+      cudaGraph_t g;
+      AVX_CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+      enqueue_shape(s, shape, b1);
+      AVX_CK(cudaStreamEndCapture(s->stream, &g));
+      AVX_CK(cudaGraphInstantiate(&s->gexec[shape], g, 0));
+      cudaGraphDestroy(g);
+    }
+    AVX_CK(cudaGraphLaunch(s->gexec[shape], s->stream));
+    if (s->p.stopPDGap > 0 && (shape & 2) && (k % 100 == 0)) {
+      int stop = 0;
+      AVX_CK(cudaMemcpyAsync(&stop, &s->st.p->stop, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+      AVX_CK(cudaStreamSynchronize(s->stream));
+      if (stop) {
+        ++k;
+        break;
+      }
+    }
+  }
+  AVX_CK(cudaEventRecord(ev1, s->stream));
+  AVX_CK(cudaMemcpyAsync(x, s->primc(0), (size_t)s->N() * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
+  AVX_CK(cudaMemcpyAsync(&s->last, s->st.p, sizeof(DevState), cudaMemcpyDeviceToHost, s->stream));
+  AVX_CK(cudaStreamSynchronize(s->stream));
+  AVX_CK(cudaGetLastError());
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  s->kcount = 0;
+  s->kmean[0] = s->kmean[1] = s->kmean[2] = 0.f;
+  if (s->timing) {
+    double acc[3] = {0, 0, 0};
+    for (unsigned i = 0; i < k; ++i)
+      for (int j = 0; j < 3; ++j) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, s->events[(size_t)4 * i + j], s->events[(size_t)4 * i + j + 1]);
+        acc[j] += t;
+      }
+    s->kcount = k;
+    for (int j = 0; j < 3; ++j) s->kmean[j] = k ? (float)(acc[j] / k) : 0.f;
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  cudaEventDestroy(evin);
+  s->p.sigma = (float)s->last.sigma;
+  s->p.tau = (float)s->last.tau;
+  s->stats.iterations = (unsigned)s->last.iters;
+  s->stats.sigma = (float)s->last.sigma;
+  s->stats.tau = (float)s->last.tau;
+  s->stats.gap_count = (unsigned)s->last.ngap;
+  s->stats.last_gap = s->last.gap;
+  s->stats.stopped_by_gap = s->last.stop;
+  s->stats.elapsed_ms = ms;
+  s->stats.kernel_launches = launches;
+  if (s->last.err) return fail(AVX_E_NUMERIC, "device-side check failed");
+  return AVX_OK;
+}
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+extern "C" {
+
+const char* avx_version(void) { return "avionic-b200 0.1 (sm_100a)"; }
+const char* avx_last_error(void) { return g_err.c_str(); }
+
+avx_status avx_cartesian_operator_create(unsigned width, unsigned height, unsigned coils, unsigned frames,
+                                         const float* d_mask, int centered, avx_operator** out) {
+  if (!out) return fail(AVX_E_ARG, "null output handle");
+  avx_status r = check_dims(width, height, coils, frames);
+  if (r != AVX_OK) return r;
+  r = configure_once();
+  if (r != AVX_OK) return r;
+  std::vector<float> hm;
+  if (d_mask) {
+    hm.resize((size_t)width * height * frames);
+    AVX_CK(cudaMemcpy(hm.data(), d_mask, hm.size() * sizeof(float), cudaMemcpyDeviceToHost));
+  }
+  avx_operator* op = new avx_operator();
+  op->W = (int)width; op->H = (int)height; op->C = (int)coils; op->T = (int)frames;
+  op->centered = centered ? 1 : 0;
+  r = build_operator(op, d_mask ? hm.data() : nullptr);
+  if (r != AVX_OK) {
+    delete op;
+    return r;
+  }
+  *out = op;
+  return AVX_OK;
+}
+
+avx_status avx_operator_backward(avx_operator* op, const avx_cf32* d_x, avx_cf32* d_k, const avx_cf32* d_b1) {
+  if (!op || !d_x || !d_k || !d_b1) return fail(AVX_E_ARG, "null argument");
+  const size_t K = (size_t)op->W * op->H * op->C * op->T;
+  AVX_CK(cudaMemset(d_k, 0, K * sizeof(float2)));
+  KArgs k;
+  memset(&k, 0, sizeof(k));
+  k.g = op->geom();
+  k.b1 = reinterpret_cast<const float2*>(d_b1);
+  k.in = reinterpret_cast<const float2*>(d_x);
+  k.dense_out = reinterpret_cast<float2*>(d_k);
+  if (op->R) avx::launch_kspace(k, 3, 0);
+  AVX_CK(cudaGetLastError());
+  AVX_CK(cudaDeviceSynchronize());
+  return AVX_OK;
+}
+
+avx_status avx_operator_forward(avx_operator* op, avx_cf32* d_k, avx_cf32* d_x, const avx_cf32* d_b1) {
+  if (!op || !d_x || !d_k || !d_b1) return fail(AVX_E_ARG, "null argument");
+  KArgs k;
+  memset(&k, 0, sizeof(k));
+  k.g = op->geom();
+  k.b1 = reinterpret_cast<const float2*>(d_b1);
+  k.qp = op->d_qp.p;
+  avx::launch_dense_rowidft(k.g, reinterpret_cast<float2*>(d_k), op->d_qp.p, op->has_mask ? op->d_mask.p : nullptr, 0);
+  avx::launch_adjoint(k, reinterpret_cast<float2*>(d_x), 0);
+  AVX_CK(cudaGetLastError());
+  AVX_CK(cudaDeviceSynchronize());
+  return AVX_OK;
+}
+
+avx_status avx_operator_adapt_lambda(const avx_operator* op, float k, float d, float* lambda_out) {
+  if (!op || !lambda_out) return fail(AVX_E_ARG, "null argument");
+  double subfac = (double)op->W * op->H * op->T;
+  if (op->has_mask)
+    subfac /= op->mask_norm2;
+  else
+    subfac /= (double)op->W * op->H * op->T;
+  *lambda_out = (float)(subfac * k + d);
+  return AVX_OK;
+}
+
+void avx_operator_destroy(avx_operator* op) { delete op; }
+
+avx_status avx_default_params(int method, avx_pd_params* p) {
+  if (!p) return fail(AVX_E_ARG, "null params");
+  if (!method_ok(method)) return fail(AVX_E_UNSUPPORTED, "method not provided (TV, TGV2, ICTGV2 are)");
+  memset(p, 0, sizeof(*p));
+  p->maxIt = 500;
+  p->stopPDGap = 0.f;
+  p->sigma = (float)(1.0 / 3.0);
+  p->tau = (float)(1.0 / 3.0);
+  p->sigmaTauRatio = 1.f;
+  p->dx = p->dy = p->dt = 1.f;
+  p->dx2 = p->dy2 = p->dt2 = 1.f;
+  p->alpha0 = (float)std::sqrt(2.0);
+  p->alpha1 = 1.f;
+  p->adaptLambda = 1;
+  if (method == AVX_METHOD_ICTGV2) {
+    p->timeSpaceWeight = 6.5f;  // ictgv2.cpp:46-58
+    p->timeSpaceWeight2 = 2.5f;
+    p->alpha = 0.6423f;
+    p->adaptK = (float)(0.4 / (5.1191 * 0.35));
+    p->adaptD = (float)(10.0 / (5.1191 * 0.35));
+  } else {
+    p->timeSpaceWeight = 5.f;  // tv.cpp:48, tgv2.cpp:45
+    p->adaptK = (float)(0.4 * 0.2991);
+    p->adaptD = (float)(10.0 * 0.2991);
+  }
+  p->lambda = 1.f;
+  return AVX_OK;
+}
+
+avx_status avx_solver_create(int method, unsigned width, unsigned height, unsigned coils, unsigned frames,
+                             const avx_pd_params* params, avx_operator* op, avx_solver** out) {
+  if (!out || !op) return fail(AVX_E_ARG, "null argument");
+  if (!method_ok(method)) return fail(AVX_E_UNSUPPORTED, "method not provided (TV, TGV2, ICTGV2 are)");
+  if ((int)width != op->W || (int)height != op->H || (int)coils != op->C || (int)frames != op->T)
+    return fail(AVX_E_ARG, "solver dimensions differ from the operator's");
+  avx_solver* s = new avx_solver();
+  s->method = method;
+  s->W = (int)width; s->H = (int)height; s->C = (int)coils; s->T = (int)frames;
+  s->op = op;
+  if (params)
+    s->p = *params;
+  else
+    avx_default_params(method, &s->p);
+  if (s->p.adaptLambda) avx_operator_adapt_lambda(op, s->p.adaptK, s->p.adaptD, &s->p.lambda);
+  *out = s;
+  return AVX_OK;
+}
+
+avx_status avx_solver_get_params(const avx_solver* s, avx_pd_params* p) {
+  if (!s || !p) return fail(AVX_E_ARG, "null argument");
+  *p = s->p;
+  return AVX_OK;
+}
+avx_status avx_solver_set_params(avx_solver* s, const avx_pd_params* p) {
+  if (!s || !p) return fail(AVX_E_ARG, "null argument");
+  s->p = *p;
+  return AVX_OK;
+}
+avx_status avx_solver_set_verbose(avx_solver* s, int v) {
+  if (!s) return fail(AVX_E_ARG, "null solver");
+  s->verbose = v != 0;
+  return AVX_OK;
+}
+avx_status avx_solver_set_debug(avx_solver* s, int debug, int debugstep) {
+  if (!s) return fail(AVX_E_ARG, "null solver");
+  s->debug = debug != 0;
+  s->debugstep = debugstep;
+  return AVX_OK;
+}
+avx_status avx_solver_set_stream(avx_solver* s, void* st) {
+  if (!s) return fail(AVX_E_ARG, "null solver");
+  s->user_stream = (cudaStream_t)st;
+  return AVX_OK;
+}
+
+avx_status avx_solver_run(avx_solver* s, const avx_cf32* d_data, avx_cf32* d_x, const avx_cf32* d_b1) {
+  if (!s || !d_data || !d_x || !d_b1) return fail(AVX_E_ARG, "null argument");
+  return solver_run(s, reinterpret_cast<const float2*>(d_data), reinterpret_cast<float2*>(d_x),
+                    reinterpret_cast<const float2*>(d_b1));
+}
+
+avx_status avx_solver_adapt_step_size(avx_solver* s, const avx_cf32* const* d_diff, const avx_cf32* d_b1) {
+  if (!s || !d_diff || !d_b1) return fail(AVX_E_ARG, "null argument");
+  avx_status r = solver_alloc(s);
+  if (r != AVX_OK) return r;
+  const int P = method_P(s->method);
+  const size_t N = (size_t)s->N();
+  r = prepare_run(s, nullptr, nullptr);
+  if (r != AVX_OK) return r;
+  // e = xbar - x with xbar = 0 gives -diff; the norms are sign-invariant
+  for (int c = 0; c < P; ++c) {
+    AVX_CK(cudaMemcpyAsync(s->primc(c), d_diff[c], N * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
+    AVX_CK(cudaMemsetAsync(s->extc(c), 0, N * sizeof(float2), s->stream));
+  }
+  const PDArgs a = make_pdargs(s);
+  avx::Ptr8 e;
+  for (int c = 0; c < 8; ++c) e.p[c] = c < P ? s->escrc(c) : nullptr;
+  const KArgs ke = make_kargs(s, reinterpret_cast<const float2*>(d_b1), s->escrc(0), nullptr);
+  avx::launch_step(s->method, a, ke, e, P, s->pimg.p, s->pk.p, s->p.sigmaTauRatio, s->stream);
+  AVX_CK(cudaGetLastError());
+  DevState h;
+  AVX_CK(cudaMemcpyAsync(&h, s->st.p, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  AVX_CK(cudaStreamSynchronize(s->stream));
+  s->p.sigma = (float)h.sigma;
+  s->p.tau = (float)h.tau;
+  return AVX_OK;
+}
+
+avx_status avx_solver_compute_gap(avx_solver* s, const avx_cf32* const* d_x, const avx_cf32* const* d_y,
+                                  const avx_cf32* d_z, const avx_cf32* d_data, const avx_cf32* d_b1, double* gstar,
+                                  double* gap) {
+  if (!s || !d_x || !d_y || !d_z || !d_data || !d_b1) return fail(AVX_E_ARG, "null argument");
+  avx_status r = solver_alloc(s);
+  if (r != AVX_OK) return r;
+  const int P = method_P(s->method), D = method_D(s->method);
+  const size_t N = (size_t)s->N();
+  r = prepare_run(s, reinterpret_cast<const float2*>(d_data), nullptr);
+  if (r != AVX_OK) return r;
+  for (int c = 0; c < P; ++c)
+    AVX_CK(cudaMemcpyAsync(s->primc(c), d_x[c], N * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
+  for (int c = 0; c < D; ++c)
+    AVX_CK(cudaMemcpyAsync(s->dualc(c), d_y[c], N * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
+  if (s->op->R) avx::launch_gather_rows(s->op->geom(), reinterpret_cast<const float2*>(d_z), s->z.p, 0, s->stream);
+  PDArgs a = make_pdargs(s);
+  const KArgs kx = make_kargs(s, reinterpret_cast<const float2*>(d_b1), s->primc(0), nullptr);
+  avx::GapConst gc = make_gapconst(s);
+  gc.stop_gap = -1.0;
+  double* h = s->hist.p;
+  avx::launch_gap(s->method, a, kx, s->pimg.p, s->pk.p, gc, h, h + (s->cap + 1), h + 2 * (s->cap + 1), s->cap, 0,
+                  s->stream);
+  AVX_CK(cudaGetLastError());
+  const int nk = s->C * s->T, nimg = avx::gap_img_blocks(s->W, s->H, s->T);
+  std::vector<double> pk(3 * nk), pi(8 * nimg);
+  AVX_CK(cudaMemcpyAsync(pk.data(), s->pk.p, pk.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  AVX_CK(cudaMemcpyAsync(pi.data(), s->pimg.p, pi.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  AVX_CK(cudaStreamSynchronize(s->stream));
+  double v[11] = {0};
+  for (int i = 0; i < nk; ++i)
+    for (int j = 0; j < 3; ++j) v[j] += pk[j * nk + i];
+  for (int i = 0; i < nimg; ++i)
+    for (int j = 0; j < 8; ++j) v[3 + j] += pi[j * nimg + i];
+  const double lam = s->p.lambda;
+  const double g = 0.5 * lam * (v[0] + s->d_off_energy) + v[1] + v[2] / (2.0 * lam) + v[3] + v[4] + v[5] + v[6];
+  double reg;
+  if (s->method == AVX_METHOD_TV)
+    reg = v[7];
+  else if (s->method == AVX_METHOD_TGV2)
+    reg = s->p.alpha1 * v[7] + s->p.alpha0 * v[8];
+  else
+    reg = gc.ic_a * (s->p.alpha1 * v[7] + s->p.alpha0 * v[8]) + gc.ic_b * (s->p.alpha1 * v[9] + s->p.alpha0 * v[10]);
+  if (gstar) *gstar = g;
+  if (gap) *gap = std::fabs(g + reg);
+  return AVX_OK;
+}
+
+avx_status avx_solver_export(avx_solver* s, const char* dir, avx_export_cb cb, void* user) {
+  if (!s || !cb) return fail(AVX_E_ARG, "null argument");
+  auto send = [&](const char* name, const std::vector<double>& v) {
+    std::vector<avx_cf32> c(v.size());
+    for (size_t i = 0; i < v.size(); ++i) c[i] = avx_cf32{(float)v[i], 0.f};
+    cb(dir, name, c.data(), c.size(), user);
+  };
+  if (s->method == AVX_METHOD_ICTGV2 && s->prim.p) {
+    std::vector<avx_cf32> x3((size_t)s->N());
+    AVX_CK(cudaMemcpy(x3.data(), s->primc(4), x3.size() * sizeof(avx_cf32), cudaMemcpyDeviceToHost));
+    cb(dir, "x3_component", x3.data(), x3.size(), user);
+  }
+  if (s->debug && s->hist.p) {
+    const int ng = s->last.ngap;
+    std::vector<double> h((size_t)3 * (s->cap + 1));
+    AVX_CK(cudaMemcpy(h.data(), s->hist.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    send("PDGap", std::vector<double>(h.begin(), h.begin() + ng));
+    if (s->method == AVX_METHOD_ICTGV2) {
+      const size_t o = s->cap + 1;
+      send("ICTGVnorm", std::vector<double>(h.begin() + o, h.begin() + o + ng + 1));
+      send("DATAfidelity", std::vector<double>(h.begin() + 2 * o, h.begin() + 2 * o + ng + 1));
+    }
+  }
+  return AVX_OK;
+}
+
+avx_status avx_solver_get_stats(const avx_solver* s, avx_run_stats* st) {
+  if (!s || !st) return fail(AVX_E_ARG, "null argument");
+  *st = s->stats;
+  return AVX_OK;
+}
+
+avx_status avx_solver_set_timing(avx_solver* s, int on) {
+  if (!s) return fail(AVX_E_ARG, "null solver");
+  s->timing = on != 0;
+  return AVX_OK;
+}
+
+avx_status avx_solver_kernel_times(const avx_solver* s, float* mean_ms, unsigned* count) {
+  if (!s || !mean_ms) return fail(AVX_E_ARG, "null argument");
+  for (int j = 0; j < 3; ++j) mean_ms[j] = s->kmean[j];
+  if (count) *count = s->kcount;
+  return AVX_OK;
+}
+
+void avx_solver_destroy(avx_solver* s) { delete s; }
+
+// ---------------------------------------------------------------------------
+// utils
+// ---------------------------------------------------------------------------
+
+static avx::Ptr18 ptrs(const avx_cf32* const* p, int n) {
+  avx::Ptr18 r;
+  for (int i = 0; i < 18; ++i) r.p[i] = i < n ? const_cast<float2*>(reinterpret_cast<const float2*>(p[i])) : nullptr;
+  return r;
+}
+
+avx_status avx_gradient(const avx_cf32* d_u, avx_cf32* const* d_g, unsigned W, unsigned H, unsigned T, float dx,
+                        float dy, float dt) {
+  if (!d_u || !d_g) return fail(AVX_E_ARG, "null argument");
+  avx::launch_gradient(reinterpret_cast<const float2*>(d_u), ptrs(d_g, 3), W, H, T, make_wts(dx, dy, dt), 0);
+  AVX_CK(cudaDeviceSynchronize());
+  return AVX_OK;
+}
+avx_status avx_divergence(const avx_cf32* const* d_y, avx_cf32* d_div, unsigned W, unsigned H, unsigned T, float dx,
+                          float dy, float dt) {
+  if (!d_y || !d_div) return fail(AVX_E_ARG, "null argument");
+  avx::launch_divergence(ptrs(d_y, 3), reinterpret_cast<float2*>(d_div), W, H, T, make_wts(dx, dy, dt), 0);
+  AVX_CK(cudaDeviceSynchronize());
+  return AVX_OK;
+}
+avx_status avx_sym_gradient(const avx_cf32* const* d_v, avx_cf32* const* d_e, unsigned W, unsigned H, unsigned T,
+                            float dx, float dy, float dt) {
+  if (!d_v || !d_e) return fail(AVX_E_ARG, "null argument");
+  avx::launch_symgrad(ptrs(d_v, 3), ptrs(d_e, 6), W, H, T, make_wts(dx, dy, dt), 0);
+  AVX_CK(cudaDeviceSynchronize());
+  return AVX_OK;
+}
+avx_status avx_sym_divergence(const avx_cf32* const* d_w, avx_cf32* const* d_d, unsigned W, unsigned H, unsigned T,
+                              float dx, float dy, float dt) {
+  if (!d_w || !d_d) return fail(AVX_E_ARG, "null argument");
+  avx::launch_symdiv(ptrs(d_w, 6), ptrs(d_d, 3), W, H, T, make_wts(dx, dy, dt), 0);
+  AVX_CK(cudaDeviceSynchronize());
+  return AVX_OK;
+}
+avx_status avx_prox3(avx_cf32* const* d_y, unsigned N, float scale) {
+  if (!d_y) return fail(AVX_E_ARG, "null argument");
+  avx::launch_prox(ptrs(d_y, 3), 3, N, scale, 0);
+  AVX_CK(cudaDeviceSynchronize());
+  return AVX_OK;
+}
+avx_status avx_prox6(avx_cf32* const* d_y, unsigned N, float scale) {
+  if (!d_y) return fail(AVX_E_ARG, "null argument");
+  avx::launch_prox(ptrs(d_y, 6), 6, N, scale, 0);
+  AVX_CK(cudaDeviceSynchronize());
+  return AVX_OK;
+}
+avx_status avx_norm3(const avx_cf32* const* d_g, float* d_norm, unsigned N) {
+  if (!d_g || !d_norm) return fail(AVX_E_ARG, "null argument");
+  avx::launch_norm(ptrs(d_g, 3), 3, d_norm, N, 0);
+  AVX_CK(cudaDeviceSynchronize());
+  return AVX_OK;
+}
+avx_status avx_norm6(const avx_cf32* const* d_g, float* d_norm, unsigned N) {
+  if (!d_g || !d_norm) return fail(AVX_E_ARG, "null argument");
+  avx::launch_norm(ptrs(d_g, 6), 6, d_norm, N, 0);
+  AVX_CK(cudaDeviceSynchronize());
+  return AVX_OK;
+}
+
+static avx_status regnorm(const float2* u, const float2* u2, const avx_cf32* const* v, unsigned W, unsigned H,
+                          unsigned T, Wts w, double* s1, double* s2) {
+  const int nb = 256;
+  DevBuf<double> part;
+  AVX_CK(part.alloc(2 * nb));
+  avx::launch_regnorm(u, u2, v ? ptrs(v, 3) : avx::Ptr18{}, v ? 1 : 0, W, H, T, w, part.p, nb, 0);
+  std::vector<double> h(2 * nb);
+  AVX_CK(cudaMemcpy(h.data(), part.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  double a = 0, b = 0;
+  for (int i = 0; i < nb; ++i) {
+    a += h[i];
+    b += h[nb + i];
+  }
+  *s1 = a;
+  *s2 = b;
+  return AVX_OK;
+}
+
+avx_status avx_tv_norm(const avx_cf32* d_u, unsigned W, unsigned H, unsigned T, float dx, float dy, float dt,
+                       double* out) {
+  if (!d_u || !out) return fail(AVX_E_ARG, "null argument");
+  double a, b;
+  avx_status r = regnorm(reinterpret_cast<const float2*>(d_u), nullptr, nullptr, W, H, T, make_wts(dx, dy, dt), &a, &b);
+  *out = a;
+  return r;
+}
+avx_status avx_tgv2_norm(const avx_cf32* d_x1, const avx_cf32* const* d_x2, float alpha0, float alpha1, unsigned W,
+                         unsigned H, unsigned T, float dx, float dy, float dt, double* out) {
+  if (!d_x1 || !d_x2 || !out) return fail(AVX_E_ARG, "null argument");
+  double a, b;
+  avx_status r = regnorm(reinterpret_cast<const float2*>(d_x1), nullptr, d_x2, W, H, T, make_wts(dx, dy, dt), &a, &b);
+  *out = alpha1 * a + alpha0 * b;
+  return r;
+}
+avx_status avx_ictgv2_norm(const avx_cf32* d_x1, const avx_cf32* const* d_x2, const avx_cf32* d_x3,
+                           const avx_cf32* const* d_x4, float alpha0, float alpha1, float alpha, unsigned W, unsigned H,
+                           unsigned T, const float* w1, const float* w2, double* out) {
+  if (!d_x1 || !d_x2 || !d_x3 || !d_x4 || !w1 || !w2 || !out) return fail(AVX_E_ARG, "null argument");
+  double a1, b1, a2, b2;
+  avx_status r = regnorm(reinterpret_cast<const float2*>(d_x1), reinterpret_cast<const float2*>(d_x3), d_x2, W, H, T,
+                         make_wts(w1[0], w1[1], w1[2]), &a1, &b1);
+  if (r != AVX_OK) return r;
+  r = regnorm(reinterpret_cast<const float2*>(d_x3), nullptr, d_x4, W, H, T, make_wts(w2[0], w2[1], w2[2]), &a2, &b2);
+  const double m = std::min((double)alpha, 1.0 - alpha);
+  *out = (alpha / m) * (alpha1 * a1 + alpha0 * b1) + ((1.0 - alpha) / m) * (alpha1 * a2 + alpha0 * b2);
+  return r;
+}
+
+float avx_ellipke(float m) {
+  if (!(m >= 0.f && m <= 1.f)) {
+    g_err = "Ellipke: only values in the range of [0,1] are allowed";
+    return NAN;
+  }
+  return (float)ellipke_d(m);
+}
+
+avx_status avx_time_space_weights(float tsw, float* ds, float* dt) {
+  if (!ds || !dt) return fail(AVX_E_ARG, "null argument");
+  double a, b;
+  if (!time_space_weights(tsw, &a, &b)) return fail(AVX_E_ARG, "ComputeTimeSpaceWeights: invalid ratio");
+  *ds = (float)a;
+  *dt = (float)b;
+  return AVX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// host-buffer path
+// ---------------------------------------------------------------------------
+
+avx_status avx_reconstruct_host(int method, unsigned W, unsigned H, unsigned C, unsigned T, const avx_pd_params* params,
+                                int debugstep, const avx_cf32* h_kdata, const float* h_mask, const avx_cf32* h_b1,
+                                const avx_cf32* h_u0, avx_cf32* h_x, avx_run_stats* stats) {
+  if (!h_kdata || !h_b1 || !h_x) return fail(AVX_E_ARG, "null argument");
+  avx_status r = check_dims(W, H, C, T);
+  if (r != AVX_OK) return r;
+  const size_t N = (size_t)W * H * T, K = N * C, HW = (size_t)W * H;
+  DevBuf<float2> dk, db1, dx;
+  DevBuf<float> dm;
+  AVX_CK(dk.alloc(K));
+  AVX_CK(db1.alloc(HW * C));
+  AVX_CK(dx.alloc(N));
+  AVX_CK(cudaMemcpy(dk.p, h_kdata, K * sizeof(float2), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(db1.p, h_b1, HW * C * sizeof(float2), cudaMemcpyHostToDevice));
+  if (h_mask) {
+    AVX_CK(dm.alloc(N));
+    AVX_CK(cudaMemcpy(dm.p, h_mask, N * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  for (unsigned t = 0; t < T; ++t) {
+    if (h_u0)
+      AVX_CK(cudaMemcpy(dx.p + t * HW, h_u0, HW * sizeof(float2), cudaMemcpyHostToDevice));
+    else
+      AVX_CK(cudaMemset(dx.p + t * HW, 0, HW * sizeof(float2)));
+  }
+  avx_operator* op = nullptr;
+  r = avx_cartesian_operator_create(W, H, C, T, h_mask ? dm.p : nullptr, 0, &op);
+  if (r != AVX_OK) return r;
+  // zero the data outside the mask (main.cpp:507-519): the compact rows only
+  // read sampled rows, and the rest enter the gap's data term as zeros.
+  if (h_mask) {
+    avx::launch_dense_rowidft(op->geom(), dk.p, op->d_qp.p, dm.p, 0);  // masks dk in place
+    AVX_CK(cudaDeviceSynchronize());
+  }
+  avx_solver* s = nullptr;
+  r = avx_solver_create(method, W, H, C, T, params, op, &s);
+  if (r != AVX_OK) {
+    avx_operator_destroy(op);
+    return r;
+  }
+  avx_solver_set_debug(s, debugstep > 0, debugstep);
+  r = avx_solver_run(s, reinterpret_cast<avx_cf32*>(dk.p), reinterpret_cast<avx_cf32*>(dx.p),
+                     reinterpret_cast<avx_cf32*>(db1.p));
+  if (r == AVX_OK) {
+    cudaError_t e = cudaMemcpy(h_x, dx.p, N * sizeof(float2), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) r = fail(AVX_E_CUDA, cudaGetErrorString(e));
+    if (stats) *stats = s->stats;
+  }
+  avx_solver_destroy(s);
+  avx_operator_destroy(op);
+  return r;
+}
+
+}  // extern "C"

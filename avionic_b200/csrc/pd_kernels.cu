@@ -1,0 +1,797 @@
+// Primal-dual kernels of the AVIONIC B200 reconstruction core.
+//
+// One PD iteration of TV / TGV2 / ICTGV2 (reference loops: CUDA/src/tv.cpp:137-198,
+// tgv2.cpp:234-335, ictgv2.cpp:334-490) runs as three kernels:
+//   dual_kernel    y <- prox(y + sigma * K_reg xbar)        (pointwise + stencils)
+//   kspace_kernel  z <- prox(z + sigma (K xbar - d)); Q' = row-IDFT(mask z)
+//                  one CTA per (coil, frame), compact sampled rows only
+//   primal_kernel  K^H z (column IDFT of Q', coil combine) fused with the
+//                  divergence stencils, the primal update and the extragradient
+// The step-size rule (pd_recon.cpp:40-61) and the primal-dual gap
+// (tv.cpp:202-235, tgv2.cpp:130-176, ictgv2.cpp:163-249) are FP64 block
+// reductions plus a one-block finaliser that updates device-resident scalars.
+#include "pd_kernels.cuh"
+#include "stencil.cuh"
+
+namespace avx {
+
+// ---------------------------------------------------------------------------
+// dual update
+// ---------------------------------------------------------------------------
+
+template <int M>
+__global__ void __launch_bounds__(256) dual_kernel(PDArgs a) {
+  if (a.st->stop) return;
+  // iteration counter (loopCnt of the reference) kept on the device so that
+  // every iteration launches identical work and can be replayed from a graph
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) a.st->iters += 1;
+  const int HW = a.W * a.H;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= HW) return;
+  const int t = blockIdx.y;
+  const PixCoord p = make_pix(j % a.W, j / a.W, t, a.W, a.H, a.T);
+  const float sig = (float)a.st->sigma;
+
+  if (M == AVX_M_TV) {
+    float2 g[3], y[3];
+    grad3(a.xb[0], p, a.w1, g);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float2 v = a.y[k][p.i];
+      y[k] = make_float2(v.x + sig * g[k].x, v.y + sig * g[k].y);
+    }
+    prox_div<3>(y, nrm3(y), a.r1);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) a.y[k][p.i] = y[k];
+  } else {
+    // branch 1: y1 += sigma (grad u - v), y2 += sigma E v
+    // TGV2: u = xbar1, v = xbar2.  ICTGV2: u = xbar1 - xbar3, v = xbar2.
+    {
+      float2 g[3], y1[3], e[6], y2[6];
+      if (M == AVX_M_TGV2)
+        grad3(a.xb[0], p, a.w1, g);
+      else
+        grad3_diff(a.xb[0], a.xb[4], p, a.w1, g);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        float2 v = a.y[k][p.i];
+        float2 q = ldc(a.xb[1 + k], p.i);
+        float2 d = csub(g[k], q);
+        y1[k] = make_float2(v.x + sig * d.x, v.y + sig * d.y);
+      }
+      prox_div<3>(y1, nrm3(y1), a.r1);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) a.y[k][p.i] = y1[k];
+      symgrad(a.xb[1], a.xb[2], a.xb[3], p, a.w1, e);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        float2 v = a.y[3 + k][p.i];
+        y2[k] = make_float2(v.x + sig * e[k].x, v.y + sig * e[k].y);
+      }
+      prox_div<6>(y2, nrm6(y2), a.r2);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) a.y[3 + k][p.i] = y2[k];
+    }
+    if (M == AVX_M_ICTGV2) {
+      // branch 2: y3 += sigma (grad2 xbar3 - xbar4), y4 += sigma E2 xbar4
+      float2 g[3], y3[3], e[6], y4[6];
+      grad3(a.xb[4], p, a.w2, g);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        float2 v = a.y[9 + k][p.i];
+        float2 d = csub(g[k], ldc(a.xb[5 + k], p.i));
+        y3[k] = make_float2(v.x + sig * d.x, v.y + sig * d.y);
+      }
+      prox_div<3>(y3, nrm3(y3), a.r3);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) a.y[9 + k][p.i] = y3[k];
+      symgrad(a.xb[5], a.xb[6], a.xb[7], p, a.w2, e);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        float2 v = a.y[12 + k][p.i];
+        y4[k] = make_float2(v.x + sig * e[k].x, v.y + sig * e[k].y);
+      }
+      prox_div<6>(y4, nrm6(y4), a.r4);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) a.y[12 + k][p.i] = y4[k];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k-space kernel: one CTA per (coil, frame), sampled rows in chunks of KC.
+//
+// For a chunk of compact rows k (ky_k):
+//   P[k][x]  = 1/sqrt(H) sum_y  e^{+2 pi i (ky_k-sy)(y-sy)/H} b1[c,y,x] u[t,y,x]
+//   X[k][kx] = 1/sqrt(W) sum_x  e^{+2 pi i (kx-sx)(x-sx)/W} P[k][x]
+// which is the unitary image -> k-space transform of the reference restricted
+// to the kept rows (see oracle/cartesian.py for the sign).  Then, by mode:
+//   0  PD step:   z <- mask * (z + sigma mask X - sigma d) / (1 + sigma/lambda)
+//                 (tgv2.cpp:254-264 followed by the in-place masking of
+//                 ForwardOperation, cartesian_operator.cpp:83-88), and
+//                 Q'[k][x] = 1/sqrt(W) sum_kx e^{-2 pi i ..} z[k][kx]
+//   1  step rule: sum |mask X|^2 of u = in - in2
+//   2  gap:       sum |mask X - d|^2, Re<d,z>, |z|^2, then z <- mask z and Q'
+//   3  apply:     dense_out[t,c,ky,kx] = mask X
+// ---------------------------------------------------------------------------
+
+template <int KC>
+__global__ void __launch_bounds__(256) kspace_kernel(KArgs a, int mode) {
+  if (a.st && a.st->stop && mode != 3) return;
+  constexpr int KCP = KC + 2;  // padded row stride (keeps 16-byte alignment)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const CartGeomDev& g = a.g;
+  const int W = g.W, H = g.H, C = g.C;
+  const int c = blockIdx.x % C;
+  const int t = blockIdx.x / C;
+  const int r0 = g.row_off[t], r1 = g.row_off[t + 1];
+  const int S = r1 - r0;
+  const long long HW = (long long)W * H;
+  const long long zb = kbase(g, t, c, r0, r1);
+
+  float2* coefY = reinterpret_cast<float2*>(smem_raw);   // [H][KCP]
+  float2* P = coefY + (size_t)H * KCP;                     // [W][KCP]
+  float2* X = P + (size_t)W * KCP;                         // [W][KCP]
+  float2* twx = X + (size_t)W * KCP;                       // [W]
+  double* red = reinterpret_cast<double*>(twx + W);        // [32*3]
+
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int j = tid; j < W; j += nt) twx[j] = g.twx[j];
+
+  const float sig = a.st ? (float)a.st->sigma : 0.f;
+  const float zscale = (mode == 0) ? (float)(1.0 / (1.0 + a.st->sigma / (double)a.lam)) : 1.f;
+  double acc_r[3] = {0.0, 0.0, 0.0};
+
+  const float2* __restrict__ b1 = a.b1 + (long long)c * HW;
+  const float2* __restrict__ u = a.in + (long long)t * HW;
+  const float2* __restrict__ u2 = a.in2 ? a.in2 + (long long)t * HW : nullptr;
+
+  for (int k0 = 0; k0 < S; k0 += KC) {
+    const int kc = min(KC, S - k0);
+    __syncthreads();
+    // column coefficients of this chunk
+    for (int e = tid; e < H * KC; e += nt) {
+      const int y = e / KC, kk = e % KC;
+      float2 v = czero();
+      if (kk < kc) {
+        const int ky = g.rows[r0 + k0 + kk];
+        const int a1 = (ky - g.sy + H) % H, a2 = (y - g.sy + H) % H;
+        v = cscale(g.twy[(a1 * a2) % H], g.inv_sqrt_h);
+      }
+      coefY[y * KCP + kk] = v;
+    }
+    __syncthreads();
+    // partial DFT along y: thread per x
+    for (int x = tid; x < W; x += nt) {
+      float2 acc[KC];
+#pragma unroll
+      for (int kk = 0; kk < KC; ++kk) acc[kk] = czero();
+      for (int y = 0; y < H; ++y) {
+        float2 v = u[(long long)y * W + x];
+        if (u2) v = csub(v, u2[(long long)y * W + x]);
+        v = cmul(__ldg(b1 + (long long)y * W + x), v);
+        const float4* cy = reinterpret_cast<const float4*>(coefY + y * KCP);
+#pragma unroll
+        for (int kk = 0; kk < KC; kk += 2) {
+          float4 q = cy[kk >> 1];
+          cfma(acc[kk], make_float2(q.x, q.y), v);
+          cfma(acc[kk + 1], make_float2(q.z, q.w), v);
+        }
+      }
+      float4* pr = reinterpret_cast<float4*>(P + x * KCP);
+#pragma unroll
+      for (int kk = 0; kk < KC; kk += 2)
+        pr[kk >> 1] = make_float4(acc[kk].x, acc[kk].y, acc[kk + 1].x, acc[kk + 1].y);
+    }
+    __syncthreads();
+    // DFT along x: thread per kx
+    for (int kx = tid; kx < W; kx += nt) {
+      float2 acc[KC];
+#pragma unroll
+      for (int kk = 0; kk < KC; ++kk) acc[kk] = czero();
+      const int step = (kx - g.sx + W) % W;
+      int jj = (step * ((W - g.sx) % W)) % W;  // index for x = 0
+      for (int x = 0; x < W; ++x) {
+        const float2 tw = twx[jj];
+        const float4* pr = reinterpret_cast<const float4*>(P + x * KCP);
+#pragma unroll
+        for (int kk = 0; kk < KC; kk += 2) {
+          float4 q = pr[kk >> 1];
+          cfma(acc[kk], tw, make_float2(q.x, q.y));
+          cfma(acc[kk + 1], tw, make_float2(q.z, q.w));
+        }
+        jj += step;
+        if (jj >= W) jj -= W;
+      }
+      float4* xr = reinterpret_cast<float4*>(X + kx * KCP);
+#pragma unroll
+      for (int kk = 0; kk < KC; kk += 2)
+        xr[kk >> 1] = make_float4(acc[kk].x * g.inv_sqrt_w, acc[kk].y * g.inv_sqrt_w,
+                                  acc[kk + 1].x * g.inv_sqrt_w, acc[kk + 1].y * g.inv_sqrt_w);
+    }
+    __syncthreads();
+    // pointwise stage on the kept samples
+    for (int e = tid; e < kc * W; e += nt) {
+      const int kk = e / W, kx = e % W;
+      const long long gi = zb + (long long)(k0 + kk) * W + kx;
+      const float m = g.mrow[(long long)(r0 + k0 + kk) * W + kx];
+      const float2 Xv = X[kx * KCP + kk];
+      const float2 mX = cscale(Xv, m);
+      if (mode == 0) {
+        const float2 zo = a.z[gi], dv = a.d[gi];
+        // z += sigma * (mask X); z = (z - sigma d) * 1/(1 + sigma/lambda); z *= mask
+        float2 zn = make_float2(zo.x + sig * mX.x, zo.y + sig * mX.y);
+        zn = make_float2(zn.x - sig * dv.x, zn.y - sig * dv.y);
+        zn = cscale(zn, zscale);
+        zn = cscale(zn, m);
+        a.z[gi] = zn;
+        X[kx * KCP + kk] = zn;
+      } else if (mode == 1) {
+        acc_r[0] += (double)cabs2(mX);
+      } else if (mode == 2) {
+        const float2 zo = a.z[gi], dv = a.d[gi];
+        const float2 r = csub(mX, dv);
+        acc_r[0] += (double)cabs2(r);
+        acc_r[1] += (double)dv.x * zo.x + (double)dv.y * zo.y;
+        acc_r[2] += (double)cabs2(zo);
+        const float2 zm = cscale(zo, m);
+        if (!a.binary_mask) a.z[gi] = zm;
+        X[kx * KCP + kk] = zm;
+      } else {
+        const int ky = g.rows[r0 + k0 + kk];
+        a.dense_out[(((long long)t * C + c) * H + ky) * W + kx] = mX;
+      }
+    }
+    if (mode == 1 || mode == 3) continue;
+    __syncthreads();
+    // inverse DFT along x: thread per x
+    for (int x = tid; x < W; x += nt) {
+      float2 acc[KC];
+#pragma unroll
+      for (int kk = 0; kk < KC; ++kk) acc[kk] = czero();
+      const int step = (x - g.sx + W) % W;
+      int jj = (step * ((W - g.sx) % W)) % W;  // index for kx = 0
+      for (int kx = 0; kx < W; ++kx) {
+        const float2 tw = twx[jj];
+        const float2 twc = make_float2(tw.x, -tw.y);
+        const float4* xr = reinterpret_cast<const float4*>(X + kx * KCP);
+#pragma unroll
+        for (int kk = 0; kk < KC; kk += 2) {
+          float4 q = xr[kk >> 1];
+          cfma(acc[kk], twc, make_float2(q.x, q.y));
+          cfma(acc[kk + 1], twc, make_float2(q.z, q.w));
+        }
+        jj += step;
+        if (jj >= W) jj -= W;
+      }
+      for (int kk = 0; kk < kc; ++kk)
+        a.qp[zb + (long long)(k0 + kk) * W + x] = cscale(acc[kk], g.inv_sqrt_w);
+    }
+  }
+  if (mode == 1 || mode == 2) {
+    block_sum<3>(acc_r, red);
+    if (tid == 0) {
+      const int nb = gridDim.x;
+      a.partial[0 * nb + blockIdx.x] = acc_r[0];
+      a.partial[1 * nb + blockIdx.x] = acc_r[1];
+      a.partial[2 * nb + blockIdx.x] = acc_r[2];
+    }
+  }
+}
+
+size_t kspace_smem_bytes(int W, int H) {
+  const int KCP = KSPACE_KC + 2;
+  return sizeof(float2) * ((size_t)H * KCP + 2 * (size_t)W * KCP + W) + sizeof(double) * 32 * 3;
+}
+
+// ---------------------------------------------------------------------------
+// Column adjoint of the compact rows for a 32 x 16 pixel tile of frame t:
+//   acc[y,x] = sum_c conj(b1[c,y,x]) 1/sqrt(H) sum_k e^{-2 pi i (ky_k-sy)(y-sy)/H} Q'[t,c,k,x]
+// which completes K^H (cartesian_operator.cpp:65-111) from Q'.
+// ---------------------------------------------------------------------------
+
+struct AdjSmem {
+  float2 q[ADJ_KQ * ADJ_TX];
+  float2 cf[ADJ_KQ * ADJ_TH];
+};
+
+AVX_D void adjoint_tile(const KArgs& k, int t, int x0, int y0, float2 (&acc)[ADJ_YP], AdjSmem& sm) {
+  const CartGeomDev& g = k.g;
+  const int W = g.W, H = g.H;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + ADJ_TX * ty;
+  const int nthr = ADJ_TX * ADJ_TY;
+  const int r0 = g.row_off[t], r1 = g.row_off[t + 1];
+  const int S = r1 - r0;
+  const int x = x0 + tx;
+  const long long HW = (long long)W * H;
+#pragma unroll
+  for (int j = 0; j < ADJ_YP; ++j) acc[j] = czero();
+  for (int c = 0; c < g.C; ++c) {
+    float2 racc[ADJ_YP];
+#pragma unroll
+    for (int j = 0; j < ADJ_YP; ++j) racc[j] = czero();
+    const long long base = kbase(g, t, c, r0, r1);
+    for (int k0 = 0; k0 < S; k0 += ADJ_KQ) {
+      const int kc = min(ADJ_KQ, S - k0);
+      __syncthreads();
+      for (int e = tid; e < ADJ_KQ * ADJ_TX; e += nthr) {
+        const int kk = e / ADJ_TX, xx = e % ADJ_TX;
+        sm.q[e] = (kk < kc && x0 + xx < W) ? k.qp[base + (long long)(k0 + kk) * W + x0 + xx] : czero();
+      }
+      for (int e = tid; e < ADJ_KQ * ADJ_TH; e += nthr) {
+        const int kk = e / ADJ_TH, yy = e % ADJ_TH;
+        float2 v = czero();
+        if (kk < kc && y0 + yy < H) {
+          const int ky = g.rows[r0 + k0 + kk];
+          const int a1 = (ky - g.sy + H) % H, a2 = (y0 + yy - g.sy + H) % H;
+          const float2 w = g.twy[(a1 * a2) % H];
+          v = make_float2(w.x * g.inv_sqrt_h, -w.y * g.inv_sqrt_h);
+        }
+        sm.cf[e] = v;
+      }
+      __syncthreads();
+      for (int kk = 0; kk < kc; ++kk) {
+        const float2 q = sm.q[kk * ADJ_TX + tx];
+#pragma unroll
+        for (int j = 0; j < ADJ_YP; ++j) cfma(racc[j], sm.cf[kk * ADJ_TH + ty * ADJ_YP + j], q);
+      }
+    }
+    if (x < W) {
+#pragma unroll
+      for (int j = 0; j < ADJ_YP; ++j) {
+        const int y = y0 + ty * ADJ_YP + j;
+        if (y < H) acc[j] = cadd(acc[j], cmulc(__ldg(k.b1 + c * HW + (long long)y * W + x), racc[j]));
+      }
+    }
+  }
+}
+
+// k-space -> image (operator apply): img[t] = K^H from Q'.
+__global__ void __launch_bounds__(ADJ_TX* ADJ_TY) adjoint_kernel(KArgs k, float2* img) {
+  __shared__ AdjSmem sm;
+  const int t = blockIdx.z;
+  const int x0 = blockIdx.x * ADJ_TX, y0 = blockIdx.y * ADJ_TH;
+  float2 acc[ADJ_YP];
+  adjoint_tile(k, t, x0, y0, acc, sm);
+  const int x = x0 + threadIdx.x;
+  if (x >= k.g.W) return;
+#pragma unroll
+  for (int j = 0; j < ADJ_YP; ++j) {
+    const int y = y0 + threadIdx.y * ADJ_YP + j;
+    if (y < k.g.H) img[((long long)t * k.g.H + y) * k.g.W + x] = acc[j];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// primal update fused with K^H z
+// ---------------------------------------------------------------------------
+
+template <int M>
+__global__ void __launch_bounds__(ADJ_TX* ADJ_TY) primal_kernel(PDArgs a, KArgs k) {
+  if (a.st->stop) return;
+  __shared__ AdjSmem sm;
+  const int t = blockIdx.z;
+  const int x0 = blockIdx.x * ADJ_TX, y0 = blockIdx.y * ADJ_TH;
+  float2 kh[ADJ_YP];
+  adjoint_tile(k, t, x0, y0, kh, sm);
+  const int x = x0 + threadIdx.x;
+  if (x >= a.W) return;
+  const float tau = (float)a.st->tau;
+#pragma unroll
+  for (int j = 0; j < ADJ_YP; ++j) {
+    const int y = y0 + threadIdx.y * ADJ_YP + j;
+    if (y >= a.H) continue;
+    const PixCoord p = make_pix(x, y, t, a.W, a.H, a.T);
+    // x1 <- x1 - tau (K^H z - div y1)
+    const float2 dv1 = div3(a.y[0], a.y[1], a.y[2], p, a.w1);
+    {
+      const float2 xo = a.x[0][p.i];
+      const float2 r = csub(kh[j], dv1);
+      const float2 xn = make_float2(xo.x - tau * r.x, xo.y - tau * r.y);
+      a.x[0][p.i] = xn;
+      a.xb[0][p.i] = make_float2(2.f * xn.x - xo.x, 2.f * xn.y - xo.y);
+    }
+    if (M == AVX_M_TV) continue;
+    // x2 <- x2 + tau (y1 + symdiv y2)
+    {
+      float2 sd[3];
+      symdiv(a.y + 3, p, a.w1, sd);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float2 r = cadd(ldc(a.y[c], p.i), sd[c]);
+        const float2 xo = a.x[1 + c][p.i];
+        const float2 xn = make_float2(xo.x + tau * r.x, xo.y + tau * r.y);
+        a.x[1 + c][p.i] = xn;
+        a.xb[1 + c][p.i] = make_float2(2.f * xn.x - xo.x, 2.f * xn.y - xo.y);
+      }
+    }
+    if (M == AVX_M_ICTGV2) {
+      // x3 <- x3 - tau (div1 y1 - div2 y3)
+      const float2 dv3 = div3(a.y[9], a.y[10], a.y[11], p, a.w2);
+      {
+        const float2 r = csub(dv1, dv3);
+        const float2 xo = a.x[4][p.i];
+        const float2 xn = make_float2(xo.x - tau * r.x, xo.y - tau * r.y);
+        a.x[4][p.i] = xn;
+        a.xb[4][p.i] = make_float2(2.f * xn.x - xo.x, 2.f * xn.y - xo.y);
+      }
+      // x4 <- x4 + tau (y3 + symdiv2 y4)
+      float2 sd[3];
+      symdiv(a.y + 12, p, a.w2, sd);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float2 r = cadd(ldc(a.y[9 + c], p.i), sd[c]);
+        const float2 xo = a.x[5 + c][p.i];
+        const float2 xn = make_float2(xo.x + tau * r.x, xo.y + tau * r.y);
+        a.x[5 + c][p.i] = xn;
+        a.xb[5 + c][p.i] = make_float2(2.f * xn.x - xo.x, 2.f * xn.y - xo.y);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// step rule: image-side norms of e = xbar - x
+// (TV::AdaptStepSize tv.cpp:79-97, TGV2 tgv2.cpp:89-128, ICTGV2 ictgv2.cpp:97-161)
+// slot 0: sum of squared regulariser-operator norms; slot 1: sum |e|^2
+// ---------------------------------------------------------------------------
+
+template <int M>
+__global__ void __launch_bounds__(256) step_img_kernel(PDArgs a, Ptr8 e, double* partial) {
+  if (a.st->stop) return;
+  __shared__ double red[32 * 2];
+  double acc[2] = {0.0, 0.0};
+  const long long HW = (long long)a.W * a.H;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(i / HW);
+    const int r = (int)(i - t * HW);
+    const PixCoord p = make_pix(r % a.W, r / a.W, t, a.W, a.H, a.T);
+    if (M == AVX_M_TV) {
+      float2 g[3];
+      grad3(e.p[0], p, a.w1, g);
+      acc[0] += (double)ss3(g);
+      acc[1] += (double)cabs2(ldc(e.p[0], p.i));
+    } else {
+      float2 g[3], s[6];
+      if (M == AVX_M_TGV2)
+        grad3(e.p[0], p, a.w1, g);
+      else
+        grad3_diff(e.p[0], e.p[4], p, a.w1, g);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) g[c] = csub(g[c], ldc(e.p[1 + c], p.i));
+      acc[0] += (double)ss3(g);
+      symgrad(e.p[1], e.p[2], e.p[3], p, a.w1, s);
+      acc[0] += (double)ss6(s);
+      float nx = cabs2(ldc(e.p[0], p.i));
+#pragma unroll
+      for (int c = 0; c < 3; ++c) nx += cabs2(ldc(e.p[1 + c], p.i));
+      if (M == AVX_M_ICTGV2) {
+        grad3(e.p[4], p, a.w2, g);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) g[c] = csub(g[c], ldc(e.p[5 + c], p.i));
+        acc[0] += (double)ss3(g);
+        symgrad(e.p[5], e.p[6], e.p[7], p, a.w2, s);
+        acc[0] += (double)ss6(s);
+        nx += cabs2(ldc(e.p[4], p.i));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) nx += cabs2(ldc(e.p[5 + c], p.i));
+      }
+      acc[1] += (double)nx;
+    }
+  }
+  block_sum<2>(acc, red);
+  if (threadIdx.x == 0) {
+    partial[0 * gridDim.x + blockIdx.x] = acc[0];
+    partial[1 * gridDim.x + blockIdx.x] = acc[1];
+  }
+}
+
+// e = xbar - x for every primal component (the reference's subVector before
+// AdaptStepSize, tgv2.cpp:306-314)
+__global__ void diff_kernel(PDArgs a, Ptr8 e, int P) {
+  if (a.st->stop) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.N;
+       i += (long long)gridDim.x * blockDim.x) {
+    for (int c = 0; c < P; ++c) e.p[c][i] = csub(a.xb[c][i], a.x[c][i]);
+  }
+}
+
+__global__ void step_finalize_kernel(DevState* st, const double* pimg, int nimg, const double* pk,
+                                     int nk, double ratio) {
+  if (st->stop) return;
+  __shared__ double red[32 * 3];
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int i = threadIdx.x; i < nimg; i += blockDim.x) {
+    v[0] += pimg[i];
+    v[1] += pimg[nimg + i];
+  }
+  for (int i = threadIdx.x; i < nk; i += blockDim.x) v[2] += pk[i];
+  block_sum<3>(v, red);
+  if (threadIdx.x == 0) {
+    const double nKx = sqrt(fabs(v[0] + v[2]));
+    const double nx = sqrt(fabs(v[1]));
+    st->nKx2 = v[0] + v[2];
+    st->nx2 = v[1];
+    // PDRecon::AdaptStepSize (pd_recon.cpp:40-61)
+    const double tmp = nx / nKx;
+    const double theta = 0.95;
+    double s = st->sigma, tt = st->tau;
+    if (s * tt > tmp * tmp) {
+      if (theta * theta * s * tt < tmp * tmp) {
+        s *= theta;
+        tt *= theta;
+      } else {
+        s = tmp * ratio;
+        tt = tmp / ratio;
+      }
+    }
+    st->sigma = (double)(float)s;
+    st->tau = (double)(float)tt;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// primal-dual gap, image side (needs K^H z from a fresh Q').
+// slots: 0 g3 = |K^H z - div y1|_1, 1 g4, 2 g5, 3 g6,
+//        4..7 regulariser L1 sums n1..n4 (see gap_finalize_kernel)
+// ---------------------------------------------------------------------------
+
+template <int M>
+__global__ void __launch_bounds__(ADJ_TX* ADJ_TY) gap_img_kernel(PDArgs a, KArgs k, double* partial) {
+  if (a.st->stop) return;
+  __shared__ AdjSmem sm;
+  __shared__ double red[32 * 8];
+  const int t = blockIdx.z;
+  const int x0 = blockIdx.x * ADJ_TX, y0 = blockIdx.y * ADJ_TH;
+  float2 kh[ADJ_YP];
+  adjoint_tile(k, t, x0, y0, kh, sm);
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int x = x0 + threadIdx.x;
+  if (x < a.W) {
+#pragma unroll
+    for (int j = 0; j < ADJ_YP; ++j) {
+      const int y = y0 + threadIdx.y * ADJ_YP + j;
+      if (y >= a.H) continue;
+      const PixCoord p = make_pix(x, y, t, a.W, a.H, a.T);
+      const float2 dv1 = div3(a.y[0], a.y[1], a.y[2], p, a.w1);
+      acc[0] += (double)sqrtf(cabs2(csub(kh[j], dv1)));
+      float2 g[3];
+      if (M == AVX_M_TV) {
+        grad3(a.x[0], p, a.w1, g);
+        acc[4] += (double)nrm3(g);
+        continue;
+      }
+      float2 sd[3], e[6];
+      symdiv(a.y + 3, p, a.w1, sd);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc[1] += (double)sqrtf(cabs2(cadd(sd[c], ldc(a.y[c], p.i))));
+      if (M == AVX_M_TGV2)
+        grad3(a.x[0], p, a.w1, g);
+      else
+        grad3_diff(a.x[0], a.x[4], p, a.w1, g);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) g[c] = csub(g[c], ldc(a.x[1 + c], p.i));
+      acc[4] += (double)nrm3(g);
+      symgrad(a.x[1], a.x[2], a.x[3], p, a.w1, e);
+      acc[5] += (double)nrm6(e);
+      if (M == AVX_M_ICTGV2) {
+        const float2 dv3 = div3(a.y[9], a.y[10], a.y[11], p, a.w2);
+        acc[2] += (double)sqrtf(cabs2(csub(dv1, dv3)));
+        symdiv(a.y + 12, p, a.w2, sd);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[3] += (double)sqrtf(cabs2(cadd(sd[c], ldc(a.y[9 + c], p.i))));
+        grad3(a.x[4], p, a.w2, g);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) g[c] = csub(g[c], ldc(a.x[5 + c], p.i));
+        acc[6] += (double)nrm3(g);
+        symgrad(a.x[5], a.x[6], a.x[7], p, a.w2, e);
+        acc[7] += (double)nrm6(e);
+      }
+    }
+  }
+  block_sum<8>(acc, red);
+  const int nb = gridDim.x * gridDim.y * gridDim.z;
+  const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+#pragma unroll
+    for (int s = 0; s < 8; ++s) partial[s * nb + b] = acc[s];
+  }
+}
+
+// Assembles G* + R (tv.cpp:202-235, tgv2.cpp:130-176, ictgv2.cpp:163-249),
+// records the history and raises the stop flag.
+template <int M>
+__global__ void gap_finalize_kernel(DevState* st, const double* pk, int nk, const double* pimg, int nimg,
+                                    GapConst gc, double* hist_gap, double* hist_norm, double* hist_fid,
+                                    int cap, int init_only) {
+  if (st->stop) return;
+  __shared__ double red[32 * 11];
+  double v[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+    v[0] += pk[i];
+    v[1] += pk[nk + i];
+    v[2] += pk[2 * nk + i];
+  }
+  for (int i = threadIdx.x; i < nimg; i += blockDim.x) {
+#pragma unroll
+    for (int s = 0; s < 8; ++s) v[3 + s] += pimg[s * nimg + i];
+  }
+  block_sum<11>(v, red);
+  if (threadIdx.x != 0) return;
+  const double lam = gc.lam;
+  const double res2 = v[0] + gc.d_off_energy;
+  const double g1 = 0.5 * lam * res2;
+  const double g2 = v[1] + v[2] / (2.0 * lam);
+  const double g36 = v[3] + v[4] + v[5] + v[6];
+  double reg;
+  if (M == AVX_M_TV)
+    reg = v[7];
+  else if (M == AVX_M_TGV2)
+    reg = gc.alpha1 * v[7] + gc.alpha0 * v[8];
+  else
+    reg = gc.ic_a * (gc.alpha1 * v[7] + gc.alpha0 * v[8]) + gc.ic_b * (gc.alpha1 * v[9] + gc.alpha0 * v[10]);
+  const double gap = fabs(g1 + g2 + g36 + reg) / gc.N;
+  const double fid = sqrt(fabs(res2)) * lam / 2.0;
+  if (init_only) {
+    // ICTGV2 records norm and data fidelity once before its loop (ictgv2.cpp:318-328)
+    if (hist_norm) hist_norm[0] = reg;
+    if (hist_fid) hist_fid[0] = fid;
+    return;
+  }
+  st->gap = gap;
+  const bool stop = gap < gc.stop_gap;
+  // TGV2 returns before recording the gap that stops it (tgv2.cpp:325-328)
+  const bool record = !(M == AVX_M_TGV2 && stop);
+  if (record && st->ngap < cap) {
+    hist_gap[st->ngap] = gap;
+    if (hist_norm) hist_norm[st->ngap + 1] = reg;
+    if (hist_fid) hist_fid[st->ngap + 1] = fid;
+    st->ngap += 1;
+  }
+  if (stop) st->stop = 1;
+}
+
+// ---------------------------------------------------------------------------
+// data movement helpers
+// ---------------------------------------------------------------------------
+
+// dense (T,C,H,W) -> compact rows, optionally multiplied by the mask
+__global__ void gather_rows_kernel(CartGeomDev g, const float2* dense, float2* compact, int apply_mask) {
+  const int c = blockIdx.x % g.C, t = blockIdx.x / g.C;
+  const int r0 = g.row_off[t], r1 = g.row_off[t + 1];
+  const long long zb = kbase(g, t, c, r0, r1);
+  for (int e = threadIdx.x; e < (r1 - r0) * g.W; e += blockDim.x) {
+    const int kk = e / g.W, kx = e % g.W;
+    const int ky = g.rows[r0 + kk];
+    float2 v = dense[(((long long)t * g.C + c) * g.H + ky) * g.W + kx];
+    if (apply_mask) v = cscale(v, g.mrow[(long long)(r0 + kk) * g.W + kx]);
+    compact[zb + (long long)kk * g.W + kx] = v;
+  }
+}
+
+// k-space -> image transform of a dense k-space vector, first stage: mask the
+// input in place (cartesian_operator.cpp:83-88; rows outside the kept set
+// carry mask 0 and are cleared) and row-IDFT the kept rows into Q'.
+__global__ void dense_rowidft_kernel(CartGeomDev g, float2* dense, float2* qp, const float* mask_dense) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* row = reinterpret_cast<float2*>(smem_raw);  // [W]
+  const int c = blockIdx.x % g.C, t = blockIdx.x / g.C;
+  const int r0 = g.row_off[t], r1 = g.row_off[t + 1];
+  const long long zb = kbase(g, t, c, r0, r1);
+  float2* slice = dense + ((long long)t * g.C + c) * g.H * g.W;
+  if (mask_dense) {
+    const float* ms = mask_dense + (long long)t * g.H * g.W;
+    for (long long e = threadIdx.x; e < (long long)g.H * g.W; e += blockDim.x) slice[e] = cscale(slice[e], ms[e]);
+  }
+  __syncthreads();
+  for (int kk = 0; kk < r1 - r0; ++kk) {
+    const int ky = g.rows[r0 + kk];
+    for (int kx = threadIdx.x; kx < g.W; kx += blockDim.x) row[kx] = slice[(long long)ky * g.W + kx];
+    __syncthreads();
+    for (int x = threadIdx.x; x < g.W; x += blockDim.x) {
+      float2 acc = czero();
+      const int step = (x - g.sx + g.W) % g.W;
+      int jj = (step * ((g.W - g.sx) % g.W)) % g.W;
+      for (int kx = 0; kx < g.W; ++kx) {
+        const float2 tw = g.twx[jj];
+        cfma(acc, make_float2(tw.x, -tw.y), row[kx]);
+        jj += step;
+        if (jj >= g.W) jj -= g.W;
+      }
+      qp[zb + (long long)kk * g.W + x] = cscale(acc, g.inv_sqrt_w);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// explicit template instantiations and launch helpers
+// ---------------------------------------------------------------------------
+
+template <int M>
+static void launch_iteration_impl(const PDArgs& a, const KArgs& k, cudaStream_t s) {
+  const int HW = a.W * a.H;
+  dim3 gd((HW + 255) / 256, a.T);
+  dual_kernel<M><<<gd, 256, 0, s>>>(a);
+  kspace_kernel<KSPACE_KC><<<k.g.C * k.g.T, 256, kspace_smem_bytes(a.W, a.H), s>>>(k, 0);
+  dim3 gp((a.W + ADJ_TX - 1) / ADJ_TX, (a.H + ADJ_TH - 1) / ADJ_TH, a.T);
+  primal_kernel<M><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k);
+}
+
+void launch_iteration(int method, const PDArgs& a, const KArgs& k, cudaStream_t s) {
+  if (method == AVX_M_TV) launch_iteration_impl<AVX_M_TV>(a, k, s);
+  else if (method == AVX_M_TGV2) launch_iteration_impl<AVX_M_TGV2>(a, k, s);
+  else launch_iteration_impl<AVX_M_ICTGV2>(a, k, s);
+}
+
+void launch_primal(int method, const PDArgs& a, const KArgs& k, cudaStream_t s) {
+  dim3 gp((a.W + ADJ_TX - 1) / ADJ_TX, (a.H + ADJ_TH - 1) / ADJ_TH, a.T);
+  if (method == AVX_M_TV) primal_kernel<AVX_M_TV><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k);
+  else if (method == AVX_M_TGV2) primal_kernel<AVX_M_TGV2><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k);
+  else primal_kernel<AVX_M_ICTGV2><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k);
+}
+
+void launch_dual(int method, const PDArgs& a, cudaStream_t s) {
+  dim3 gd((a.W * a.H + 255) / 256, a.T);
+  if (method == AVX_M_TV) dual_kernel<AVX_M_TV><<<gd, 256, 0, s>>>(a);
+  else if (method == AVX_M_TGV2) dual_kernel<AVX_M_TGV2><<<gd, 256, 0, s>>>(a);
+  else dual_kernel<AVX_M_ICTGV2><<<gd, 256, 0, s>>>(a);
+}
+
+void launch_kspace(const KArgs& k, int mode, cudaStream_t s) {
+  kspace_kernel<KSPACE_KC><<<k.g.C * k.g.T, 256, kspace_smem_bytes(k.g.W, k.g.H), s>>>(k, mode);
+}
+
+void launch_adjoint(const KArgs& k, float2* img, cudaStream_t s) {
+  dim3 gp((k.g.W + ADJ_TX - 1) / ADJ_TX, (k.g.H + ADJ_TH - 1) / ADJ_TH, k.g.T);
+  adjoint_kernel<<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(k, img);
+}
+
+int gap_img_blocks(int W, int H, int T) {
+  return ((W + ADJ_TX - 1) / ADJ_TX) * ((H + ADJ_TH - 1) / ADJ_TH) * T;
+}
+
+void launch_step(int method, const PDArgs& a, const KArgs& k_e, const Ptr8& e_dev, int P,
+                 double* pimg, double* pk, double ratio, cudaStream_t s) {
+  diff_kernel<<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, P);
+  if (method == AVX_M_TV) step_img_kernel<AVX_M_TV><<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, pimg);
+  else if (method == AVX_M_TGV2) step_img_kernel<AVX_M_TGV2><<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, pimg);
+  else step_img_kernel<AVX_M_ICTGV2><<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, pimg);
+  kspace_kernel<KSPACE_KC><<<k_e.g.C * k_e.g.T, 256, kspace_smem_bytes(k_e.g.W, k_e.g.H), s>>>(k_e, 1);
+  step_finalize_kernel<<<1, 256, 0, s>>>(a.st, pimg, AVX_RED_BLOCKS, pk, k_e.g.C * k_e.g.T, ratio);
+}
+
+void launch_gap(int method, const PDArgs& a, const KArgs& k_x, double* pimg, double* pk, const GapConst& gc,
+                double* hg, double* hn, double* hf, int cap, int init_only, cudaStream_t s) {
+  kspace_kernel<KSPACE_KC><<<k_x.g.C * k_x.g.T, 256, kspace_smem_bytes(k_x.g.W, k_x.g.H), s>>>(k_x, 2);
+  dim3 gp((a.W + ADJ_TX - 1) / ADJ_TX, (a.H + ADJ_TH - 1) / ADJ_TH, a.T);
+  const int nimg = gap_img_blocks(a.W, a.H, a.T);
+  const int nk = k_x.g.C * k_x.g.T;
+  if (method == AVX_M_TV) {
+    gap_img_kernel<AVX_M_TV><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k_x, pimg);
+    gap_finalize_kernel<AVX_M_TV><<<1, 256, 0, s>>>(a.st, pk, nk, pimg, nimg, gc, hg, hn, hf, cap, init_only);
+  } else if (method == AVX_M_TGV2) {
+    gap_img_kernel<AVX_M_TGV2><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k_x, pimg);
+    gap_finalize_kernel<AVX_M_TGV2><<<1, 256, 0, s>>>(a.st, pk, nk, pimg, nimg, gc, hg, hn, hf, cap, init_only);
+  } else {
+    gap_img_kernel<AVX_M_ICTGV2><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k_x, pimg);
+    gap_finalize_kernel<AVX_M_ICTGV2><<<1, 256, 0, s>>>(a.st, pk, nk, pimg, nimg, gc, hg, hn, hf, cap, init_only);
+  }
+}
+
+void launch_gather_rows(const CartGeomDev& g, const float2* dense, float2* compact, int apply_mask, cudaStream_t s) {
+  gather_rows_kernel<<<g.C * g.T, 256, 0, s>>>(g, dense, compact, apply_mask);
+}
+
+void launch_dense_rowidft(const CartGeomDev& g, float2* dense, float2* qp, const float* mask_dense, cudaStream_t s) {
+  dense_rowidft_kernel<<<g.C * g.T, 256, sizeof(float2) * g.W, s>>>(g, dense, qp, mask_dense);
+}
+
+cudaError_t configure_kernels() {
+  // opt in to the full 227 KB of dynamic shared memory per CTA (sm_100)
+  return cudaFuncSetAttribute(kspace_kernel<KSPACE_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}
+
+}  // namespace avx

@@ -1,0 +1,237 @@
+/*
+ * avionic.h -- C ABI of the AVIONIC B200 reconstruction core (libavionic_core.so).
+ *
+ * Drop-in boundary for the reference's reconstruction path.  Each entry point
+ * replaces one piece of the reference's C++ interface (citations are paths in
+ * the IMTtugraz/AVIONIC tree):
+ *
+ *   operators  <- BaseOperator / CartesianOperator
+ *                 (CUDA/include/base_operator.h:24-112,
+ *                  CUDA/include/cartesian_operator.h:22-125)
+ *   solvers    <- PDRecon / TV / TGV2 / ICTGV2
+ *                 (CUDA/include/pd_recon.h:88-185, tv.h, tgv2.h, ictgv2.h)
+ *   utils      <- namespace utils stencils, norms, proximal maps, Ellipke
+ *                 (CUDA/include/utils.h, CUDA/src/utils.cpp)
+ *   host path  <- the avionic CLI's load -> reconstruct -> store sequence
+ *                 (CUDA/src/main.cpp:323-917)
+ *
+ * Conventions.  complex64 values are avx_cf32 {re, im} (the memory layout of
+ * std::complex<float>, CUDA/include/types.h:16).  Layouts follow the reference:
+ * image x + W*(y + H*t); k-space x + W*(y + H*(c + C*t)); coil maps
+ * x + W*(y + H*c); mask float x + W*(y + H*t).  Pointers named d_* are CUDA
+ * device pointers of the current device; h_* are host pointers.  Functions
+ * return avx_status and never throw; avx_last_error() describes the last
+ * failure of the calling thread.  Nothing here allocates on the host-visible
+ * side beyond the opaque handles.
+ */
+#ifndef AVIONIC_H_
+#define AVIONIC_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct avx_cf32 {
+  float re, im;
+} avx_cf32;
+
+typedef enum avx_status {
+  AVX_OK = 0,
+  AVX_E_ARG = 1,         /* invalid argument or dimension mismatch */
+  AVX_E_CUDA = 2,        /* CUDA runtime error */
+  AVX_E_NOMEM = 3,       /* device allocation failed */
+  AVX_E_IO = 4,          /* file could not be read or written */
+  AVX_E_UNSUPPORTED = 5, /* method or mode not provided by this library */
+  AVX_E_NUMERIC = 6      /* non-finite value detected in a result */
+} avx_status;
+
+/* Method numbers of the reference's Method enum (CUDA/include/options_parser.h,
+ * parsed at CUDA/src/options_parser.cpp:5-48). */
+enum {
+  AVX_METHOD_TV = 0,
+  AVX_METHOD_TVTEMP = 1,
+  AVX_METHOD_TGV2 = 2,
+  AVX_METHOD_TGV2_3D = 3,
+  AVX_METHOD_ICTV = 4,
+  AVX_METHOD_ICTGV2 = 5
+};
+
+/* Union of PDParams, TGV2Params and ICTGV2Params
+ * (CUDA/include/pd_recon.h:20-74, tgv2.h:9-16, ictgv2.h:9-21) plus the
+ * AdaptLambdaParams (pd_recon.h:20-32).  Fields a method does not use are
+ * ignored. */
+typedef struct avx_pd_params {
+  unsigned maxIt;
+  float stopPDGap;
+  float sigma, tau, sigmaTauRatio;
+  float timeSpaceWeight;
+  float lambda;
+  float dx, dy, dt;          /* overwritten from timeSpaceWeight by a run, as in the reference */
+  float alpha0, alpha1;      /* TGV2 / ICTGV2 */
+  float alpha;               /* ICTGV2 trade-off */
+  float timeSpaceWeight2;    /* ICTGV2 second branch */
+  float dx2, dy2, dt2;       /* ICTGV2 second branch (overwritten by a run) */
+  int adaptLambda;           /* 1: lambda = AdaptLambda(adaptK, adaptD) at solver creation */
+  float adaptK, adaptD;
+} avx_pd_params;
+
+typedef struct avx_run_stats {
+  unsigned iterations;   /* PD iterations executed */
+  float sigma, tau;      /* final step sizes */
+  unsigned gap_count;    /* gap evaluations recorded */
+  double last_gap;       /* last normalised gap (gap / N) */
+  int stopped_by_gap;    /* 1 when stopPDGap ended the run early */
+  float elapsed_ms;      /* device time of the iteration loop */
+  unsigned kernel_launches; /* kernels this library launched in the loop */
+} avx_run_stats;
+
+typedef struct avx_operator avx_operator;
+typedef struct avx_solver avx_solver;
+
+/* Export callback: the reference's ResultExportCallback
+ * (CUDA/include/pd_recon.h:76) with the data already on the host. */
+typedef void (*avx_export_cb)(const char* output_dir, const char* name, const avx_cf32* values,
+                              size_t n, void* user);
+
+const char* avx_version(void);
+const char* avx_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* Cartesian operator                                                  */
+/* ------------------------------------------------------------------ */
+
+/* CartesianOperator(width, height, coils, frames, mask, centered)
+ * (CUDA/src/cartesian_operator.cpp:3-34).  d_mask may be NULL (the reference's
+ * empty-mask constructors).  The mask is copied; the operator does not keep
+ * d_mask. */
+avx_status avx_cartesian_operator_create(unsigned width, unsigned height, unsigned coils, unsigned frames,
+                                         const float* d_mask, int centered, avx_operator** op);
+
+/* BackwardOperation(img -> k-space) (cartesian_operator.cpp:122-160):
+ * d_k[t,c] = mask[t] * F(b1[c] * x[t]); d_k is dense (W*H*C*T). */
+avx_status avx_operator_backward(avx_operator* op, const avx_cf32* d_x, avx_cf32* d_k, const avx_cf32* d_b1);
+
+/* ForwardOperation(k-space -> img) (cartesian_operator.cpp:65-111):
+ * d_x[t] = sum_c conj(b1[c]) F^-1(mask[t] * k[t,c]).  Like the reference, it
+ * multiplies d_k by the mask in place. */
+avx_status avx_operator_forward(avx_operator* op, avx_cf32* d_k, avx_cf32* d_x, const avx_cf32* d_b1);
+
+/* AdaptLambda(k, d) (cartesian_operator.cpp:47-62). */
+avx_status avx_operator_adapt_lambda(const avx_operator* op, float k, float d, float* lambda_out);
+
+void avx_operator_destroy(avx_operator* op);
+
+/* ------------------------------------------------------------------ */
+/* Primal-dual solvers                                                 */
+/* ------------------------------------------------------------------ */
+
+/* InitParams() defaults of TV / TGV2 / ICTGV2 (tv.cpp:39-57,
+ * tgv2.cpp:36-56, ictgv2.cpp:37-63), with adaptLambda = 1 and the method's
+ * (k, d). */
+avx_status avx_default_params(int method, avx_pd_params* params);
+
+/* TV/TGV2/ICTGV2(width, height, coils, frames, params, mrOp)
+ * (tv.cpp:13-19, tgv2.cpp:10-16, ictgv2.cpp:11-17).  params == NULL uses
+ * avx_default_params.  When params->adaptLambda is set, lambda is replaced
+ * by AdaptLambda(adaptK, adaptD) here (InitLambda, tv.cpp:25-37).  The
+ * solver keeps a pointer to op, which must outlive it. */
+avx_status avx_solver_create(int method, unsigned width, unsigned height, unsigned coils, unsigned frames,
+                             const avx_pd_params* params, avx_operator* op, avx_solver** solver);
+
+avx_status avx_solver_get_params(const avx_solver* s, avx_pd_params* params); /* GetParams() */
+avx_status avx_solver_set_params(avx_solver* s, const avx_pd_params* params);
+avx_status avx_solver_set_verbose(avx_solver* s, int verbose);               /* SetVerbose */
+avx_status avx_solver_set_debug(avx_solver* s, int debug, int debugstep);    /* SetDebug */
+avx_status avx_solver_set_stream(avx_solver* s, void* cuda_stream);          /* cudaStream_t, 0 = default */
+
+/* IterativeReconstruction(data, x, b1) (pd_recon.h:134-135): d_data dense
+ * k-space (W*H*C*T), d_x initial image in / result out (W*H*T), d_b1 coil maps
+ * (W*H*C).  Runs asynchronously on the solver's stream until the final
+ * stop-state read, then returns. */
+avx_status avx_solver_run(avx_solver* s, const avx_cf32* d_data, avx_cf32* d_x, const avx_cf32* d_b1);
+
+/* AdaptStepSize on given extragradient differences (tv.cpp:79-97,
+ * tgv2.cpp:89-128, ictgv2.cpp:97-161).  d_diff holds P component pointers
+ * (TV 1: e; TGV2 4: e1, e2[3]; ICTGV2 8: e1, e2[3], e3, e4[3]). */
+avx_status avx_solver_adapt_step_size(avx_solver* s, const avx_cf32* const* d_diff, const avx_cf32* d_b1);
+
+/* ComputeGStar / ComputePDGap (tv.cpp:202-235, tgv2.cpp:130-176,
+ * ictgv2.cpp:178-249) on given primal components (P pointers, as above), dual
+ * components (D pointers: TV 3, TGV2 9, ICTGV2 18), dense z and data.  The
+ * gap is returned un-normalised, as ComputePDGap returns it.  Uses the
+ * solver's current params (dx.. as set, no time-space recomputation). */
+avx_status avx_solver_compute_gap(avx_solver* s, const avx_cf32* const* d_x, const avx_cf32* const* d_y,
+                                  const avx_cf32* d_z, const avx_cf32* d_data, const avx_cf32* d_b1,
+                                  double* gstar, double* gap);
+
+/* ExportAdditionalResults (tv.cpp:237-248, tgv2.cpp:340-355,
+ * ictgv2.cpp:494-516): x3_component (ICTGV2), and with debug on PDGap,
+ * ICTGVnorm, DATAfidelity (ICTGV2). */
+avx_status avx_solver_export(avx_solver* s, const char* output_dir, avx_export_cb cb, void* user);
+avx_status avx_solver_get_stats(const avx_solver* s, avx_run_stats* stats);
+
+/* Per-kernel timing: with timing on, a run launches its kernels directly
+ * (not from CUDA graphs) with CUDA events around the dual, k-space and primal
+ * kernels of every iteration on the solver's stream.  avx_solver_kernel_times
+ * returns their mean durations in ms of the last run ([0] dual, [1] k-space,
+ * [2] primal) and how many launches of each were timed. */
+avx_status avx_solver_set_timing(avx_solver* s, int on);
+avx_status avx_solver_kernel_times(const avx_solver* s, float* mean_ms, unsigned* count);
+void avx_solver_destroy(avx_solver* s);
+
+/* ------------------------------------------------------------------ */
+/* utils: stencils, norms, proximal maps (device pointers, 3D W x H x T) */
+/* ------------------------------------------------------------------ */
+
+/* utils::Gradient (utils.cpp:99-118): d_g[0..2] = D+x u/dx, D+y u/dy, D+t u/dt */
+avx_status avx_gradient(const avx_cf32* d_u, avx_cf32* const* d_g, unsigned W, unsigned H, unsigned T,
+                        float dx, float dy, float dt);
+/* utils::Divergence (utils.cpp:733-757) */
+avx_status avx_divergence(const avx_cf32* const* d_y, avx_cf32* d_div, unsigned W, unsigned H, unsigned T,
+                          float dx, float dy, float dt);
+/* utils::SymmetricGradient, 7-argument form (utils.cpp:397-456) */
+avx_status avx_sym_gradient(const avx_cf32* const* d_v, avx_cf32* const* d_e, unsigned W, unsigned H,
+                            unsigned T, float dx, float dy, float dt);
+/* utils::SymmetricDivergence, 8-argument form (utils.cpp:961-1012) */
+avx_status avx_sym_divergence(const avx_cf32* const* d_w, avx_cf32* const* d_d, unsigned W, unsigned H,
+                              unsigned T, float dx, float dy, float dt);
+/* utils::ProximalMap3 / ProximalMap6 (utils.cpp:1341-1351), in place */
+avx_status avx_prox3(avx_cf32* const* d_y, unsigned N, float scale);
+avx_status avx_prox6(avx_cf32* const* d_y, unsigned N, float scale);
+/* utils::GradientNorm / SymmetricGradientNorm (utils.cpp:209-222, 610-631): real norms */
+avx_status avx_norm3(const avx_cf32* const* d_g, float* d_norm, unsigned N);
+avx_status avx_norm6(const avx_cf32* const* d_g, float* d_norm, unsigned N);
+/* utils::TVNorm / TGV2Norm / ICTGV2Norm (utils.cpp:1119-1287), FP64 sums */
+avx_status avx_tv_norm(const avx_cf32* d_u, unsigned W, unsigned H, unsigned T, float dx, float dy, float dt,
+                       double* out);
+avx_status avx_tgv2_norm(const avx_cf32* d_x1, const avx_cf32* const* d_x2, float alpha0, float alpha1,
+                         unsigned W, unsigned H, unsigned T, float dx, float dy, float dt, double* out);
+avx_status avx_ictgv2_norm(const avx_cf32* d_x1, const avx_cf32* const* d_x2, const avx_cf32* d_x3,
+                           const avx_cf32* const* d_x4, float alpha0, float alpha1, float alpha, unsigned W,
+                           unsigned H, unsigned T, const float* w1 /*dx,dy,dt*/, const float* w2, double* out);
+/* utils::Ellipke (utils.cpp:18-47); returns NaN outside [0, 1] */
+float avx_ellipke(float m);
+/* PDRecon::ComputeTimeSpaceWeights (pd_recon.cpp:72-98) */
+avx_status avx_time_space_weights(float time_space_weight, float* ds, float* dt);
+
+/* ------------------------------------------------------------------ */
+/* Host-buffer reconstruction (the CLI path, main.cpp:507-839)         */
+/* ------------------------------------------------------------------ */
+
+/* Copies the host inputs to the device, masks the data (main.cpp:507-519),
+ * replicates u0 over the frames (main.cpp:775-779), runs the method and
+ * copies the image back.  h_mask may be NULL (all ones); h_u0 is one frame
+ * (W*H) or NULL (zeros).  debugstep > 0 enables the gap history
+ * (options_parser.cpp:79).  stats may be NULL. */
+avx_status avx_reconstruct_host(int method, unsigned width, unsigned height, unsigned coils, unsigned frames,
+                                const avx_pd_params* params, int debugstep, const avx_cf32* h_kdata,
+                                const float* h_mask, const avx_cf32* h_b1, const avx_cf32* h_u0,
+                                avx_cf32* h_x, avx_run_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AVIONIC_H_ */

@@ -24,12 +24,30 @@ uncentred form, main.cpp:755-756).
 
 import numpy as np
 
+# When set (an int), the 2D transforms run through scipy.fft with that many
+# threads; used only to time the oracle on all host cores.
+FFT_WORKERS = None
+
+
+def _fft2(a):
+    if FFT_WORKERS:
+        import scipy.fft as sf
+        return sf.fft2(a, norm="ortho", workers=FFT_WORKERS)
+    return np.fft.fft2(a, norm="ortho")
+
+
+def _ifft2(a):
+    if FFT_WORKERS:
+        import scipy.fft as sf
+        return sf.ifft2(a, norm="ortho", workers=FFT_WORKERS)
+    return np.fft.ifft2(a, norm="ortho")
+
 
 def fft2u(a, centered=False):
     """Unitary image -> k-space transform (e^{+2 pi i} kernel)."""
     if centered:
         a = np.fft.ifftshift(a, axes=(-2, -1))
-    r = np.fft.ifft2(a, norm="ortho")
+    r = _ifft2(a)
     if centered:
         r = np.fft.fftshift(r, axes=(-2, -1))
     return r
@@ -39,7 +57,7 @@ def ifft2u(a, centered=False):
     """Unitary k-space -> image transform (e^{-2 pi i} kernel)."""
     if centered:
         a = np.fft.ifftshift(a, axes=(-2, -1))
-    r = np.fft.fft2(a, norm="ortho")
+    r = _fft2(a)
     if centered:
         r = np.fft.fftshift(r, axes=(-2, -1))
     return r

@@ -1,0 +1,56 @@
+"""CPU checks of the C ABI boundary: the library loads without a GPU and
+exports every function include/avionic.h declares, and the Python binding
+declares each of them."""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "avionic.h")
+LIB = os.path.join(ROOT, "avionic_b200", "libavionic_core.so")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(avx_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "avx_solver_run" in names and "avx_cartesian_operator_create" in names
+    assert len(names) >= 30
+
+
+@pytest.mark.skipif(not os.path.exists(LIB), reason="library not built")
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(LIB)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+@pytest.mark.skipif(not os.path.exists(LIB), reason="library not built")
+def test_python_binding_covers_header():
+    from avionic_b200 import _abi
+    assert sorted(_abi.SIGNATURES) == declared_functions()
+
+
+@pytest.mark.skipif(not os.path.exists(LIB), reason="library not built")
+def test_cpu_only_entry_points():
+    """Entry points that do no device work answer on a CPU-only host."""
+    import avionic_b200 as av
+    assert av.lib.avx_version().startswith(b"avionic-b200")
+    assert abs(av.ellipke(0.5) - 1.3506) < 1e-3
+    ds, dt = av.time_space_weights(5.0)
+    from oracle import stencils as st
+    rds, rdt = st.time_space_weights(5.0)
+    assert abs(ds - rds) < 1e-6 and abs(dt - rdt) < 1e-6
+    p = av.default_params(av.ICTGV2)
+    assert p.maxIt == 500 and abs(p.alpha - 0.6423) < 1e-6 and abs(p.timeSpaceWeight - 6.5) < 1e-6
+    with pytest.raises(av.AvionicError):
+        av.default_params(av.TGV2_3D)
+    with pytest.raises(av.AvionicError):
+        av.time_space_weights(-1.0)

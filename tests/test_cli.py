@@ -1,0 +1,115 @@
+"""The avionic executable: flags, configuration, .bin formats, exports.
+
+CPU tests cover the paths that end before any device work (usage, invalid
+method, unknown configuration keys, dimension mismatch, truncated files);
+the GPU test runs a full reconstruction through the executable and compares
+the written image with the float64 oracle.
+"""
+
+import os
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import binfmt
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "avionic_b200", "avionic")
+
+needs_exe = pytest.mark.skipif(not os.path.exists(EXE), reason="avionic executable not built")
+
+
+def run(args, **kw):
+    return subprocess.run([EXE] + args, capture_output=True, text=True, timeout=600, **kw)
+
+
+def write_problem(tmp, prob, with_u0=True):
+    T, C, H, W = prob["kdata"].shape
+    paths = {k: str(tmp / (k + ".bin")) for k in ("kdata", "mask", "b1", "u0")}
+    binfmt.write_bin(paths["kdata"], prob["kdata"].astype(np.complex128))
+    binfmt.write_bin(paths["mask"], prob["mask"].astype(np.float64))
+    binfmt.write_bin(paths["b1"], prob["b1"].astype(np.complex128))
+    if with_u0:
+        binfmt.write_bin(paths["u0"], np.zeros((H, W), np.complex128))
+    return paths, "%d:%d:1:%d:%d:1:%d:%d" % (W, H, W, H, C, T)
+
+
+@needs_exe
+def test_usage_and_errors(tmp_path):
+    r = run(["-h"])
+    assert r.returncode == 255 and "Usage: avionic" in r.stdout
+    r = run([])
+    assert r.returncode == 255
+    rng = np.random.default_rng(0)
+    prob = {"kdata": (rng.standard_normal((2, 2, 4, 5)) + 0j).astype(np.complex64),
+            "mask": np.ones((2, 4, 5), np.float32), "b1": np.ones((2, 4, 5), np.complex64)}
+    paths, dims = write_problem(tmp_path, prob)
+    out = str(tmp_path / "x.bin")
+    r = run(["-m", "NOPE", "-d", dims, "-s", paths["b1"], paths["kdata"], paths["mask"], out])
+    assert r.returncode == 255 and "invalid method" in r.stderr
+    r = run(["-m", "TGV2_3D", "-d", dims, "-s", paths["b1"], paths["kdata"], paths["mask"], out])
+    assert r.returncode == 255 and "not provided" in r.stderr
+    cfg = tmp_path / "bad.cfg"
+    cfg.write_text("[tv]\nlambdaa = 3\n")
+    r = run(["-p", str(cfg), "-m", "TV", "-d", dims, "-s", paths["b1"], paths["kdata"], paths["mask"], out])
+    assert r.returncode == 255 and "unrecognised option 'tv.lambdaa'" in r.stderr
+    bad_dims = dims.replace(":2:2", ":3:2")
+    r = run(["-m", "TV", "-d", bad_dims, "-s", paths["b1"], paths["kdata"], paths["mask"], out])
+    assert r.returncode == 255 and "dims require" in r.stderr
+    trunc = tmp_path / "trunc.bin"
+    with open(paths["kdata"], "rb") as f:
+        trunc.write_bytes(f.read()[:40])
+    r = run(["-m", "TV", "-d", dims, "-s", paths["b1"], str(trunc), paths["mask"], out])
+    assert r.returncode == 255 and "truncated" in r.stderr
+
+
+def test_bin_format_roundtrip(tmp_path):
+    """The .bin layout of matlab/writebin_vector.m:35-44."""
+    v = np.arange(5) + 1j * np.arange(5, 10)
+    p = tmp_path / "v.bin"
+    binfmt.write_bin(str(p), v)
+    raw = p.read_bytes()
+    assert raw[0] == 1 and struct.unpack("<I", raw[1:5])[0] == 5 and len(raw) == 5 + 80
+    assert np.array_equal(binfmt.read_bin(str(p)), v)
+    binfmt.write_bin(str(p), np.arange(3.0))
+    assert p.read_bytes()[0] == 0 and len(p.read_bytes()) == 5 + 24
+
+
+@needs_exe
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["TV", "TGV2", "ICTGV2"])
+def test_cli_reconstruction_matches_oracle(tmp_path, method):
+    from avionic_b200 import synth
+    from oracle import solvers as so
+    from oracle.cartesian import CartesianOperator
+    prob = synth.small(21)
+    T, C, H, W = prob["kdata"].shape
+    paths, dims = write_problem(tmp_path, prob)
+    out = str(tmp_path / "recon.bin")
+    cfg = tmp_path / "run.cfg"
+    cfg.write_text("maxIt = 80\n[tv]\nlambda = 2.5\ntimeSpaceWeight = 3.0\n[tgv2]\nlambda = 2.5\n"
+                   "timeSpaceWeight = 1.4\n[ictgv2]\nlambda = 2.5\ntimeSpaceWeight = 4.0\n"
+                   "timeSpaceWeight2 = 0.5\nalpha = 0.5\n")
+    r = run(["-m", method, "-p", str(cfg), "-e", "-g", "10", "-d", dims, "-s", paths["b1"], "-u", paths["u0"],
+             paths["kdata"], paths["mask"], out])
+    assert r.returncode == 0, r.stderr + r.stdout
+    x = binfmt.read_bin(out).reshape(T, H, W)
+
+    op = CartesianOperator(W, H, C, T, mask=prob["mask"], centered=False)
+    p = so.init_params(method)
+    p.maxIt, p.lam, p.sigma, p.tau = 80, 2.5, 0.3333, 0.3333
+    p.timeSpaceWeight = {"TV": 3.0, "TGV2": 1.4, "ICTGV2": 4.0}[method]
+    p.timeSpaceWeight2, p.alpha = 0.5, 0.5
+    p.alpha0 = 1.41421356
+    p.debug, p.debugstep = True, 10
+    tr = {}
+    xo = so.run(method, prob["kdata"].astype(complex), np.zeros((T, H, W), complex), prob["b1"].astype(complex),
+                op, p, tr)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-4
+    gaps = binfmt.read_bin(str(tmp_path / "PDGap"))
+    assert np.allclose(gaps.real, tr["PDGap"], rtol=2e-4)
+    if method == "ICTGV2":
+        assert binfmt.read_bin(str(tmp_path / "x3_component")).size == T * H * W
+        assert binfmt.read_bin(str(tmp_path / "ICTGVnorm")).size == len(tr["ICTGVnorm"])

@@ -1,0 +1,182 @@
+"""CUDA path vs the float64 oracle on seeded synthetic problems.
+
+Tolerances: operator outputs 1e-5 relative L2 (FP32 arithmetic against
+FP64); adjointness <Kx, z> = <x, K^H z> to 1e-5 relative; reconstructions
+1e-4 relative L2 image error, the bar the method is held to.
+"""
+
+import numpy as np
+import pytest
+
+from oracle import solvers as so
+from oracle.cartesian import CartesianOperator as OCart
+
+pytestmark = pytest.mark.gpu
+
+REL_OP = 1e-5
+REL_IMG = 1e-4
+
+
+@pytest.fixture(scope="module")
+def av():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import avionic_b200
+    return avionic_b200
+
+
+def rel(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def cplx(rng, shape):
+    return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(np.complex64)
+
+
+CASES = [
+    # W, H, C, T, mask kind, centered
+    (12, 10, 3, 4, "lines", False),
+    (13, 9, 2, 3, "random", True),
+    (32, 24, 4, 5, "weights", False),
+    (20, 20, 3, 2, None, True),
+    (96, 64, 2, 3, "lines", False),
+]
+
+
+def _mask(kind, T, H, W, rng):
+    if kind is None:
+        return None
+    if kind == "lines":
+        m = np.zeros((T, H, W), np.float32)
+        for t in range(T):
+            m[t, rng.choice(H, size=max(1, H // 3), replace=False), :] = 1
+        return m
+    if kind == "random":
+        return (rng.random((T, H, W)) > 0.6).astype(np.float32)
+    m = np.zeros((T, H, W), np.float32)
+    for t in range(T):
+        m[t, rng.choice(H, size=max(1, H // 2), replace=False), :] = 1
+    return m * rng.uniform(0.3, 1.7, size=(T, H, W)).astype(np.float32)
+
+
+@pytest.mark.parametrize("W,H,C,T,kind,centered", CASES)
+def test_operator_matches_oracle(av, W, H, C, T, kind, centered):
+    rng = np.random.default_rng(W * 1000 + H)
+    mask = _mask(kind, T, H, W, rng)
+    x, b1, k = cplx(rng, (T, H, W)), cplx(rng, (C, H, W)), cplx(rng, (T, C, H, W))
+    op = av.CartesianOperator(W, H, C, T, mask=None if mask is None else av.to_device(mask), centered=centered)
+    oop = OCart(W, H, C, T, mask=mask, centered=centered)
+    kg = op.backward(av.to_device(x), av.to_device(b1)).cpu().numpy()
+    ko = oop.backward(x.astype(complex), b1.astype(complex))
+    assert rel(kg, ko) < REL_OP
+    kd = av.to_device(k)
+    ig = op.forward(kd, av.to_device(b1)).cpu().numpy()
+    kref = k.astype(complex)
+    io = oop.forward(kref, b1.astype(complex))
+    assert rel(ig, io) < REL_OP
+    # the input is masked in place, as in the reference
+    assert rel(kd.cpu().numpy(), kref) < 1e-6 or np.linalg.norm(kref) == 0
+
+
+@pytest.mark.parametrize("W,H,C,T,kind,centered", CASES)
+def test_operator_adjointness(av, W, H, C, T, kind, centered):
+    """test_adjointness.m:1-13 / cartesian_operator.cc:150-200 on the device."""
+    rng = np.random.default_rng(7 + W)
+    mask = _mask(kind, T, H, W, rng)
+    if mask is not None:
+        mask = (mask != 0).astype(np.float32)  # K^H is the adjoint for a 0/1 mask
+    x, b1, z = cplx(rng, (T, H, W)), cplx(rng, (C, H, W)), cplx(rng, (T, C, H, W))
+    op = av.CartesianOperator(W, H, C, T, mask=None if mask is None else av.to_device(mask), centered=centered)
+    kx = op.backward(av.to_device(x), av.to_device(b1)).cpu().numpy().astype(complex)
+    khz = op.forward(av.to_device(z), av.to_device(b1)).cpu().numpy().astype(complex)
+    lhs = np.vdot(kx, z.astype(complex))
+    rhs = np.vdot(x.astype(complex), khz)
+    assert abs(lhs - rhs) / abs(lhs) < REL_OP
+
+
+def _oracle_run(method, prob, iters, debugstep=0, stop=0.0, centered=False, u0=None):
+    T, C, H, W = prob["kdata"].shape
+    op = OCart(W, H, C, T, mask=prob["mask"], centered=centered)
+    p = so.init_params(method)
+    p.lam = op.adapt_lambda(*p.adapt_kd)
+    p.maxIt = iters
+    p.debug = debugstep > 0
+    p.debugstep = max(debugstep, 1)
+    p.stopPDGap = stop
+    x0 = np.zeros((T, H, W), complex) if u0 is None else np.repeat(u0[None].astype(complex), T, axis=0)
+    tr = {}
+    x = so.run(method, prob["kdata"].astype(complex), x0, prob["b1"].astype(complex), op, p, tr)
+    return x, tr, p
+
+
+def _gpu_run(av, method, prob, iters, debugstep=0, stop=0.0, centered=False, u0=None):
+    import torch
+    T, C, H, W = prob["kdata"].shape
+    op = av.CartesianOperator(W, H, C, T, mask=av.to_device(prob["mask"]), centered=centered)
+    s = av.Solver(method, op)
+    p = s.params
+    p.maxIt = iters
+    p.stopPDGap = stop
+    s.params = p
+    s.set_debug(debugstep > 0, max(debugstep, 1))
+    x = torch.zeros((T, H, W), dtype=torch.complex64, device="cuda") if u0 is None else \
+        av.to_device(np.repeat(u0[None], T, axis=0))
+    s.run(av.to_device(prob["kdata"]), x, av.to_device(prob["b1"]))
+    return x.cpu().numpy(), s
+
+
+@pytest.mark.parametrize("method", ["TV", "TGV2", "ICTGV2"])
+@pytest.mark.parametrize("binary", [True, False])
+def test_solver_matches_oracle_small(av, method, binary):
+    from avionic_b200 import synth
+    prob = synth.small(11, binary=binary)
+    xo, tro, _ = _oracle_run(method, prob, 120, debugstep=10)
+    xg, s = _gpu_run(av, method, prob, 120, debugstep=10)
+    assert rel(xg, xo) < REL_IMG, rel(xg, xo)
+    st = s.stats()
+    assert st.iterations == 120
+    assert abs(st.sigma - tro["steps"][-1][0]) < 1e-5 * tro["steps"][-1][0]
+    ex = s.export()
+    gaps = ex["PDGap"].real
+    assert len(gaps) == len(tro["PDGap"])
+    assert np.allclose(gaps, tro["PDGap"], rtol=2e-4)
+    if method == "ICTGV2":
+        assert "x3_component" in ex
+        assert np.allclose(ex["ICTGVnorm"].real, tro["ICTGVnorm"], rtol=2e-4)
+        assert np.allclose(ex["DATAfidelity"].real, tro["DATAfidelity"], rtol=2e-4)
+
+
+@pytest.mark.parametrize("method", ["TV", "TGV2", "ICTGV2"])
+def test_stop_criterion(av, method):
+    """stopPDGap ends the loop at the same gap evaluation as the oracle
+    (tv.cpp:186-190, tgv2.cpp:325-326, ictgv2.cpp:481-482)."""
+    from avionic_b200 import synth
+    prob = synth.small(5)
+    xo, tro, _ = _oracle_run(method, prob, 400, stop=2e-3)
+    xg, s = _gpu_run(av, method, prob, 400, stop=2e-3)
+    st = s.stats()
+    assert st.stopped_by_gap == 1
+    assert st.iterations == tro["iterations"] + 1
+    assert rel(xg, xo) < REL_IMG
+
+
+def test_config0_tv_full(av):
+    """Benchmark configuration 0 (128x128, 20 frames, 8 coils, 500 iterations)."""
+    from avionic_b200 import synth
+    prob = synth.config0(0)
+    u0 = synth.time_average_u0(prob["kdata"], prob["mask"], prob["b1"])
+    xo, _, _ = _oracle_run("TV", prob, 500, u0=u0)
+    xg, _ = _gpu_run(av, "TV", prob, 500, u0=u0)
+    assert rel(xg, xo) < REL_IMG, rel(xg, xo)
+
+
+def test_reconstruct_host_matches_device_path(av):
+    from avionic_b200 import synth
+    prob = synth.small(3)
+    p = av.default_params(av.TGV2)
+    p.maxIt = 60
+    x, st = av.reconstruct_host("TGV2", prob["kdata"], prob["mask"], prob["b1"], params=p)
+    xo, _, _ = _oracle_run("TGV2", prob, 60)
+    assert rel(x, xo) < REL_IMG
+    assert st.iterations == 60
