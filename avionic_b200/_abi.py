@@ -64,6 +64,7 @@ SIGNATURES = {
     "avx_tgv2_norm": (I, [VP, C.POINTER(VP), F, F, U, U, U, F, F, F, C.POINTER(D)]),
     "avx_ictgv2_norm": (I, [VP, C.POINTER(VP), VP, C.POINTER(VP), F, F, F, U, U, U, C.POINTER(F), C.POINTER(F),
                             C.POINTER(D)]),
+    "avx_tv_norm_noalloc": (I, [VP, U, U, U, F, F, F, C.POINTER(D)]),
     "avx_ellipke": (F, [F]),
     "avx_time_space_weights": (I, [F, C.POINTER(F), C.POINTER(F)]),
     "avx_reconstruct_host": (I, [I, U, U, U, U, C.POINTER(PDParams), I, VP, VP, VP, VP, VP, C.POINTER(RunStats)]),

@@ -152,6 +152,8 @@ avx_status configure_once() {
 
 }  // namespace
 
+void avx_internal_set_error(const char* msg) { g_err = msg; }
+
 // ===========================================================================
 // Cartesian operator
 // ===========================================================================

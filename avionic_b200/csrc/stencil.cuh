@@ -9,7 +9,7 @@
 // difference direction, the extent n and the stride s of that direction.
 #pragma once
 
-#include "common.cuh"
+#include "pd_args.cuh"
 
 AVX_D float2 ldc(const float2* __restrict__ u, long long i) { return __ldg(u + i); }
 

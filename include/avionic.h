@@ -211,6 +211,17 @@ avx_status avx_tgv2_norm(const avx_cf32* d_x1, const avx_cf32* const* d_x2, floa
 avx_status avx_ictgv2_norm(const avx_cf32* d_x1, const avx_cf32* const* d_x2, const avx_cf32* d_x3,
                            const avx_cf32* const* d_x4, float alpha0, float alpha1, float alpha, unsigned W,
                            unsigned H, unsigned T, const float* w1 /*dx,dy,dt*/, const float* w2, double* out);
+/* TV norm that allocates nothing (no counterpart in the reference).  Same
+ * result as avx_tv_norm, for callers that cannot allocate device memory when
+ * they need it: the partial sums live in a fixed 64 KiB __device__ array that
+ * every GPU loading the library holds until exit.  W*H*T must not exceed
+ * 2,097,152 pixels (AVX_E_ARG otherwise).  The first call on a device resolves
+ * the array's address and should precede any stream capture; calls that
+ * overlap on the GPU race on the shared array.  Runs on the legacy default
+ * stream and returns after the result reached *out. */
+avx_status avx_tv_norm_noalloc(const avx_cf32* d_u, unsigned W, unsigned H, unsigned T, float dx, float dy,
+                               float dt, double* out);
+
 /* utils::Ellipke (utils.cpp:18-47); returns NaN outside [0, 1] */
 float avx_ellipke(float m);
 /* PDRecon::ComputeTimeSpaceWeights (pd_recon.cpp:72-98) */
