@@ -21,6 +21,7 @@
 
 #include "../../include/avionic.h"
 #include "pd_kernels.cuh"
+#include "radial.cuh"
 #include "utils_kernels.cuh"
 
 
@@ -146,6 +147,7 @@ bool g_configured = false;
 avx_status configure_once() {
   if (g_configured) return AVX_OK;
   AVX_CK(avx::configure_kernels());
+  AVX_CK(avx::configure_radial_kernels());
   g_configured = true;
   return AVX_OK;
 }
@@ -158,8 +160,27 @@ void avx_internal_set_error(const char* msg) { g_err = msg; }
 // Cartesian operator
 // ===========================================================================
 
+// Radix passes of a length-n FFT (4s first, then 2, 3, 5, 7, 11, 13); empty
+// when n has a larger prime factor, in which case the dense DFT is used.
+static std::vector<int> fft_radices(int n) {
+  std::vector<int> r;
+  while (n % 4 == 0) { r.push_back(4); n /= 4; }
+  for (int p : {2, 3, 5, 7, 11, 13})
+    while (n % p == 0) { r.push_back(p); n /= p; }
+  if (n != 1 || r.size() > 12) r.clear();
+  return r;
+}
+
 struct avx_operator {
+  int kind = 0;  // 0 Cartesian, 1 radial
   int W = 0, H = 0, C = 0, T = 0, centered = 0;
+  std::vector<int> radx;
+  // radial (gridding) operator
+  int S = 0, spf = 0;
+  RadialGeomDev rg{};
+  DevBuf<float> r_traj, r_sqrtw, r_ipx, r_ipy;
+  DevBuf<int> r_order, r_secstart;
+  DevBuf<float2> r_twgx, r_twgy, r_grid, r_khz;
   bool has_mask = false, binary = true;
   std::vector<int> rows, row_off;
   int R = 0;
@@ -180,6 +201,8 @@ struct avx_operator {
     g.twy = d_twy.p;
     g.inv_sqrt_w = (float)(1.0 / std::sqrt((double)W));
     g.inv_sqrt_h = (float)(1.0 / std::sqrt((double)H));
+    g.nrad = (int)radx.size();
+    for (int i = 0; i < 12; ++i) g.rad[i] = i < g.nrad ? radx[i] : 0;
     return g;
   }
 };
@@ -212,6 +235,7 @@ static avx_status build_operator(avx_operator* op, const float* h_mask) {
   }
   op->row_off[T] = (int)op->rows.size();
   op->R = (int)op->rows.size();
+  op->radx = fft_radices(W);
   std::vector<float2> twx(W), twy(H);
   for (int j = 0; j < W; ++j) twx[j] = make_float2((float)std::cos(2.0 * M_PI * j / W), (float)std::sin(2.0 * M_PI * j / W));
   for (int j = 0; j < H; ++j) twy[j] = make_float2((float)std::cos(2.0 * M_PI * j / H), (float)std::sin(2.0 * M_PI * j / H));
@@ -231,6 +255,167 @@ static avx_status build_operator(avx_operator* op, const float* h_mask) {
     AVX_CK(cudaMemcpy(op->d_mask.p, h_mask, (size_t)T * H * W * sizeof(float), cudaMemcpyHostToDevice));
   }
   return AVX_OK;
+}
+
+// 64-point Gauss-Legendre nodes and weights on [-1, 1] (Newton on P_n)
+static void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+  x.resize(n);
+  w.resize(n);
+  for (int i = 0; i < n; ++i) {
+    double z = std::cos(M_PI * (i + 0.75) / (n + 0.5)), pp = 1.0;
+    for (int it = 0; it < 100; ++it) {
+      double p1 = 1.0, p2 = 0.0;
+      for (int j = 1; j <= n; ++j) {
+        const double p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = n * (z * p1 - p2) / (z * z - 1.0);
+      const double dz = p1 / pp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-15) break;
+    }
+    x[i] = z;
+    w[i] = 2.0 / ((1.0 - z * z) * pp * pp);
+  }
+}
+
+static double kb_weight(double u, double J, double beta) {
+  if (!(std::fabs(u) < J / 2.0)) return 0.0;
+  const double r = 2.0 * u / J;
+  return (std::cyl_bessel_i(0.0, beta * std::sqrt(std::max(1.0 - r * r, 0.0))) - 1.0) /
+         (std::cyl_bessel_i(0.0, beta) - 1.0);
+}
+
+static bool smooth13(int n) {
+  for (int p : {2, 3, 5, 7, 11, 13})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+// oversampled grid: the smallest even size >= osf * d whose prime factors are <= 13
+static int radial_grid_size(int d, double osf) {
+  int n = 2 * (int)std::ceil(osf * d / 2.0);
+  while (!smooth13(n)) n += 2;
+  return n;
+}
+
+static avx_status build_radial(avx_operator* op, const float* h_traj, const float* h_dens, float J, float sw, float osf) {
+  const int W = op->W, H = op->H, T = op->T, S = op->S;
+  if (!(J > 0.f && J <= 7.f)) return fail(AVX_E_ARG, "kernelWidth must lie in (0, 7]");
+  if (!(osf > 1.0f)) return fail(AVX_E_ARG, "osf must exceed 1");
+  const int isw = (int)sw;
+  if (isw < 2 || isw > 32 || (float)isw != sw) return fail(AVX_E_ARG, "sectorWidth must be an integer in [2, 32]");
+  RadialGeomDev& g = op->rg;
+  g.W = W; g.H = H; g.C = op->C; g.T = T; g.S = S;
+  g.Gx = radial_grid_size(W, osf);
+  g.Gy = radial_grid_size(H, osf);
+  g.sw = isw;
+  g.nsx = (g.Gx + isw - 1) / isw;
+  g.nsy = (g.Gy + isw - 1) / isw;
+  const int lastx = g.Gx - (g.nsx - 1) * isw, lasty = g.Gy - (g.nsy - 1) * isw;
+  if (J / 2.f > (float)std::min(lastx, lasty) || J / 2.f > (float)isw)
+    return fail(AVX_E_ARG, "kernelWidth too wide for the sector layout");
+  g.nw = (int)std::ceil(J) + 1;
+  g.J = J;
+  const double beta = M_PI * std::sqrt((J / osf) * (J / osf) * (osf - 0.5) * (osf - 0.5) - 0.8);
+  g.beta = (float)beta;
+  g.kb_norm = (float)(1.0 / (std::cyl_bessel_i(0.0, beta) - 1.0));
+  g.norm = (float)(1.0 / std::sqrt((double)W * H));
+  // deapodisation psi(p) = int w(t) cos(2 pi t p / G) dt
+  std::vector<double> gx, gw;
+  gauss_legendre(64, gx, gw);
+  auto deap = [&](int d, int G, std::vector<float>& inv) {
+    inv.resize(d);
+    for (int n = 0; n < d; ++n) {
+      const double p = n - d / 2;
+      double acc = 0.0;
+      for (int i = 0; i < 64; ++i) {
+        const double t = gx[i] * J / 2.0;
+        acc += gw[i] * (J / 2.0) * kb_weight(t, J, beta) * std::cos(2.0 * M_PI * t * p / G);
+      }
+      inv[n] = (float)(1.0 / acc);
+    }
+  };
+  std::vector<float> ipx, ipy;
+  deap(W, g.Gx, ipx);
+  deap(H, g.Gy, ipy);
+  // sector of every sample in float32 arithmetic, then a stable sort by sector
+  const int nsec = g.nsx * g.nsy;
+  std::vector<int> order((size_t)T * S), start((size_t)T * (nsec + 1));
+  std::vector<float> sqw((size_t)T * S);
+  for (int f = 0; f < T; ++f) {
+    std::vector<int> sec(S);
+    for (int s = 0; s < S; ++s) {
+      float px = h_traj[((size_t)f * 2 + 0) * S + s] * (float)g.Gx;
+      float py = h_traj[((size_t)f * 2 + 1) * S + s] * (float)g.Gy;
+      if (px < 0.f) px += (float)g.Gx;
+      if (py < 0.f) py += (float)g.Gy;
+      int sx = (int)std::floor(px / (float)isw), sy = (int)std::floor(py / (float)isw);
+      sx = std::min(std::max(sx, 0), g.nsx - 1);
+      sy = std::min(std::max(sy, 0), g.nsy - 1);
+      sec[s] = sy * g.nsx + sx;
+      sqw[(size_t)f * S + s] = (float)std::sqrt((double)h_dens[(size_t)f * S + s]);
+    }
+    int* ord = &order[(size_t)f * S];
+    for (int s = 0; s < S; ++s) ord[s] = s;
+    std::stable_sort(ord, ord + S, [&](int a, int b) { return sec[a] < sec[b]; });
+    int* st = &start[(size_t)f * (nsec + 1)];
+    std::fill(st, st + nsec + 1, 0);
+    for (int s = 0; s < S; ++s) st[sec[s] + 1]++;
+    for (int k = 0; k < nsec; ++k) st[k + 1] += st[k];
+  }
+  const std::vector<int> rx = fft_radices(g.Gx), ry = fft_radices(g.Gy);
+  if (rx.empty() || ry.empty()) return fail(AVX_E_UNSUPPORTED, "grid size has no FFT plan");
+  g.nradx = (int)rx.size();
+  g.nrady = (int)ry.size();
+  for (int i = 0; i < 12; ++i) {
+    g.radx[i] = i < g.nradx ? rx[i] : 0;
+    g.rady[i] = i < g.nrady ? ry[i] : 0;
+  }
+  if (avx::radial_fft_smem_bytes(std::max(g.Gx, g.Gy)) > 227 * 1024)
+    return fail(AVX_E_UNSUPPORTED, "oversampled grid too large for the grid FFT tile");
+  std::vector<float2> twx(g.Gx), twy(g.Gy);
+  for (int j = 0; j < g.Gx; ++j) twx[j] = make_float2((float)std::cos(2.0 * M_PI * j / g.Gx), (float)std::sin(2.0 * M_PI * j / g.Gx));
+  for (int j = 0; j < g.Gy; ++j) twy[j] = make_float2((float)std::cos(2.0 * M_PI * j / g.Gy), (float)std::sin(2.0 * M_PI * j / g.Gy));
+  AVX_CK(op->r_traj.alloc((size_t)T * 2 * S));
+  AVX_CK(op->r_sqrtw.alloc((size_t)T * S));
+  AVX_CK(op->r_ipx.alloc(W));
+  AVX_CK(op->r_ipy.alloc(H));
+  AVX_CK(op->r_order.alloc(order.size()));
+  AVX_CK(op->r_secstart.alloc(start.size()));
+  AVX_CK(op->r_twgx.alloc(g.Gx));
+  AVX_CK(op->r_twgy.alloc(g.Gy));
+  AVX_CK(op->r_grid.alloc((size_t)T * op->C * g.Gx * g.Gy));
+  AVX_CK(op->r_khz.alloc((size_t)T * H * W));
+  AVX_CK(cudaMemcpy(op->r_traj.p, h_traj, (size_t)T * 2 * S * sizeof(float), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(op->r_sqrtw.p, sqw.data(), sqw.size() * sizeof(float), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(op->r_ipx.p, ipx.data(), W * sizeof(float), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(op->r_ipy.p, ipy.data(), H * sizeof(float), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(op->r_order.p, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(op->r_secstart.p, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(op->r_twgx.p, twx.data(), g.Gx * sizeof(float2), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(op->r_twgy.p, twy.data(), g.Gy * sizeof(float2), cudaMemcpyHostToDevice));
+  g.traj = op->r_traj.p;
+  g.sqrt_w = op->r_sqrtw.p;
+  g.inv_psi_x = op->r_ipx.p;
+  g.inv_psi_y = op->r_ipy.p;
+  g.order = op->r_order.p;
+  g.sec_start = op->r_secstart.p;
+  g.twgx = op->r_twgx.p;
+  g.twgy = op->r_twgy.p;
+  return AVX_OK;
+}
+
+static RArgs make_rargs(avx_operator* op, const float2* b1, const float2* in, const float2* in2) {
+  RArgs r;
+  memset(&r, 0, sizeof(r));
+  r.g = op->rg;
+  r.b1 = b1;
+  r.in = in;
+  r.in2 = in2;
+  r.grid = op->r_grid.p;
+  return r;
 }
 
 static avx_status check_dims(unsigned W, unsigned H, unsigned C, unsigned T) {

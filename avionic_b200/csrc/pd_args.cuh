@@ -19,6 +19,8 @@ struct CartGeomDev {
   const float2* twx;      // [W] exp(+2 pi i j / W)
   const float2* twy;      // [H] exp(+2 pi i j / H)
   float inv_sqrt_w, inv_sqrt_h;
+  int nrad;               // radix passes of the length-W row FFT (0: dense DFT)
+  int rad[12];            // radices, first pass first
 };
 
 AVX_HD long long kbase(const CartGeomDev& g, int t, int c, int r0, int r1) {
@@ -41,6 +43,7 @@ struct PDArgs {
   float r1, r2, r3, r4;  // prox scales (1/radius) of y1, y2, y3, y4
   float alpha0, alpha1, alpha;  // regulariser weights (norm evaluation)
   float ic_a, ic_b;             // ICTGV2 branch factors alpha/m, (1-alpha)/m
+  const float2* khz;            // K^H z image when the operator supplies it (radial)
   DevState* st;
 };
 

@@ -12,6 +12,7 @@
 // reductions plus a one-block finaliser that updates device-resident scalars.
 #include "pd_kernels.cuh"
 #include "stencil.cuh"
+#include "fft.cuh"
 
 namespace avx {
 
@@ -166,6 +167,7 @@ __global__ void __launch_bounds__(256) kspace_kernel(KArgs a, int mode) {
       float2 acc[KC];
 #pragma unroll
       for (int kk = 0; kk < KC; ++kk) acc[kk] = czero();
+#pragma unroll 4
       for (int y = 0; y < H; ++y) {
         float2 v = u[(long long)y * W + x];
         if (u2) v = csub(v, u2[(long long)y * W + x]);
@@ -178,13 +180,20 @@ __global__ void __launch_bounds__(256) kspace_kernel(KArgs a, int mode) {
           cfma(acc[kk + 1], make_float2(q.z, q.w), v);
         }
       }
-      float4* pr = reinterpret_cast<float4*>(P + x * KCP);
+      // with the FFT, sequence position n holds x = n + sx (the ifftshift of
+      // the centred transform); the dense DFT indexes x directly
+      const int xs = g.nrad ? (x - g.sx + W) % W : x;
+      float4* pr = reinterpret_cast<float4*>(P + xs * KCP);
 #pragma unroll
       for (int kk = 0; kk < KC; kk += 2)
         pr[kk >> 1] = make_float4(acc[kk].x, acc[kk].y, acc[kk + 1].x, acc[kk + 1].y);
     }
     __syncthreads();
-    // DFT along x: thread per kx
+    float2* Xb = X;  // buffer holding the row transform, index (kx - sx) mod W with the FFT
+    if (g.nrad) {
+      Xb = row_fft<KC>(P, X, twx, W, g.nrad, g.rad, +1);
+    } else {
+    // dense DFT along x: thread per kx
     for (int kx = tid; kx < W; kx += nt) {
       float2 acc[KC];
 #pragma unroll
@@ -206,16 +215,17 @@ __global__ void __launch_bounds__(256) kspace_kernel(KArgs a, int mode) {
       float4* xr = reinterpret_cast<float4*>(X + kx * KCP);
 #pragma unroll
       for (int kk = 0; kk < KC; kk += 2)
-        xr[kk >> 1] = make_float4(acc[kk].x * g.inv_sqrt_w, acc[kk].y * g.inv_sqrt_w,
-                                  acc[kk + 1].x * g.inv_sqrt_w, acc[kk + 1].y * g.inv_sqrt_w);
+        xr[kk >> 1] = make_float4(acc[kk].x, acc[kk].y, acc[kk + 1].x, acc[kk + 1].y);
     }
     __syncthreads();
-    // pointwise stage on the kept samples
+    }
+    // pointwise stage on the kept samples; Xb[n] holds kx = n + sx (FFT) or kx
     for (int e = tid; e < kc * W; e += nt) {
       const int kk = e / W, kx = e % W;
+      const int n = g.nrad ? (kx - g.sx + W) % W : kx;
       const long long gi = zb + (long long)(k0 + kk) * W + kx;
       const float m = g.mrow[(long long)(r0 + k0 + kk) * W + kx];
-      const float2 Xv = X[kx * KCP + kk];
+      const float2 Xv = cscale(Xb[n * KCP + kk], g.inv_sqrt_w);
       const float2 mX = cscale(Xv, m);
       if (mode == 0) {
         const float2 zo = a.z[gi], dv = a.d[gi];
@@ -225,7 +235,7 @@ __global__ void __launch_bounds__(256) kspace_kernel(KArgs a, int mode) {
         zn = cscale(zn, zscale);
         zn = cscale(zn, m);
         a.z[gi] = zn;
-        X[kx * KCP + kk] = zn;
+        Xb[n * KCP + kk] = zn;
       } else if (mode == 1) {
         acc_r[0] += (double)cabs2(mX);
       } else if (mode == 2) {
@@ -236,7 +246,7 @@ __global__ void __launch_bounds__(256) kspace_kernel(KArgs a, int mode) {
         acc_r[2] += (double)cabs2(zo);
         const float2 zm = cscale(zo, m);
         if (!a.binary_mask) a.z[gi] = zm;
-        X[kx * KCP + kk] = zm;
+        Xb[n * KCP + kk] = zm;
       } else {
         const int ky = g.rows[r0 + k0 + kk];
         a.dense_out[(((long long)t * C + c) * H + ky) * W + kx] = mX;
@@ -244,7 +254,17 @@ __global__ void __launch_bounds__(256) kspace_kernel(KArgs a, int mode) {
     }
     if (mode == 1 || mode == 3) continue;
     __syncthreads();
-    // inverse DFT along x: thread per x
+    if (g.nrad) {
+      // inverse row FFT; Xb position n holds kx = n + sx, the result position n holds x = n + sx
+      float2* Qb = row_fft<KC>(Xb, Xb == X ? P : X, twx, W, g.nrad, g.rad, -1);
+      for (int e = tid; e < kc * W; e += nt) {
+        const int kk = e / W, x = e % W;
+        const int n = (x - g.sx + W) % W;
+        a.qp[zb + (long long)(k0 + kk) * W + x] = cscale(Qb[n * KCP + kk], g.inv_sqrt_w);
+      }
+      continue;
+    }
+    // dense inverse DFT along x: thread per x
     for (int x = tid; x < W; x += nt) {
       float2 acc[KC];
 #pragma unroll
@@ -290,7 +310,7 @@ size_t kspace_smem_bytes(int W, int H) {
 // which completes K^H (cartesian_operator.cpp:65-111) from Q'.
 // ---------------------------------------------------------------------------
 
-struct AdjSmem {
+struct __align__(16) AdjSmem {
   float2 q[ADJ_KQ * ADJ_TX];
   float2 cf[ADJ_KQ * ADJ_TH];
 };
@@ -333,8 +353,13 @@ AVX_D void adjoint_tile(const KArgs& k, int t, int x0, int y0, float2 (&acc)[ADJ
       __syncthreads();
       for (int kk = 0; kk < kc; ++kk) {
         const float2 q = sm.q[kk * ADJ_TX + tx];
+        const float4* cf4 = reinterpret_cast<const float4*>(sm.cf + kk * ADJ_TH + ty * ADJ_YP);
 #pragma unroll
-        for (int j = 0; j < ADJ_YP; ++j) cfma(racc[j], sm.cf[kk * ADJ_TH + ty * ADJ_YP + j], q);
+        for (int j = 0; j < ADJ_YP; j += 2) {
+          const float4 c2 = cf4[j >> 1];
+          cfma(racc[j], make_float2(c2.x, c2.y), q);
+          cfma(racc[j + 1], make_float2(c2.z, c2.w), q);
+        }
       }
     }
     if (x < W) {
@@ -367,14 +392,24 @@ __global__ void __launch_bounds__(ADJ_TX* ADJ_TY) adjoint_kernel(KArgs k, float2
 // primal update fused with K^H z
 // ---------------------------------------------------------------------------
 
-template <int M>
+template <int M, bool CART>
 __global__ void __launch_bounds__(ADJ_TX* ADJ_TY) primal_kernel(PDArgs a, KArgs k) {
   if (a.st->stop) return;
   __shared__ AdjSmem sm;
   const int t = blockIdx.z;
   const int x0 = blockIdx.x * ADJ_TX, y0 = blockIdx.y * ADJ_TH;
   float2 kh[ADJ_YP];
-  adjoint_tile(k, t, x0, y0, kh, sm);
+  if (CART) {
+    adjoint_tile(k, t, x0, y0, kh, sm);
+  } else {
+    // K^H z supplied as an image by the operator (radial)
+#pragma unroll
+    for (int j = 0; j < ADJ_YP; ++j) {
+      const int y = y0 + threadIdx.y * ADJ_YP + j;
+      const int x = x0 + threadIdx.x;
+      kh[j] = (x < a.W && y < a.H) ? a.khz[((long long)t * a.H + y) * a.W + x] : czero();
+    }
+  }
   const int x = x0 + threadIdx.x;
   if (x >= a.W) return;
   const float tau = (float)a.st->tau;
@@ -538,7 +573,7 @@ __global__ void step_finalize_kernel(DevState* st, const double* pimg, int nimg,
 //        4..7 regulariser L1 sums n1..n4 (see gap_finalize_kernel)
 // ---------------------------------------------------------------------------
 
-template <int M>
+template <int M, bool CART>
 __global__ void __launch_bounds__(ADJ_TX* ADJ_TY) gap_img_kernel(PDArgs a, KArgs k, double* partial) {
   if (a.st->stop) return;
   __shared__ AdjSmem sm;
@@ -546,7 +581,16 @@ __global__ void __launch_bounds__(ADJ_TX* ADJ_TY) gap_img_kernel(PDArgs a, KArgs
   const int t = blockIdx.z;
   const int x0 = blockIdx.x * ADJ_TX, y0 = blockIdx.y * ADJ_TH;
   float2 kh[ADJ_YP];
-  adjoint_tile(k, t, x0, y0, kh, sm);
+  if (CART) {
+    adjoint_tile(k, t, x0, y0, kh, sm);
+  } else {
+#pragma unroll
+    for (int j = 0; j < ADJ_YP; ++j) {
+      const int y = y0 + threadIdx.y * ADJ_YP + j;
+      const int x = x0 + threadIdx.x;
+      kh[j] = (x < a.W && y < a.H) ? a.khz[((long long)t * a.H + y) * a.W + x] : czero();
+    }
+  }
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const int x = x0 + threadIdx.x;
   if (x < a.W) {
@@ -717,7 +761,7 @@ static void launch_iteration_impl(const PDArgs& a, const KArgs& k, cudaStream_t 
   dual_kernel<M><<<gd, 256, 0, s>>>(a);
   kspace_kernel<KSPACE_KC><<<k.g.C * k.g.T, 256, kspace_smem_bytes(a.W, a.H), s>>>(k, 0);
   dim3 gp((a.W + ADJ_TX - 1) / ADJ_TX, (a.H + ADJ_TH - 1) / ADJ_TH, a.T);
-  primal_kernel<M><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k);
+  primal_kernel<M, true><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k);
 }
 
 void launch_iteration(int method, const PDArgs& a, const KArgs& k, cudaStream_t s) {
@@ -726,11 +770,18 @@ void launch_iteration(int method, const PDArgs& a, const KArgs& k, cudaStream_t 
   else launch_iteration_impl<AVX_M_ICTGV2>(a, k, s);
 }
 
-void launch_primal(int method, const PDArgs& a, const KArgs& k, cudaStream_t s) {
+void launch_primal(int method, const PDArgs& a, const KArgs& k, cudaStream_t s, bool cart) {
   dim3 gp((a.W + ADJ_TX - 1) / ADJ_TX, (a.H + ADJ_TH - 1) / ADJ_TH, a.T);
-  if (method == AVX_M_TV) primal_kernel<AVX_M_TV><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k);
-  else if (method == AVX_M_TGV2) primal_kernel<AVX_M_TGV2><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k);
-  else primal_kernel<AVX_M_ICTGV2><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k);
+  dim3 bl(ADJ_TX, ADJ_TY);
+  if (cart) {
+    if (method == AVX_M_TV) primal_kernel<AVX_M_TV, true><<<gp, bl, 0, s>>>(a, k);
+    else if (method == AVX_M_TGV2) primal_kernel<AVX_M_TGV2, true><<<gp, bl, 0, s>>>(a, k);
+    else primal_kernel<AVX_M_ICTGV2, true><<<gp, bl, 0, s>>>(a, k);
+  } else {
+    if (method == AVX_M_TV) primal_kernel<AVX_M_TV, false><<<gp, bl, 0, s>>>(a, k);
+    else if (method == AVX_M_TGV2) primal_kernel<AVX_M_TGV2, false><<<gp, bl, 0, s>>>(a, k);
+    else primal_kernel<AVX_M_ICTGV2, false><<<gp, bl, 0, s>>>(a, k);
+  }
 }
 
 void launch_dual(int method, const PDArgs& a, cudaStream_t s) {
@@ -753,32 +804,48 @@ int gap_img_blocks(int W, int H, int T) {
   return ((W + ADJ_TX - 1) / ADJ_TX) * ((H + ADJ_TH - 1) / ADJ_TH) * T;
 }
 
-void launch_step(int method, const PDArgs& a, const KArgs& k_e, const Ptr8& e_dev, int P,
-                 double* pimg, double* pk, double ratio, cudaStream_t s) {
+void launch_step_img(int method, const PDArgs& a, const Ptr8& e_dev, int P, double* pimg, cudaStream_t s) {
   diff_kernel<<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, P);
   if (method == AVX_M_TV) step_img_kernel<AVX_M_TV><<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, pimg);
   else if (method == AVX_M_TGV2) step_img_kernel<AVX_M_TGV2><<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, pimg);
   else step_img_kernel<AVX_M_ICTGV2><<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, pimg);
+}
+
+void launch_step_finalize(const PDArgs& a, double* pimg, double* pk, int nk, double ratio, cudaStream_t s) {
+  step_finalize_kernel<<<1, 256, 0, s>>>(a.st, pimg, AVX_RED_BLOCKS, pk, nk, ratio);
+}
+
+void launch_step(int method, const PDArgs& a, const KArgs& k_e, const Ptr8& e_dev, int P,
+                 double* pimg, double* pk, double ratio, cudaStream_t s) {
+  launch_step_img(method, a, e_dev, P, pimg, s);
   kspace_kernel<KSPACE_KC><<<k_e.g.C * k_e.g.T, 256, kspace_smem_bytes(k_e.g.W, k_e.g.H), s>>>(k_e, 1);
-  step_finalize_kernel<<<1, 256, 0, s>>>(a.st, pimg, AVX_RED_BLOCKS, pk, k_e.g.C * k_e.g.T, ratio);
+  launch_step_finalize(a, pimg, pk, k_e.g.C * k_e.g.T, ratio, s);
+}
+
+void launch_gap_tail(int method, const PDArgs& a, const KArgs& k_x, double* pimg, double* pk, int nk,
+                     const GapConst& gc, double* hg, double* hn, double* hf, int cap, int init_only, bool cart,
+                     cudaStream_t s) {
+  dim3 gp((a.W + ADJ_TX - 1) / ADJ_TX, (a.H + ADJ_TH - 1) / ADJ_TH, a.T);
+  dim3 bl(ADJ_TX, ADJ_TY);
+  const int nimg = gap_img_blocks(a.W, a.H, a.T);
+#define GAP_IMG(MM)                                                        \
+  if (cart) gap_img_kernel<MM, true><<<gp, bl, 0, s>>>(a, k_x, pimg);     \
+  else gap_img_kernel<MM, false><<<gp, bl, 0, s>>>(a, k_x, pimg);         \
+  gap_finalize_kernel<MM><<<1, 256, 0, s>>>(a.st, pk, nk, pimg, nimg, gc, hg, hn, hf, cap, init_only);
+  if (method == AVX_M_TV) {
+    GAP_IMG(AVX_M_TV)
+  } else if (method == AVX_M_TGV2) {
+    GAP_IMG(AVX_M_TGV2)
+  } else {
+    GAP_IMG(AVX_M_ICTGV2)
+  }
+#undef GAP_IMG
 }
 
 void launch_gap(int method, const PDArgs& a, const KArgs& k_x, double* pimg, double* pk, const GapConst& gc,
                 double* hg, double* hn, double* hf, int cap, int init_only, cudaStream_t s) {
   kspace_kernel<KSPACE_KC><<<k_x.g.C * k_x.g.T, 256, kspace_smem_bytes(k_x.g.W, k_x.g.H), s>>>(k_x, 2);
-  dim3 gp((a.W + ADJ_TX - 1) / ADJ_TX, (a.H + ADJ_TH - 1) / ADJ_TH, a.T);
-  const int nimg = gap_img_blocks(a.W, a.H, a.T);
-  const int nk = k_x.g.C * k_x.g.T;
-  if (method == AVX_M_TV) {
-    gap_img_kernel<AVX_M_TV><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k_x, pimg);
-    gap_finalize_kernel<AVX_M_TV><<<1, 256, 0, s>>>(a.st, pk, nk, pimg, nimg, gc, hg, hn, hf, cap, init_only);
-  } else if (method == AVX_M_TGV2) {
-    gap_img_kernel<AVX_M_TGV2><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k_x, pimg);
-    gap_finalize_kernel<AVX_M_TGV2><<<1, 256, 0, s>>>(a.st, pk, nk, pimg, nimg, gc, hg, hn, hf, cap, init_only);
-  } else {
-    gap_img_kernel<AVX_M_ICTGV2><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k_x, pimg);
-    gap_finalize_kernel<AVX_M_ICTGV2><<<1, 256, 0, s>>>(a.st, pk, nk, pimg, nimg, gc, hg, hn, hf, cap, init_only);
-  }
+  launch_gap_tail(method, a, k_x, pimg, pk, k_x.g.C * k_x.g.T, gc, hg, hn, hf, cap, init_only, true, s);
 }
 
 void launch_gather_rows(const CartGeomDev& g, const float2* dense, float2* compact, int apply_mask, cudaStream_t s) {

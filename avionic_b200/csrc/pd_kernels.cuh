@@ -27,7 +27,12 @@ cudaError_t configure_kernels();
 
 void launch_iteration(int method, const PDArgs& a, const KArgs& k, cudaStream_t s);
 void launch_dual(int method, const PDArgs& a, cudaStream_t s);
-void launch_primal(int method, const PDArgs& a, const KArgs& k, cudaStream_t s);
+void launch_primal(int method, const PDArgs& a, const KArgs& k, cudaStream_t s, bool cart = true);
+void launch_step_img(int method, const PDArgs& a, const Ptr8& e_dev, int P, double* pimg, cudaStream_t s);
+void launch_step_finalize(const PDArgs& a, double* pimg, double* pk, int nk, double ratio, cudaStream_t s);
+void launch_gap_tail(int method, const PDArgs& a, const KArgs& k_x, double* pimg, double* pk, int nk,
+                     const GapConst& gc, double* hg, double* hn, double* hf, int cap, int init_only, bool cart,
+                     cudaStream_t s);
 void launch_kspace(const KArgs& k, int mode, cudaStream_t s);
 void launch_adjoint(const KArgs& k, float2* img, cudaStream_t s);
 void launch_step(int method, const PDArgs& a, const KArgs& k_e, const Ptr8& e_dev, int P,

@@ -1,0 +1,329 @@
+// Radial gridding operator kernels (see radial.cuh and oracle/radial.py).
+//
+// Forward  (image -> samples): pad+deapodise -> 2D DFT (sign -1) -> interpolate
+// Adjoint  (samples -> image): spread (sector gather) -> 2D DFT (sign +1) ->
+//                              crop+deapodise+coil-combine
+// The spreading step gathers: one CTA per (frame, sector) owns the sector's
+// grid cells and reads every sample of the 3x3 neighbouring sectors, so each
+// grid value is a fixed-order sum (no floating-point atomics, deterministic).
+#include "fft.cuh"
+#include "radial.cuh"
+
+namespace avx {
+
+#define RAD_FFT_KC 16
+#define RAD_SPREAD_BATCH 64
+#define RAD_SPREAD_CC 8  // coils accumulated per pass of the spreading kernel
+
+// tapered Kaiser-Bessel weight at offset u (grid units); zero for |u| >= J/2
+AVX_D float kbw(float u, const RadialGeomDev& g) {
+  if (!(fabsf(u) < 0.5f * g.J)) return 0.f;
+  const float r = 2.f * u / g.J;
+  return (cyl_bessel_i0f(g.beta * sqrtf(fmaxf(1.f - r * r, 0.f))) - 1.f) * g.kb_norm;
+}
+
+AVX_D int imod(int a, int n) {
+  const int r = a % n;
+  return r < 0 ? r + n : r;
+}
+
+// grid index -> image index along one axis, or -1 outside the image
+AVX_D int grid_to_img(int m, int d, int G) {
+  const int h = d / 2;
+  if (m < d - h) return m + h;
+  if (m >= G - h) return m - G + h;
+  return -1;
+}
+
+__global__ void rad_pad_kernel(RArgs a) {
+  const RadialGeomDev& g = a.g;
+  const int slice = blockIdx.y;  // f * C + c
+  const int c = slice % g.C, f = slice / g.C;
+  const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= g.Gx * g.Gy) return;
+  const int gy = cell / g.Gx, gx = cell % g.Gx;
+  const int ny = grid_to_img(gy, g.H, g.Gy), nx = grid_to_img(gx, g.W, g.Gx);
+  float2 v = czero();
+  if (ny >= 0 && nx >= 0) {
+    const long long pi = ((long long)f * g.H + ny) * g.W + nx;
+    float2 u = a.in[pi];
+    if (a.in2) u = csub(u, a.in2[pi]);
+    v = cscale(cmul(a.b1[((long long)c * g.H + ny) * g.W + nx], u), g.inv_psi_y[ny] * g.inv_psi_x[nx]);
+  }
+  a.grid[(long long)slice * g.Gx * g.Gy + cell] = v;
+}
+
+// rows (along x) of 16 grid lines per CTA
+__global__ void __launch_bounds__(256) rad_fft_rows_kernel(RArgs a, int sign) {
+  constexpr int KC = RAD_FFT_KC, KCP = KC + 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const RadialGeomDev& g = a.g;
+  const int G = g.Gx;
+  float2* A = reinterpret_cast<float2*>(smem_raw);
+  float2* B = A + (size_t)G * KCP;
+  float2* tw = B + (size_t)G * KCP;
+  const int slice = blockIdx.y;
+  const int r0 = blockIdx.x * KC;
+  const int rows = min(KC, g.Gy - r0);
+  float2* base = a.grid + (long long)slice * g.Gx * g.Gy;
+  for (int j = threadIdx.x; j < G; j += blockDim.x) tw[j] = g.twgx[j];
+  for (int e = threadIdx.x; e < KC * G; e += blockDim.x) {
+    const int kk = e / G, x = e % G;
+    A[x * KCP + kk] = kk < rows ? base[(long long)(r0 + kk) * G + x] : czero();
+  }
+  __syncthreads();
+  const float2* R = row_fft<KC>(A, B, tw, G, g.nradx, g.radx, sign);
+  for (int e = threadIdx.x; e < rows * G; e += blockDim.x) {
+    const int kk = e / G, x = e % G;
+    base[(long long)(r0 + kk) * G + x] = R[x * KCP + kk];
+  }
+}
+
+// columns (along y) of 16 grid columns per CTA
+__global__ void __launch_bounds__(256) rad_fft_cols_kernel(RArgs a, int sign) {
+  constexpr int KC = RAD_FFT_KC, KCP = KC + 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const RadialGeomDev& g = a.g;
+  const int G = g.Gy;
+  float2* A = reinterpret_cast<float2*>(smem_raw);
+  float2* B = A + (size_t)G * KCP;
+  float2* tw = B + (size_t)G * KCP;
+  const int slice = blockIdx.y;
+  const int c0 = blockIdx.x * KC;
+  const int cols = min(KC, g.Gx - c0);
+  float2* base = a.grid + (long long)slice * g.Gx * g.Gy;
+  for (int j = threadIdx.x; j < G; j += blockDim.x) tw[j] = g.twgy[j];
+  for (int e = threadIdx.x; e < KC * G; e += blockDim.x) {
+    const int kk = e % KC, y = e / KC;
+    A[y * KCP + kk] = kk < cols ? base[(long long)y * g.Gx + c0 + kk] : czero();
+  }
+  __syncthreads();
+  const float2* R = row_fft<KC>(A, B, tw, G, g.nrady, g.rady, sign);
+  for (int e = threadIdx.x; e < KC * G; e += blockDim.x) {
+    const int kk = e % KC, y = e / KC;
+    if (kk < cols) base[(long long)y * g.Gx + c0 + kk] = R[y * KCP + kk];
+  }
+}
+
+// window of one sample along one axis: start index (unwrapped) and weights
+template <int NW>
+AVX_D int sample_window(float kappa, const RadialGeomDev& g, float (&w)[NW]) {
+  const int g0 = (int)floorf(kappa - 0.5f * g.J);
+#pragma unroll
+  for (int o = 0; o < NW; ++o) w[o] = kbw(kappa - (float)(g0 + o), g);
+  return g0;
+}
+
+template <int NW>
+__global__ void __launch_bounds__(256) rad_interp_kernel(RArgs a, int mode) {
+  if (a.st && a.st->stop && mode != 3) return;
+  __shared__ double red[32 * 3];
+  const RadialGeomDev& g = a.g;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double acc_r[3] = {0.0, 0.0, 0.0};
+  if (i < (long long)g.T * g.S) {
+    const int f = (int)(i / g.S), s = (int)(i % g.S);
+    const float kx = g.traj[((long long)f * 2 + 0) * g.S + s];
+    const float ky = g.traj[((long long)f * 2 + 1) * g.S + s];
+    float wx[NW], wy[NW];
+    const int g0x = sample_window<NW>(kx * (float)g.Gx, g, wx);
+    const int g0y = sample_window<NW>(ky * (float)g.Gy, g, wy);
+    int ix[NW], iy[NW];
+#pragma unroll
+    for (int o = 0; o < NW; ++o) {
+      ix[o] = imod(g0x + o, g.Gx);
+      iy[o] = imod(g0y + o, g.Gy);
+    }
+    const float sc = g.sqrt_w[(long long)f * g.S + s] * g.norm;
+    const float sig = a.st ? (float)a.st->sigma : 0.f;
+    const float zscale = (mode == 0) ? (float)(1.0 / (1.0 + a.st->sigma / (double)a.lam)) : 1.f;
+    for (int c = 0; c < g.C; ++c) {
+      const float2* gr = a.grid + ((long long)f * g.C + c) * g.Gx * g.Gy;
+      float2 v = czero();
+#pragma unroll
+      for (int oy = 0; oy < NW; ++oy) {
+        float2 row = czero();
+#pragma unroll
+        for (int ox = 0; ox < NW; ++ox) {
+          const float2 q = gr[(long long)iy[oy] * g.Gx + ix[ox]];
+          row.x = fmaf(wx[ox], q.x, row.x);
+          row.y = fmaf(wx[ox], q.y, row.y);
+        }
+        v.x = fmaf(wy[oy], row.x, v.x);
+        v.y = fmaf(wy[oy], row.y, v.y);
+      }
+      const float2 k = cscale(v, sc);
+      const long long zi = ((long long)f * g.C + c) * g.S + s;
+      if (mode == 0) {
+        // z += sigma K x; z = (z - sigma d) / (1 + sigma / lambda)   (tgv2.cpp:254-264)
+        const float2 zo = a.z[zi], dv = a.d[zi];
+        float2 zn = make_float2(zo.x + sig * k.x, zo.y + sig * k.y);
+        zn = make_float2(zn.x - sig * dv.x, zn.y - sig * dv.y);
+        a.z[zi] = cscale(zn, zscale);
+      } else if (mode == 1) {
+        acc_r[0] += (double)cabs2(k);
+      } else if (mode == 2) {
+        const float2 zo = a.z[zi], dv = a.d[zi];
+        acc_r[0] += (double)cabs2(csub(k, dv));
+        acc_r[1] += (double)dv.x * zo.x + (double)dv.y * zo.y;
+        acc_r[2] += (double)cabs2(zo);
+      } else {
+        a.out[zi] = k;
+      }
+    }
+  }
+  if (mode == 1 || mode == 2) {
+    block_sum<3>(acc_r, red);
+    if (threadIdx.x == 0) {
+      const int nb = gridDim.x;
+      a.partial[blockIdx.x] = acc_r[0];
+      a.partial[nb + blockIdx.x] = acc_r[1];
+      a.partial[2 * nb + blockIdx.x] = acc_r[2];
+    }
+  }
+}
+
+// one CTA per (sector, frame); thread = grid cell of the sector
+template <int NW>
+__global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
+  if (a.st && a.st->stop) return;
+  const RadialGeomDev& g = a.g;
+  __shared__ int s_g0x[RAD_SPREAD_BATCH], s_g0y[RAD_SPREAD_BATCH];
+  __shared__ float s_wx[RAD_SPREAD_BATCH][NW], s_wy[RAD_SPREAD_BATCH][NW];
+  __shared__ float2 s_v[RAD_SPREAD_BATCH][RAD_SPREAD_CC];
+  const int f = blockIdx.y;
+  const int sec = blockIdx.x;
+  const int sxi = sec % g.nsx, syi = sec / g.nsx;
+  const int lx = threadIdx.x % g.sw, ly = threadIdx.x / g.sw;
+  const int gx = sxi * g.sw + lx, gy = syi * g.sw + ly;
+  const bool active = gx < g.Gx && gy < g.Gy;
+  const int nsec = g.nsx * g.nsy;
+  const int* order = g.order + (long long)f * g.S;
+  const int* start = g.sec_start + (long long)f * (nsec + 1);
+  // distinct neighbouring sector offsets (fewer than three sectors along an axis wrap onto themselves)
+  const int dxn = g.nsx >= 3 ? 3 : g.nsx, dyn = g.nsy >= 3 ? 3 : g.nsy;
+  for (int c0 = 0; c0 < g.C; c0 += RAD_SPREAD_CC) {
+    const int cc = min(RAD_SPREAD_CC, g.C - c0);
+    float2 acc[RAD_SPREAD_CC];
+#pragma unroll
+    for (int k = 0; k < RAD_SPREAD_CC; ++k) acc[k] = czero();
+    for (int dy = 0; dy < dyn; ++dy) {
+      for (int dx = 0; dx < dxn; ++dx) {
+        const int nsxi = imod(sxi + (dxn == 3 ? dx - 1 : dx), g.nsx);
+        const int nsyi = imod(syi + (dyn == 3 ? dy - 1 : dy), g.nsy);
+        const int ns = nsyi * g.nsx + nsxi;
+        const int p0 = start[ns], p1 = start[ns + 1];
+        for (int b0 = p0; b0 < p1; b0 += RAD_SPREAD_BATCH) {
+          const int nb = min(RAD_SPREAD_BATCH, p1 - b0);
+          __syncthreads();
+          for (int e = threadIdx.x; e < nb; e += blockDim.x) {
+            const int j = order[b0 + e];
+            const float kx = g.traj[((long long)f * 2 + 0) * g.S + j];
+            const float ky = g.traj[((long long)f * 2 + 1) * g.S + j];
+            float wx[NW], wy[NW];
+            s_g0x[e] = sample_window<NW>(kx * (float)g.Gx, g, wx);
+            s_g0y[e] = sample_window<NW>(ky * (float)g.Gy, g, wy);
+#pragma unroll
+            for (int o = 0; o < NW; ++o) {
+              s_wx[e][o] = wx[o];
+              s_wy[e][o] = wy[o];
+            }
+            const float sc = g.sqrt_w[(long long)f * g.S + j] * g.norm;
+            for (int k = 0; k < RAD_SPREAD_CC; ++k)
+              s_v[e][k] = k < cc ? cscale(samples[((long long)f * g.C + c0 + k) * g.S + j], sc) : czero();
+          }
+          __syncthreads();
+          if (active) {
+            for (int e = 0; e < nb; ++e) {
+              const int ox = imod(gx - s_g0x[e], g.Gx), oy = imod(gy - s_g0y[e], g.Gy);
+              if (ox < NW && oy < NW) {
+                const float w = s_wx[e][ox] * s_wy[e][oy];
+#pragma unroll
+                for (int k = 0; k < RAD_SPREAD_CC; ++k) {
+                  acc[k].x = fmaf(w, s_v[e][k].x, acc[k].x);
+                  acc[k].y = fmaf(w, s_v[e][k].y, acc[k].y);
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+    if (active)
+      for (int k = 0; k < cc; ++k)
+        a.grid[(((long long)f * g.C + c0 + k) * g.Gy + gy) * g.Gx + gx] = acc[k];
+  }
+}
+
+__global__ void rad_crop_kernel(RArgs a, float2* img) {
+  if (a.st && a.st->stop) return;
+  const RadialGeomDev& g = a.g;
+  const int f = blockIdx.y;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= g.W * g.H) return;
+  const int y = p / g.W, x = p % g.W;
+  const int my = imod(y - g.H / 2, g.Gy), mx = imod(x - g.W / 2, g.Gx);
+  float2 s = czero();
+  for (int c = 0; c < g.C; ++c) {
+    const float2 v = a.grid[(((long long)f * g.C + c) * g.Gy + my) * g.Gx + mx];
+    s = cadd(s, cmulc(a.b1[((long long)c * g.H + y) * g.W + x], v));
+  }
+  img[((long long)f * g.H + y) * g.W + x] = cscale(s, g.inv_psi_y[y] * g.inv_psi_x[x]);
+}
+
+// ---------------------------------------------------------------------------
+
+size_t radial_fft_smem_bytes(int G) { return sizeof(float2) * (2 * (size_t)G * (RAD_FFT_KC + 2) + G); }
+
+int radial_interp_blocks(const RadialGeomDev& g) { return (int)(((long long)g.T * g.S + 255) / 256); }
+
+cudaError_t configure_radial_kernels() {
+  cudaError_t e = cudaFuncSetAttribute(rad_fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(rad_fft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}
+
+void launch_rad_pad(const RArgs& a, cudaStream_t s) {
+  dim3 grid((a.g.Gx * a.g.Gy + 255) / 256, a.g.C * a.g.T);
+  rad_pad_kernel<<<grid, 256, 0, s>>>(a);
+}
+
+void launch_rad_fft(const RArgs& a, int sign, cudaStream_t s) {
+  dim3 gr((a.g.Gy + RAD_FFT_KC - 1) / RAD_FFT_KC, a.g.C * a.g.T);
+  rad_fft_rows_kernel<<<gr, 256, radial_fft_smem_bytes(a.g.Gx), s>>>(a, sign);
+  dim3 gc((a.g.Gx + RAD_FFT_KC - 1) / RAD_FFT_KC, a.g.C * a.g.T);
+  rad_fft_cols_kernel<<<gc, 256, radial_fft_smem_bytes(a.g.Gy), s>>>(a, sign);
+}
+
+#define RAD_NW_DISPATCH(NWV, CALL) \
+  switch (NWV) {                   \
+    case 2: CALL(2); break;        \
+    case 3: CALL(3); break;        \
+    case 4: CALL(4); break;        \
+    case 5: CALL(5); break;        \
+    case 6: CALL(6); break;        \
+    case 7: CALL(7); break;        \
+    default: CALL(8); break;       \
+  }
+
+void launch_rad_interp(const RArgs& a, int mode, cudaStream_t s) {
+  const int nb = radial_interp_blocks(a.g);
+#define CALL_I(N) rad_interp_kernel<N><<<nb, 256, 0, s>>>(a, mode)
+  RAD_NW_DISPATCH(a.g.nw, CALL_I)
+#undef CALL_I
+}
+
+void launch_rad_spread(const RArgs& a, const float2* samples, cudaStream_t s) {
+  dim3 grid(a.g.nsx * a.g.nsy, a.g.T);
+  const int threads = a.g.sw * a.g.sw;
+#define CALL_S(N) rad_spread_kernel<N><<<grid, threads, 0, s>>>(a, samples)
+  RAD_NW_DISPATCH(a.g.nw, CALL_S)
+#undef CALL_S
+}
+
+void launch_rad_crop(const RArgs& a, float2* img, cudaStream_t s) {
+  dim3 grid((a.g.W * a.g.H + 255) / 256, a.g.T);
+  rad_crop_kernel<<<grid, 256, 0, s>>>(a, img);
+}
+
+}  // namespace avx

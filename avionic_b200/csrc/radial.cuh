@@ -1,0 +1,61 @@
+// Radial (non-Cartesian) operator: geometry and launchers (radial.cu).
+//
+// K_f x = sqrt(w_f) NUFFT_f(b1_c x_f) / sqrt(HW) with a tapered Kaiser-Bessel
+// gridding NUFFT on an oversampled grid (definition in oracle/radial.py and
+// DESIGN.md); K^H its exact adjoint.  Grid layout [frame][coil][Gy][Gx];
+// samples [frame][coil][S].
+#pragma once
+
+#include "pd_args.cuh"
+
+struct RadialGeomDev {
+  int W, H, C, T, S;        // image, coils, frames, samples per frame
+  int Gx, Gy;               // oversampled grid
+  int sw, nsx, nsy;         // sector width and sector counts
+  int nw;                   // interpolation window points per axis (ceil(J) + 1)
+  float J, beta, kb_norm;   // kernel width, shape, 1 / (I0(beta) - 1)
+  float norm;               // 1 / sqrt(W H)
+  const float* traj;        // [T][2][S] kx then ky, cycles/pixel in [-0.5, 0.5)
+  const float* sqrt_w;      // [T][S]
+  const float* inv_psi_x;   // [W] 1 / deapodisation
+  const float* inv_psi_y;   // [H]
+  const int* order;         // [T][S] sample indices sorted by sector (stable)
+  const int* sec_start;     // [T][nsx*nsy + 1] offsets into order
+  const float2* twgx;       // [Gx] exp(+2 pi i j / Gx)
+  const float2* twgy;       // [Gy]
+  int nradx, radx[12];      // FFT plan along x
+  int nrady, rady[12];      // FFT plan along y
+};
+
+struct RArgs {
+  RadialGeomDev g;
+  const float2* b1;       // [C][H][W]
+  const float2* in;       // image input [T][H][W]
+  const float2* in2;      // optional: in - in2 is transformed
+  float2* grid;           // [T][C][Gy][Gx]
+  float2* z;              // [T][C][S] dual variable
+  const float2* d;        // [T][C][S] data (already sqrt(w)-weighted, as main.cpp does)
+  float2* out;            // samples out (apply) or image out (adjoint)
+  float lam;
+  DevState* st;
+  double* partial;
+};
+
+namespace avx {
+
+size_t radial_fft_smem_bytes(int G);
+int radial_interp_blocks(const RadialGeomDev& g);
+cudaError_t configure_radial_kernels();
+
+// image -> grid: zero-padded, deapodised b1 * (in - in2)
+void launch_rad_pad(const RArgs& a, cudaStream_t s);
+// in-place unnormalised 2D DFT of every grid slice, sign -1 forward, +1 inverse
+void launch_rad_fft(const RArgs& a, int sign, cudaStream_t s);
+// grid -> samples; mode 0 z prox, 1 sum |K u|^2, 2 gap sums, 3 write samples to a.out
+void launch_rad_interp(const RArgs& a, int mode, cudaStream_t s);
+// samples (a.z, or a.in as samples when from_in) -> grid, by sector gather
+void launch_rad_spread(const RArgs& a, const float2* samples, cudaStream_t s);
+// grid -> image: crop, deapodise, coil-combine with conj(b1) into a.out
+void launch_rad_crop(const RArgs& a, float2* img, cudaStream_t s);
+
+}  // namespace avx
