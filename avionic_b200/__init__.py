@@ -132,6 +132,29 @@ class CartesianOperator:
             self.handle = ctypes.c_void_p()
 
 
+class RadialOperator(CartesianOperator):
+    """``NoncartesianOperator`` (CUDA/src/noncartesian_operator.cpp:3-195):
+    radial gridding operator.  ``traj`` float32 CUDA tensor (T, 2, S) of
+    cycles/pixel, ``dens`` float32 (T, S); k-space tensors are (T, C, S)."""
+
+    def __init__(self, width, height, coils, frames, traj, dens, spokes_per_frame, kernel_width=3.0,
+                 sector_width=8.0, osf=2.0):
+        self.W, self.H, self.C, self.T = width, height, coils, frames
+        self.S = traj.shape[-1]
+        self.handle = ctypes.c_void_p()
+        nfe = self.S // spokes_per_frame
+        check(lib.avx_radial_operator_create(width, height, coils, frames, spokes_per_frame * frames, nfe,
+                                             spokes_per_frame, _cptr(traj), _cptr(dens), kernel_width, sector_width,
+                                             osf, ctypes.byref(self.handle)))
+
+    def backward(self, x, b1, out=None):
+        torch = _torch()
+        if out is None:
+            out = torch.empty((self.T, self.C, self.S), dtype=torch.complex64, device=x.device)
+        check(lib.avx_operator_backward(self.handle, _cptr(x), _cptr(out), _cptr(b1)))
+        return out
+
+
 class Solver:
     """``TV`` / ``TGV2`` / ``ICTGV2`` (PDRecon, CUDA/include/pd_recon.h:88-185)."""
 

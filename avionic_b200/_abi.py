@@ -33,6 +33,8 @@ SIGNATURES = {
     "avx_version": (C.c_char_p, []),
     "avx_last_error": (C.c_char_p, []),
     "avx_cartesian_operator_create": (I, [U, U, U, U, VP, I, C.POINTER(VP)]),
+    "avx_radial_operator_create": (I, [U, U, U, U, U, U, U, VP, VP, F, F, F, C.POINTER(VP)]),
+    "avx_radial_sector_map": (I, [VP, VP, VP, VP]),
     "avx_operator_backward": (I, [VP, VP, VP, VP]),
     "avx_operator_forward": (I, [VP, VP, VP, VP]),
     "avx_operator_adapt_lambda": (I, [VP, F, F, C.POINTER(F)]),

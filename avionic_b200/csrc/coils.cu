@@ -1,0 +1,435 @@
+// Variational H1 coil-sensitivity estimation kernels (reference:
+// CUDA/src/coil_construction.cpp:55-556, cartesian_coil_construction.cpp:23-86).
+//
+// Images are single W x H slices (coil images stacked [coil][H][W]); the 2D
+// stencils are the (x, y) restriction of the 3D ones: gradient (D+x, D+y),
+// symmetrised gradient (xx, yy, xy with 1/2 on the off-diagonal),
+// divergences as their negative adjoints (utils.cpp:156-181, 525-568,
+// 664-684, 817-844, 1078-1117).
+#include "coils.cuh"
+#include "stencil.cuh"
+
+namespace avx {
+
+struct P2 {
+  int x, y, W, H;
+  long long i;
+};
+
+AVX_D P2 p2_of(int idx, int W, int H) {
+  P2 p;
+  p.x = idx % W;
+  p.y = idx / W;
+  p.W = W;
+  p.H = H;
+  p.i = idx;
+  return p;
+}
+
+AVX_D void grad2(const float2* u, const P2& p, float2 (&g)[2]) {
+  g[0] = d_fwd(u, p.i, p.x, p.W, 1);
+  g[1] = d_fwd(u, p.i, p.y, p.H, p.W);
+}
+AVX_D float2 div2(const float2* y0, const float2* y1, const P2& p) {
+  const float2 a = cadd(d_fwd_t(y0, p.i, p.x, p.W, 1), d_fwd_t(y1, p.i, p.y, p.H, p.W));
+  return make_float2(-a.x, -a.y);
+}
+// SymmetricGradient2D (utils.cpp:525-556): (D-x v0, D-y v1, (D-y v0 + D-x v1) / 2)
+AVX_D void symgrad2(const float2* v0, const float2* v1, const P2& p, float2 (&e)[3]) {
+  e[0] = d_bwd(v0, p.i, p.x, p.W, 1);
+  e[1] = d_bwd(v1, p.i, p.y, p.H, p.W);
+  e[2] = cadd(cscale(d_bwd(v0, p.i, p.y, p.H, p.W), 0.5f), cscale(d_bwd(v1, p.i, p.x, p.W, 1), 0.5f));
+}
+// SymmetricDivergence2D (utils.cpp:1078-1117)
+AVX_D void symdiv2(const float2* w0, const float2* w1, const float2* w2, const P2& p, float2 (&d)[2]) {
+  float2 a = cadd(d_bwd_t(w0, p.i, p.x, p.W, 1), d_bwd_t(w2, p.i, p.y, p.H, p.W));
+  d[0] = make_float2(-a.x, -a.y);
+  a = cadd(d_bwd_t(w2, p.i, p.x, p.W, 1), d_bwd_t(w1, p.i, p.y, p.H, p.W));
+  d[1] = make_float2(-a.x, -a.y);
+}
+
+// ---------------------------------------------------------------------------
+// time-averaged reconstruction
+// ---------------------------------------------------------------------------
+
+__global__ void ta_sum_kernel(const float2* kdata, const float* mask, float2* out, int HW, int C, int T) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)C * HW) return;
+  const int c = (int)(i / HW), p = (int)(i % HW);
+  float2 s = czero();
+  float m = 0.f;
+  for (int t = 0; t < T; ++t) {
+    s = cadd(s, kdata[((long long)t * C + c) * HW + p]);
+    m += mask ? mask[(long long)t * HW + p] : 1.f;
+  }
+  m = fmaxf(m, 1.f);
+  out[i] = make_float2(s.x / m, s.y / m);
+}
+
+__global__ void ta_combine_kernel(float2* crec, float2* u, int HW, int C, float scale, int apply_phase) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= HW) return;
+  float s = 0.f;
+  float2 sum = czero();
+  for (int c = 0; c < C; ++c) {
+    const float2 v = cscale(crec[(long long)c * HW + p], scale);
+    crec[(long long)c * HW + p] = v;
+    s += cabs2(v);
+    sum = cadd(sum, v);
+  }
+  float2 r = make_float2(sqrtf(s), 0.f);
+  if (apply_phase) {
+    const float ang = atan2f(sum.y, sum.x);
+    r = cmul(r, make_float2(cosf(ang), sinf(ang)));
+  }
+  u[p] = r;
+}
+
+// ---------------------------------------------------------------------------
+// H1 solve: (mu |u|^2 - Laplace_periodic) x = conj(u) mu |crec_c|, complex CG
+// in FP64, one CTA per coil (cg_forward_operation.h:47-70)
+// ---------------------------------------------------------------------------
+
+AVX_D double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+AVX_D double2 h1_apply(const double2* v, const double* muu, int x, int y, int W, int H) {
+  const int i = y * W + x;
+  const int xp = x + 1 == W ? 0 : x + 1, xm = x == 0 ? W - 1 : x - 1;
+  const int yp = y + 1 == H ? 0 : y + 1, ym = y == 0 ? H - 1 : y - 1;
+  const double2 c = v[i];
+  const double2 a = v[y * W + xp], b = v[y * W + xm], d = v[yp * W + x], e = v[ym * W + x];
+  const double m = muu[i] + 4.0;
+  return make_double2(m * c.x - a.x - b.x - d.x - e.x, m * c.y - a.y - b.y - d.y - e.y);
+}
+
+template <int NT>
+AVX_D double block_dsum(double v, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  for (int k = 0; k < NT / 32; ++k) r += red[k];
+  return r;
+}
+
+__global__ void __launch_bounds__(1024) h1_cg_kernel(const float2* u, const float2* crec, double mu, int W, int H,
+                                                     int max_it, double rel_tol, double2* work, double* muu_buf,
+                                                     float2* out, int* iters) {
+  __shared__ double red[32];
+  const int c = blockIdx.x;
+  const int N = W * H;
+  double2* x = work + (size_t)c * 4 * N;
+  double2* r = x + N;
+  double2* p = r + N;
+  double2* q = p + N;
+  double* muu = muu_buf + (size_t)c * N;
+  double rr = 0.0;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    const float2 uu = u[i];
+    const double au2 = (double)uu.x * uu.x + (double)uu.y * uu.y;
+    muu[i] = mu * au2;
+    const float2 cr = crec[(size_t)c * N + i];
+    const double ac = mu * sqrt((double)cr.x * cr.x + (double)cr.y * cr.y);
+    // conj(u) * mu |crec|
+    const double2 y = make_double2((double)uu.x * ac, -(double)uu.y * ac);
+    x[i] = make_double2(0.0, 0.0);
+    r[i] = y;
+    p[i] = y;
+    rr += y.x * y.x + y.y * y.y;
+  }
+  rr = block_dsum<1024>(rr, red);
+  const double rr0 = rr;
+  int it = 0;
+  for (; it < max_it && rr > rel_tol * rel_tol * rr0 && rr > 0.0; ++it) {
+    __syncthreads();
+    double pq = 0.0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      const double2 a = h1_apply(p, muu, i % W, i / W, W, H);
+      q[i] = a;
+      const double2 pv = p[i];
+      pq += pv.x * a.x + pv.y * a.y;
+    }
+    pq = block_dsum<1024>(pq, red);
+    const double alpha = rr / pq;
+    double rn = 0.0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      const double2 pv = p[i], qv = q[i];
+      double2 xv = x[i], rv = r[i];
+      xv.x += alpha * pv.x;
+      xv.y += alpha * pv.y;
+      rv.x -= alpha * qv.x;
+      rv.y -= alpha * qv.y;
+      x[i] = xv;
+      r[i] = rv;
+      rn += rv.x * rv.x + rv.y * rv.y;
+    }
+    rn = block_dsum<1024>(rn, red);
+    const double beta = rn / rr;
+    rr = rn;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+      const double2 rv = r[i], pv = p[i];
+      p[i] = make_double2(rv.x + beta * pv.x, rv.y + beta * pv.y);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < N; i += blockDim.x) out[(size_t)c * N + i] = make_float2((float)x[i].x, (float)x[i].y);
+  if (threadIdx.x == 0 && iters) iters[c] = it;
+}
+
+// b1 <- |b1_c / sqrt(sum_c |b1_c|^2)| (coil_construction.cpp:428-444)
+__global__ void h1_normalize_kernel(float2* b1, int HW, int C) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= HW) return;
+  float s = 0.f;
+  for (int c = 0; c < C; ++c) s += cabs2(b1[(long long)c * HW + p]);
+  const float n = sqrtf(s);
+  for (int c = 0; c < C; ++c) {
+    const float2 v = b1[(long long)c * HW + p];
+    const float2 w = make_float2(v.x / n, v.y / n);
+    b1[(long long)c * HW + p] = make_float2(sqrtf(cabs2(w)), 0.f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// UTGV2Recon (coil_construction.cpp:75-215)
+// ---------------------------------------------------------------------------
+
+__global__ void utgv_prep_kernel(const float2* b10, const float2* crec0, const int* inds, int ninds, float tau, int HW,
+                                 float2* Lw, float2* Ib) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= HW) return;
+  float2 lw = czero(), sb = czero();
+  for (int k = 0; k < ninds; ++k) {
+    const float2 b = b10[(long long)inds[k] * HW + p];
+    const float2 cr = crec0[(long long)inds[k] * HW + p];
+    lw = cadd(lw, cmulc(b, cr));
+    sb = cadd(sb, cmulc(b, b));
+  }
+  Lw[p] = lw;
+  // Ib = 1 / (1 + tau sumB1) (complex division of 1 by a real-valued complex)
+  const float2 den = make_float2(1.f + tau * sb.x, tau * sb.y);
+  const float dd = cabs2(den);
+  Ib[p] = make_float2(den.x / dd, -den.y / dd);
+}
+
+__global__ void utgv_dual_kernel(CoilPD a) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= a.W * a.H) return;
+  const P2 p = p2_of(idx, a.W, a.H);
+  float2 g[2], e[3], y1[2], y2[3];
+  grad2(a.ext1, p, g);
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const float2 d = csub(g[k], ldc(a.ext2[k], p.i));
+    const float2 v = a.y1[k][p.i];
+    y1[k] = make_float2(v.x + a.sigma * d.x, v.y + a.sigma * d.y);
+  }
+  symgrad2(a.ext2[0], a.ext2[1], p, e);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float2 v = a.y2[k][p.i];
+    y2[k] = make_float2(v.x + a.sigma * e[k].x, v.y + a.sigma * e[k].y);
+  }
+  const float n1 = sqrtf(cabs2(y1[0]) + cabs2(y1[1]));
+  const float n2 = sqrtf(cabs2(y2[0]) + cabs2(y2[1]) + 2.f * cabs2(y2[2]));
+  const float d1 = fmaxf(1.f, a.s1 * n1), d2 = fmaxf(1.f, a.s2 * n2);
+#pragma unroll
+  for (int k = 0; k < 2; ++k) a.y1[k][p.i] = make_float2(y1[k].x / d1, y1[k].y / d1);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) a.y2[k][p.i] = make_float2(y2[k].x / d2, y2[k].y / d2);
+}
+
+__global__ void utgv_primal_kernel(CoilPD a) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= a.W * a.H) return;
+  const P2 p = p2_of(idx, a.W, a.H);
+  const float2 dv = div2(a.y1[0], a.y1[1], p);
+  const float2 xo = a.x1[p.i];
+  float2 n1 = make_float2(xo.x + a.tau * dv.x, xo.y + a.tau * dv.y);
+  const float2 lw = a.Lw[p.i];
+  n1 = make_float2(n1.x + a.tau * lw.x, n1.y + a.tau * lw.y);
+  n1 = cmul(n1, a.Ib[p.i]);
+  a.x1n[p.i] = n1;
+  a.ext1n[p.i] = make_float2(2.f * n1.x - xo.x, 2.f * n1.y - xo.y);
+  float2 sd[2];
+  symdiv2(a.y2[0], a.y2[1], a.y2[2], p, sd);
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const float2 r = cadd(ldc(a.y1[k], p.i), sd[k]);
+    const float2 x2 = a.x2[k][p.i];
+    const float2 n2 = make_float2(x2.x + a.tau * r.x, x2.y + a.tau * r.y);
+    a.x2[k][p.i] = n2;
+    a.ext2n[k][p.i] = make_float2(2.f * n2.x - x2.x, 2.f * n2.y - x2.y);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// B1Recon (coil_construction.cpp:217-361)
+// ---------------------------------------------------------------------------
+
+__global__ void absmax_kernel(const float2* v, int n, unsigned* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float m = 0.f;
+  if (i < n) m = sqrtf(cabs2(v[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+  // non-negative floats order like their bit patterns
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+__global__ void b1r_prep_kernel(const float2* u0, const unsigned* umax, const float2* crec, int coils, int HW,
+                                float tau, float2* Lw, float2* Iu) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= HW) return;
+  const float mx = __uint_as_float(*umax);
+  const float2 un = make_float2(u0[p].x / mx, u0[p].y / mx);
+  const float2 sumU = make_float2(1.f + tau * cabs2(un), 0.f);
+  const float2 iu = make_float2(1.f / sumU.x, 0.f);
+  for (int c = 0; c < coils; ++c) {
+    Lw[(long long)c * HW + p] = cmulc(un, crec[(long long)c * HW + p]);
+    Iu[(long long)c * HW + p] = iu;
+  }
+}
+
+__global__ void b1r_dual_kernel(CoilPD a, int coils) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int HW = a.W * a.H;
+  if (idx >= (long long)coils * HW) return;
+  const int c = (int)(idx / HW);
+  const P2 p = p2_of((int)(idx % HW), a.W, a.H);
+  const float2* e = a.ext1 + (long long)c * HW;
+  float2 g[2];
+  grad2(e, p, g);
+  const float sc = 1.f / (1.f + a.sigma / a.mu);
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const float2 v = a.y1[k][idx];
+    a.y1[k][idx] = cscale(make_float2(v.x + a.sigma * g[k].x, v.y + a.sigma * g[k].y), sc);
+  }
+}
+
+__global__ void b1r_primal_kernel(CoilPD a, int coils) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int HW = a.W * a.H;
+  if (idx >= (long long)coils * HW) return;
+  const int c = (int)(idx / HW);
+  const P2 p = p2_of((int)(idx % HW), a.W, a.H);
+  const float2 dv = div2(a.y1[0] + (long long)c * HW, a.y1[1] + (long long)c * HW, p);
+  const float2 xo = a.x1[idx];
+  float2 n1 = make_float2(xo.x + a.tau * dv.x, xo.y + a.tau * dv.y);
+  const float2 lw = a.Lw[idx];
+  n1 = cmul(make_float2(n1.x + a.tau * lw.x, n1.y + a.tau * lw.y), a.Ib[idx]);
+  a.x1n[idx] = n1;
+  a.ext1n[idx] = make_float2(2.f * n1.x - xo.x, 2.f * n1.y - xo.y);
+}
+
+__global__ void b1r_normalize_kernel(const float2* x, float2* out, int HW, int coils) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= HW) return;
+  float s = 0.f;
+  for (int c = 0; c < coils; ++c) s += cabs2(x[(long long)c * HW + p]);
+  const float n = sqrtf(s);
+  for (int c = 0; c < coils; ++c) {
+    const float2 v = x[(long long)c * HW + p];
+    out[(long long)c * HW + p] = make_float2(v.x / n, v.y / n);
+  }
+}
+
+// b1 = |absb1| * exp(i angle(x1))
+__global__ void phase_apply_kernel(const float2* absb1, const float2* x1, float2* out, int HW) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= HW) return;
+  const float ang = atan2f(x1[p].y, x1[p].x);
+  out[p] = cmul(absb1[p], make_float2(cosf(ang), sinf(ang)));
+}
+
+// w = sqrt(w*w + conj(b) b); crec_abs products and sums for the greedy order
+__global__ void weight_update_kernel(float2* w, const float2* b, int HW) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= HW) return;
+  const float2 ww = cmul(w[p], w[p]);
+  const float2 s = cadd(ww, cmulc(b[p], b[p]));
+  // complex square root of a value with zero imaginary part here
+  const float r = sqrtf(sqrtf(cabs2(s)));
+  const float th = 0.5f * atan2f(s.y, s.x);
+  w[p] = make_float2(r * cosf(th), r * sinf(th));
+}
+
+// u_in = absb1 * u * w; crec_in = crec * w
+__global__ void greedy_inputs_kernel(const float2* absb1, const float2* u, const float2* w, const float2* crec,
+                                     float2* u_in, float2* crec_in, int HW) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= HW) return;
+  u_in[p] = cmul(cmul(absb1[p], u[p]), w[p]);
+  crec_in[p] = cmul(crec[p], w[p]);
+}
+
+// FP64 sums over a coil image of |a| (b == null) or |a| |b|
+__global__ void abs_sum_kernel(const float2* a, const float2* b, int HW, double* partial) {
+  __shared__ double red[32];
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < HW; i += gridDim.x * blockDim.x) {
+    float v = sqrtf(cabs2(a[i]));
+    if (b) v *= sqrtf(cabs2(b[i]));
+    acc[0] += (double)v;
+  }
+  block_sum<1>(acc, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = acc[0];
+}
+
+static inline unsigned nb256(long long n) { return (unsigned)((n + 255) / 256); }
+
+void launch_ta_sum(const float2* kdata, const float* mask, float2* out, int HW, int C, int T, cudaStream_t s) {
+  ta_sum_kernel<<<nb256((long long)C * HW), 256, 0, s>>>(kdata, mask, out, HW, C, T);
+}
+void launch_ta_combine(float2* crec, float2* u, int HW, int C, float scale, int apply_phase, cudaStream_t s) {
+  ta_combine_kernel<<<nb256(HW), 256, 0, s>>>(crec, u, HW, C, scale, apply_phase);
+}
+void launch_h1_cg(const float2* u, const float2* crec, double mu, int W, int H, int C, int max_it, double rel_tol,
+                  double2* work, double* muu, float2* out, int* iters, cudaStream_t s) {
+  h1_cg_kernel<<<C, 1024, 0, s>>>(u, crec, mu, W, H, max_it, rel_tol, work, muu, out, iters);
+}
+void launch_h1_normalize(float2* b1, int HW, int C, cudaStream_t s) {
+  h1_normalize_kernel<<<nb256(HW), 256, 0, s>>>(b1, HW, C);
+}
+void launch_utgv_prep(const float2* b10, const float2* crec0, const int* inds, int ninds, float tau, int HW,
+                      float2* Lw, float2* Ib, cudaStream_t s) {
+  utgv_prep_kernel<<<nb256(HW), 256, 0, s>>>(b10, crec0, inds, ninds, tau, HW, Lw, Ib);
+}
+void launch_utgv_iter(const CoilPD& a, cudaStream_t s) {
+  utgv_dual_kernel<<<nb256((long long)a.W * a.H), 256, 0, s>>>(a);
+  utgv_primal_kernel<<<nb256((long long)a.W * a.H), 256, 0, s>>>(a);
+}
+void launch_absmax(const float2* v, int n, unsigned* out, cudaStream_t s) {
+  absmax_kernel<<<nb256(n), 256, 0, s>>>(v, n, out);
+}
+void launch_b1r_prep(const float2* u0, const unsigned* umax, const float2* crec, int coils, int HW, float tau,
+                     float2* Lw, float2* Iu, cudaStream_t s) {
+  b1r_prep_kernel<<<nb256(HW), 256, 0, s>>>(u0, umax, crec, coils, HW, tau, Lw, Iu);
+}
+void launch_b1r_iter(const CoilPD& a, int coils, cudaStream_t s) {
+  const long long n = (long long)coils * a.W * a.H;
+  b1r_dual_kernel<<<nb256(n), 256, 0, s>>>(a, coils);
+  b1r_primal_kernel<<<nb256(n), 256, 0, s>>>(a, coils);
+}
+void launch_b1r_normalize(const float2* x, float2* out, int HW, int coils, cudaStream_t s) {
+  b1r_normalize_kernel<<<nb256(HW), 256, 0, s>>>(x, out, HW, coils);
+}
+void launch_phase_apply(const float2* absb1, const float2* x1, float2* out, int HW, cudaStream_t s) {
+  phase_apply_kernel<<<nb256(HW), 256, 0, s>>>(absb1, x1, out, HW);
+}
+void launch_weight_update(float2* w, const float2* b, int HW, cudaStream_t s) {
+  weight_update_kernel<<<nb256(HW), 256, 0, s>>>(w, b, HW);
+}
+void launch_greedy_inputs(const float2* absb1, const float2* u, const float2* w, const float2* crec, float2* u_in,
+                          float2* crec_in, int HW, cudaStream_t s) {
+  greedy_inputs_kernel<<<nb256(HW), 256, 0, s>>>(absb1, u, w, crec, u_in, crec_in, HW);
+}
+void launch_abs_sum(const float2* a, const float2* b, int HW, double* partial, int nblocks, cudaStream_t s) {
+  abs_sum_kernel<<<nblocks, 256, 0, s>>>(a, b, HW, partial);
+}
+
+}  // namespace avx

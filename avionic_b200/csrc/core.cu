@@ -478,7 +478,7 @@ struct avx_solver {
 static avx_status solver_alloc(avx_solver* s) {
   const int P = method_P(s->method), D = method_D(s->method);
   const size_t N = (size_t)s->N();
-  const size_t K = (size_t)s->C * std::max(s->op->R, 1) * s->W;
+  const size_t K = s->op->kind == 1 ? (size_t)s->C * s->T * s->op->S : (size_t)s->C * std::max(s->op->R, 1) * s->W;
   AVX_CK(s->prim.alloc(P * N));
   AVX_CK(s->ext.alloc(P * N));
   AVX_CK(s->dual.alloc(D * N));
@@ -487,7 +487,8 @@ static avx_status solver_alloc(avx_solver* s) {
   AVX_CK(s->d.alloc(K));
   AVX_CK(s->st.alloc(1));
   AVX_CK(s->pimg.alloc((size_t)8 * std::max(AVX_RED_BLOCKS, avx::gap_img_blocks(s->W, s->H, s->T))));
-  AVX_CK(s->pk.alloc((size_t)3 * s->C * s->T));
+  const int nk = s->op->kind == 1 ? avx::radial_interp_blocks(s->op->rg) : s->C * s->T;
+  AVX_CK(s->pk.alloc((size_t)3 * std::max(nk, 1)));
   s->cap = (int)s->p.maxIt + 2;
   AVX_CK(s->hist.alloc((size_t)3 * (s->cap + 1)));
   if (!s->stream) AVX_CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
@@ -570,9 +571,69 @@ static bool gap_due(const avx_solver* s, unsigned k) {
          (s->p.stopPDGap > 0 && k % 20 == 0);
 }
 
-static unsigned shape_launches(int shape) { return 3u + ((shape & 1) ? 4u : 0u) + ((shape & 2) ? 3u : 0u); }
+static unsigned shape_launches(int kind, int shape) {
+  if (kind == 1) return 10u + ((shape & 1) ? 7u : 0u) + ((shape & 2) ? 10u : 0u);
+  return 3u + ((shape & 1) ? 4u : 0u) + ((shape & 2) ? 3u : 0u);
+}
+
+static RArgs solver_rargs(avx_solver* s, const float2* b1, const float2* in, const float2* in2) {
+  RArgs r = make_rargs(s->op, b1, in, in2);
+  r.z = s->z.p;
+  r.d = s->d.p;
+  r.lam = s->p.lambda;
+  r.st = s->st.p;
+  r.partial = s->pk.p;
+  return r;
+}
+
+// radial operator pass: K u (mode 0 z prox, 1 norm, 2 gap sums) and, for modes
+// 0 and 2, K^H z into the operator's K^H z image
+static void radial_pass(avx_solver* s, int mode, const float2* b1, const float2* in, const float2* in2) {
+  RArgs r = solver_rargs(s, b1, in, in2);
+  avx::launch_rad_pad(r, s->stream);
+  avx::launch_rad_fft(r, -1, s->stream);
+  avx::launch_rad_interp(r, mode, s->stream);
+  if (mode == 1) return;
+  avx::launch_rad_spread(r, s->z.p, s->stream);
+  avx::launch_rad_fft(r, +1, s->stream);
+  avx::launch_rad_crop(r, s->op->r_khz.p, s->stream);
+}
+
+static void enqueue_shape_radial(avx_solver* s, int shape, const float2* b1, cudaEvent_t* ev) {
+  PDArgs a = make_pdargs(s);
+  a.khz = s->op->r_khz.p;
+  const KArgs kdummy = make_kargs(s, b1, s->extc(0), nullptr);
+  if (ev) cudaEventRecord(ev[0], s->stream);
+  avx::launch_dual(s->method, a, s->stream);
+  if (ev) cudaEventRecord(ev[1], s->stream);
+  radial_pass(s, 0, b1, s->extc(0), nullptr);
+  if (ev) cudaEventRecord(ev[2], s->stream);
+  avx::launch_primal(s->method, a, kdummy, s->stream, false);
+  if (ev) cudaEventRecord(ev[3], s->stream);
+  const int nk = avx::radial_interp_blocks(s->op->rg);
+  if (shape & 1) {
+    avx::Ptr8 e;
+    const int P = method_P(s->method);
+    for (int c = 0; c < 8; ++c) e.p[c] = c < P ? s->escrc(c) : nullptr;
+    avx::launch_step_img(s->method, a, e, P, s->pimg.p, s->stream);
+    radial_pass(s, 1, b1, s->escrc(0), nullptr);
+    avx::launch_step_finalize(a, s->pimg.p, s->pk.p, nk, s->p.sigmaTauRatio, s->stream);
+  }
+  if (shape & 2) {
+    radial_pass(s, 2, b1, s->primc(0), nullptr);
+    double* h = s->hist.p;
+    const bool ic = s->method == AVX_METHOD_ICTGV2;
+    avx::launch_gap_tail(s->method, a, kdummy, s->pimg.p, s->pk.p, nk, make_gapconst(s), h,
+                         ic ? h + (s->cap + 1) : nullptr, ic ? h + 2 * (s->cap + 1) : nullptr, s->cap, 0, false,
+                         s->stream);
+  }
+}
 
 static void enqueue_shape(avx_solver* s, int shape, const float2* b1, cudaEvent_t* ev = nullptr) {
+  if (s->op->kind == 1) {
+    enqueue_shape_radial(s, shape, b1, ev);
+    return;
+  }
   const PDArgs a = make_pdargs(s);
   const KArgs ks = make_kargs(s, b1, s->extc(0), nullptr);
   if (ev) {
@@ -616,7 +677,10 @@ static avx_status prepare_run(avx_solver* s, const float2* data, const float2* x
     AVX_CK(cudaMemcpyAsync(s->primc(0), x0, N * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
     AVX_CK(cudaMemcpyAsync(s->extc(0), x0, N * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
   }
-  if (data && s->op->R) {
+  if (data && s->op->kind == 1) {
+    AVX_CK(cudaMemcpyAsync(s->d.p, data, s->d.n * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
+    s->d_off_energy = 0.0;
+  } else if (data && s->op->R) {
     avx::launch_gather_rows(s->op->geom(), data, s->d.p, 0, s->stream);
     AVX_CK(cudaGetLastError());
     // energy of the data rows the operator never samples enters g1 as a constant
@@ -658,11 +722,18 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
   r = prepare_run(s, data, x);
   if (r != AVX_OK) return r;
   if (s->method == AVX_METHOD_ICTGV2 && s->debug) {
-    const PDArgs a = make_pdargs(s);
+    PDArgs a = make_pdargs(s);
     const KArgs kx = make_kargs(s, b1, s->primc(0), nullptr);
     double* h = s->hist.p;
-    avx::launch_gap(s->method, a, kx, s->pimg.p, s->pk.p, make_gapconst(s), h, h + (s->cap + 1), h + 2 * (s->cap + 1),
-                    s->cap, 1, s->stream);
+    if (s->op->kind == 1) {
+      a.khz = s->op->r_khz.p;
+      radial_pass(s, 2, b1, s->primc(0), nullptr);
+      avx::launch_gap_tail(s->method, a, kx, s->pimg.p, s->pk.p, avx::radial_interp_blocks(s->op->rg),
+                           make_gapconst(s), h, h + (s->cap + 1), h + 2 * (s->cap + 1), s->cap, 1, false, s->stream);
+    } else {
+      avx::launch_gap(s->method, a, kx, s->pimg.p, s->pk.p, make_gapconst(s), h, h + (s->cap + 1),
+                      h + 2 * (s->cap + 1), s->cap, 1, s->stream);
+    }
     AVX_CK(cudaGetLastError());
   }
   // graphs depend on every pointer and scalar baked into the launches
@@ -685,7 +756,7 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
   unsigned k = 0;
   for (; k < s->p.maxIt; ++k) {
     const int shape = (step_due(k) ? 1 : 0) | (gap_due(s, k) ? 2 : 0);
-    launches += shape_launches(shape);
+    launches += shape_launches(s->op->kind, shape);
     if (s->timing) {
       enqueue_shape(s, shape, b1, &s->events[(size_t)4 * k]);
       AVX_CK(cudaGetLastError());
@@ -780,8 +851,63 @@ avx_status avx_cartesian_operator_create(unsigned width, unsigned height, unsign
   return AVX_OK;
 }
 
+avx_status avx_radial_operator_create(unsigned width, unsigned height, unsigned coils, unsigned frames,
+                                      unsigned nSpokes, unsigned nFE, unsigned spokesPerFrame, const float* d_traj,
+                                      const float* d_dens, float kernelWidth, float sectorWidth, float osf,
+                                      avx_operator** out) {
+  if (!out || !d_traj || !d_dens) return fail(AVX_E_ARG, "null argument");
+  if (!width || !height || !coils || !frames || !nFE || !spokesPerFrame)
+    return fail(AVX_E_ARG, "dimensions must be positive");
+  if (nSpokes != spokesPerFrame * frames) return fail(AVX_E_ARG, "nSpokes must equal spokesPerFrame * frames");
+  avx_status r = configure_once();
+  if (r != AVX_OK) return r;
+  const size_t S = (size_t)nFE * spokesPerFrame;
+  std::vector<float> ht((size_t)frames * 2 * S), hd((size_t)frames * S);
+  AVX_CK(cudaMemcpy(ht.data(), d_traj, ht.size() * sizeof(float), cudaMemcpyDeviceToHost));
+  AVX_CK(cudaMemcpy(hd.data(), d_dens, hd.size() * sizeof(float), cudaMemcpyDeviceToHost));
+  for (float v : hd)
+    if (!(v >= 0.f)) return fail(AVX_E_ARG, "density compensation must be non-negative");
+  avx_operator* op = new avx_operator();
+  op->kind = 1;
+  op->W = (int)width; op->H = (int)height; op->C = (int)coils; op->T = (int)frames;
+  op->S = (int)S;
+  op->spf = (int)spokesPerFrame;
+  r = build_radial(op, ht.data(), hd.data(), kernelWidth, sectorWidth, osf);
+  if (r != AVX_OK) {
+    delete op;
+    return r;
+  }
+  *out = op;
+  return AVX_OK;
+}
+
+avx_status avx_radial_sector_map(const avx_operator* op, int* h_order, int* h_start, int* grid_xy) {
+  if (!op || op->kind != 1) return fail(AVX_E_ARG, "not a radial operator");
+  const RadialGeomDev& g = op->rg;
+  if (grid_xy) {
+    grid_xy[0] = g.Gx;
+    grid_xy[1] = g.Gy;
+  }
+  if (h_order)
+    AVX_CK(cudaMemcpy(h_order, op->r_order.p, (size_t)g.T * g.S * sizeof(int), cudaMemcpyDeviceToHost));
+  if (h_start)
+    AVX_CK(cudaMemcpy(h_start, op->r_secstart.p, (size_t)g.T * (g.nsx * g.nsy + 1) * sizeof(int),
+                      cudaMemcpyDeviceToHost));
+  return AVX_OK;
+}
+
 avx_status avx_operator_backward(avx_operator* op, const avx_cf32* d_x, avx_cf32* d_k, const avx_cf32* d_b1) {
   if (!op || !d_x || !d_k || !d_b1) return fail(AVX_E_ARG, "null argument");
+  if (op->kind == 1) {
+    RArgs ra = make_rargs(op, reinterpret_cast<const float2*>(d_b1), reinterpret_cast<const float2*>(d_x), nullptr);
+    ra.out = reinterpret_cast<float2*>(d_k);
+    avx::launch_rad_pad(ra, 0);
+    avx::launch_rad_fft(ra, -1, 0);
+    avx::launch_rad_interp(ra, 3, 0);
+    AVX_CK(cudaGetLastError());
+    AVX_CK(cudaDeviceSynchronize());
+    return AVX_OK;
+  }
   const size_t K = (size_t)op->W * op->H * op->C * op->T;
   AVX_CK(cudaMemset(d_k, 0, K * sizeof(float2)));
   KArgs k;
@@ -798,6 +924,15 @@ avx_status avx_operator_backward(avx_operator* op, const avx_cf32* d_x, avx_cf32
 
 avx_status avx_operator_forward(avx_operator* op, avx_cf32* d_k, avx_cf32* d_x, const avx_cf32* d_b1) {
   if (!op || !d_x || !d_k || !d_b1) return fail(AVX_E_ARG, "null argument");
+  if (op->kind == 1) {
+    RArgs ra = make_rargs(op, reinterpret_cast<const float2*>(d_b1), nullptr, nullptr);
+    avx::launch_rad_spread(ra, reinterpret_cast<const float2*>(d_k), 0);
+    avx::launch_rad_fft(ra, +1, 0);
+    avx::launch_rad_crop(ra, reinterpret_cast<float2*>(d_x), 0);
+    AVX_CK(cudaGetLastError());
+    AVX_CK(cudaDeviceSynchronize());
+    return AVX_OK;
+  }
   KArgs k;
   memset(&k, 0, sizeof(k));
   k.g = op->geom();
@@ -812,6 +947,12 @@ avx_status avx_operator_forward(avx_operator* op, avx_cf32* d_k, avx_cf32* d_x, 
 
 avx_status avx_operator_adapt_lambda(const avx_operator* op, float k, float d, float* lambda_out) {
   if (!op || !lambda_out) return fail(AVX_E_ARG, "null argument");
+  if (op->kind == 1) {
+    // NoncartesianOperator::AdaptLambda (noncartesian_operator.cpp:88-95)
+    const double subfac = op->W / (op->spf * M_PI / 2.0);
+    *lambda_out = (float)(subfac * k + d);
+    return AVX_OK;
+  }
   double subfac = (double)op->W * op->H * op->T;
   if (op->has_mask)
     subfac /= op->mask_norm2;
@@ -920,8 +1061,16 @@ avx_status avx_solver_adapt_step_size(avx_solver* s, const avx_cf32* const* d_di
   const PDArgs a = make_pdargs(s);
   avx::Ptr8 e;
   for (int c = 0; c < 8; ++c) e.p[c] = c < P ? s->escrc(c) : nullptr;
-  const KArgs ke = make_kargs(s, reinterpret_cast<const float2*>(d_b1), s->escrc(0), nullptr);
-  avx::launch_step(s->method, a, ke, e, P, s->pimg.p, s->pk.p, s->p.sigmaTauRatio, s->stream);
+  const float2* b1 = reinterpret_cast<const float2*>(d_b1);
+  if (s->op->kind == 1) {
+    avx::launch_step_img(s->method, a, e, P, s->pimg.p, s->stream);
+    radial_pass(s, 1, b1, s->escrc(0), nullptr);
+    avx::launch_step_finalize(a, s->pimg.p, s->pk.p, avx::radial_interp_blocks(s->op->rg), s->p.sigmaTauRatio,
+                              s->stream);
+  } else {
+    const KArgs ke = make_kargs(s, b1, s->escrc(0), nullptr);
+    avx::launch_step(s->method, a, ke, e, P, s->pimg.p, s->pk.p, s->p.sigmaTauRatio, s->stream);
+  }
   AVX_CK(cudaGetLastError());
   DevState h;
   AVX_CK(cudaMemcpyAsync(&h, s->st.p, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
@@ -945,16 +1094,28 @@ avx_status avx_solver_compute_gap(avx_solver* s, const avx_cf32* const* d_x, con
     AVX_CK(cudaMemcpyAsync(s->primc(c), d_x[c], N * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
   for (int c = 0; c < D; ++c)
     AVX_CK(cudaMemcpyAsync(s->dualc(c), d_y[c], N * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
-  if (s->op->R) avx::launch_gather_rows(s->op->geom(), reinterpret_cast<const float2*>(d_z), s->z.p, 0, s->stream);
+  if (s->op->kind == 1)
+    AVX_CK(cudaMemcpyAsync(s->z.p, d_z, s->z.n * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));
+  else if (s->op->R)
+    avx::launch_gather_rows(s->op->geom(), reinterpret_cast<const float2*>(d_z), s->z.p, 0, s->stream);
   PDArgs a = make_pdargs(s);
   const KArgs kx = make_kargs(s, reinterpret_cast<const float2*>(d_b1), s->primc(0), nullptr);
   avx::GapConst gc = make_gapconst(s);
   gc.stop_gap = -1.0;
   double* h = s->hist.p;
-  avx::launch_gap(s->method, a, kx, s->pimg.p, s->pk.p, gc, h, h + (s->cap + 1), h + 2 * (s->cap + 1), s->cap, 0,
-                  s->stream);
+  int nk = s->C * s->T;
+  if (s->op->kind == 1) {
+    a.khz = s->op->r_khz.p;
+    nk = avx::radial_interp_blocks(s->op->rg);
+    radial_pass(s, 2, reinterpret_cast<const float2*>(d_b1), s->primc(0), nullptr);
+    avx::launch_gap_tail(s->method, a, kx, s->pimg.p, s->pk.p, nk, gc, h, h + (s->cap + 1), h + 2 * (s->cap + 1),
+                         s->cap, 0, false, s->stream);
+  } else {
+    avx::launch_gap(s->method, a, kx, s->pimg.p, s->pk.p, gc, h, h + (s->cap + 1), h + 2 * (s->cap + 1), s->cap, 0,
+                    s->stream);
+  }
   AVX_CK(cudaGetLastError());
-  const int nk = s->C * s->T, nimg = avx::gap_img_blocks(s->W, s->H, s->T);
+  const int nimg = avx::gap_img_blocks(s->W, s->H, s->T);
   std::vector<double> pk(3 * nk), pi(8 * nimg);
   AVX_CK(cudaMemcpyAsync(pk.data(), s->pk.p, pk.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
   AVX_CK(cudaMemcpyAsync(pi.data(), s->pimg.p, pi.size() * sizeof(double), cudaMemcpyDeviceToHost, s->stream));

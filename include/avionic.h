@@ -109,6 +109,27 @@ const char* avx_last_error(void);
 avx_status avx_cartesian_operator_create(unsigned width, unsigned height, unsigned coils, unsigned frames,
                                          const float* d_mask, int centered, avx_operator** op);
 
+/* NoncartesianOperator(width, height, coils, frames, nSpokes, nFE,
+ * spokesPerFrame, kTraj, dens, kernelWidth, sectorWidth, osf)
+ * (CUDA/src/noncartesian_operator.cpp:3-86): the radial gridding operator.
+ * d_traj holds per frame [kx(S) | ky(S)] in cycles/pixel, [-0.5, 0.5)
+ * (S = nFE * spokesPerFrame); d_dens the density compensation w per frame
+ * and sample.  K x = sqrt(w) NUFFT(b1 x) / sqrt(W H) with a tapered
+ * Kaiser-Bessel gridding of width kernelWidth on a grid oversampled by osf,
+ * sector-sorted by sectorWidth; k-space layout [frame][coil][sample]
+ * (noncartesian_operator.cpp:117-121).  The operator uses the coil maps of each
+ * call (the reference bakes them into its gpuNUFFT operators). */
+avx_status avx_radial_operator_create(unsigned width, unsigned height, unsigned coils, unsigned frames,
+                                      unsigned nSpokes, unsigned nFE, unsigned spokesPerFrame, const float* d_traj,
+                                      const float* d_dens, float kernelWidth, float sectorWidth, float osf,
+                                      avx_operator** op);
+
+/* Sector layout of a radial operator, for inspection: h_order [T*S] sample
+ * indices sorted by sector (stable), h_start [T*(nsectors+1)] offsets, grid_xy
+ * the oversampled grid size (Gx, Gy).  Any output may be NULL.  (No reference
+ * counterpart: gpuNUFFT keeps its sector map internal.) */
+avx_status avx_radial_sector_map(const avx_operator* op, int* h_order, int* h_start, int* grid_xy);
+
 /* BackwardOperation(img -> k-space) (cartesian_operator.cpp:122-160):
  * d_k[t,c] = mask[t] * F(b1[c] * x[t]); d_k is dense (W*H*C*T). */
 avx_status avx_operator_backward(avx_operator* op, const avx_cf32* d_x, avx_cf32* d_k, const avx_cf32* d_b1);

@@ -33,8 +33,19 @@ Data layout follows the reference: trajectory per frame [kx(S) | ky(S)]
 import numpy as np
 
 
+def _smooth13(n):
+    for p in (2, 3, 5, 7, 11, 13):
+        while n % p == 0:
+            n //= p
+    return n == 1
+
+
 def grid_size(d, osf):
-    return int(2 * np.ceil(osf * d / 2.0))
+    """Smallest even size >= osf d whose prime factors are <= 13."""
+    n = int(2 * np.ceil(osf * d / 2.0))
+    while not _smooth13(n):
+        n += 2
+    return n
 
 
 def kb_beta(J, osf):
@@ -60,25 +71,27 @@ def deapodization(d, G, J, beta, nodes=64):
 
 
 def sector_map(traj, G, sector_width):
-    """Sector of every sample (float32 arithmetic, as the device computes it):
-    g = (k + 0.5) * G, sector = min(floor(g / sw), nsec - 1) per axis; returns
-    (sector index per sample [T, S], order [T, S]: samples sorted by sector,
-    stable), with sector index = sy * nsx + sx."""
+    """Sector layout of the samples, in float32 arithmetic as the device
+    library computes it: grid position g = k G (float32), wrapped into [0, G)
+    by adding G when negative; sector = clamp(floor(g / sw), 0, nsec - 1) per
+    axis; sector index sy * nsx + sx.  Returns (order [T, S]: sample indices
+    sorted by sector, stable; start [T, nsx*nsy + 1]: offsets into order)."""
     Gy, Gx = G
     sw = np.float32(sector_width)
     nsx = int(np.ceil(Gx / sector_width))
     nsy = int(np.ceil(Gy / sector_width))
-    kx = traj[:, 0, :].astype(np.float32)
-    ky = traj[:, 1, :].astype(np.float32)
-    gx = (kx + np.float32(0.5)) * np.float32(Gx)
-    gy = (ky + np.float32(0.5)) * np.float32(Gy)
-    sx = np.minimum(np.floor(gx / sw).astype(np.int64), nsx - 1)
-    sy = np.minimum(np.floor(gy / sw).astype(np.int64), nsy - 1)
-    sx = np.maximum(sx, 0)
-    sy = np.maximum(sy, 0)
+    gx = traj[:, 0, :].astype(np.float32) * np.float32(Gx)
+    gy = traj[:, 1, :].astype(np.float32) * np.float32(Gy)
+    gx = np.where(gx < 0, gx + np.float32(Gx), gx).astype(np.float32)
+    gy = np.where(gy < 0, gy + np.float32(Gy), gy).astype(np.float32)
+    sx = np.clip(np.floor(gx / sw).astype(np.int64), 0, nsx - 1)
+    sy = np.clip(np.floor(gy / sw).astype(np.int64), 0, nsy - 1)
     sec = sy * nsx + sx
     order = np.argsort(sec, axis=1, kind="stable")
-    return sec, order
+    start = np.zeros((traj.shape[0], nsx * nsy + 1), dtype=np.int64)
+    for f in range(traj.shape[0]):
+        start[f, 1:] = np.cumsum(np.bincount(sec[f], minlength=nsx * nsy))
+    return order, start
 
 
 class RadialOperator:

@@ -434,3 +434,53 @@ def test_stencil_adjointness():
     sd = st.sym_divergence(q, *w)
     rhs = -sum(np.vdot(v[i], sd[i]) for i in range(3))
     assert abs(lhs - rhs) < 1e-9 * abs(lhs)
+
+
+# ---------------------------------------------------------------------------
+# coil_construction.cc
+# ---------------------------------------------------------------------------
+
+def _coil_fixture(k):
+    W, H, T = k["dims"]
+    C = k["coils"]
+    kd = ki.kspace(W, H, C, T)
+    return kd, np.ones((T, H, W)), C
+
+
+def test_coil_construction_kats(kats):
+    from oracle import coils as co
+    k = kats["coil_construction"]
+    kd, mask, C = _coil_fixture(k)
+    p = co.default_params()
+    u, crec = co.time_averaged_reconstruction(kd, mask)
+    for (x, y), want in k["time_averaged_u_real"]:
+        assert abs(u[y, x].real - want) < EPS
+    for (x, y, c), want in k["time_averaged_crec_real"]:
+        assert abs(crec[c, y, x].real - want) < EPS
+    lap = co.laplace_periodic(np.arange(25.0).reshape(5, 5))
+    for (x, y), want in k["laplace_periodic"]:
+        assert abs(lap[y, x] - want) < EPS
+    ua = np.abs(u).astype(complex)
+    b1 = co.b1_from_u_h1(ua, crec, p)
+    for (x, y, c), want in k["h1_abs_b1"]:
+        assert abs(abs(b1[c, y, x]) - want) < EPS
+    mi = co.find_maximum_sum(crec)
+    assert mi == k["initial_index"]
+    uM = co.utgv2_recon(b1[mi][None], crec[mi][None], np.zeros((5, 5), complex), [0], p)
+    for (x, y), want in k["utgv2_u_real"]:
+        assert abs(uM[y, x].real - want) < EPS
+    x1 = co.b1_recon(b1[1] * uM, crec[1][None], 1, p["b1NrIt"], p["b1Reg"], p)[0]
+    bb = b1[1] * np.exp(1j * np.angle(x1))
+    for (x, y), want in k["b1recon_coil1_real"]:
+        assert abs(bb[y, x].real - want) < EPS
+
+
+def test_coil_construction_loop_kat(kats):
+    from oracle import coils as co
+    k = kats["coil_construction"]
+    kd, mask, C = _coil_fixture(k)
+    u, b1 = co.perform_coil_construction(kd, mask)
+    for (x, y, c), want in k["loop_b1_real"]:
+        assert abs(b1[c, y, x].real - want) < EPS
+    for (x, y, c), want in k["loop_u_real"]:
+        assert abs(u[c, y, x].real - want) < EPS
