@@ -342,3 +342,66 @@ def reconstruct_host(method, kdata, mask, b1, u0=None, params=None, debugstep=0)
         None if u is None else u.ctypes.data_as(ctypes.c_void_p), x.ctypes.data_as(ctypes.c_void_p),
         ctypes.byref(st)))
     return x, st
+
+
+# ---------------------------------------------------------------------------
+# coil-sensitivity estimation (CoilConstruction)
+# ---------------------------------------------------------------------------
+
+CoilParams = _abi.CoilParams
+
+
+def coil_default_params():
+    p = CoilParams()
+    check(lib.avx_coil_default_params(ctypes.byref(p)))
+    return p
+
+
+def coil_time_averaged(kdata, mask, apply_phase=True):
+    """kdata (T,C,H,W), mask (T,H,W) or None -> (u (H,W), crec (C,H,W))."""
+    torch = _torch()
+    T, C, H, W = kdata.shape
+    u = torch.empty((H, W), dtype=torch.complex64, device=kdata.device)
+    crec = torch.empty((C, H, W), dtype=torch.complex64, device=kdata.device)
+    check(lib.avx_coil_time_averaged(W, H, C, T, _cptr(kdata), None if mask is None else _cptr(mask), _cptr(u),
+                                     _cptr(crec), int(apply_phase)))
+    return u, crec
+
+
+def coil_b1_from_u_h1(u, crec, params=None):
+    torch = _torch()
+    C, H, W = crec.shape
+    out = torch.empty_like(crec)
+    p = params or coil_default_params()
+    check(lib.avx_coil_b1_from_u_h1(W, H, C, ctypes.byref(p), _cptr(u), _cptr(crec), _cptr(out)))
+    return out
+
+
+def coil_utgv2(b1, crec, inds, x1, params=None):
+    H, W = x1.shape
+    arr = (ctypes.c_int * len(inds))(*inds)
+    p = params or coil_default_params()
+    check(lib.avx_coil_utgv2(W, H, ctypes.byref(p), _cptr(b1), _cptr(crec), arr, len(inds), _cptr(x1)))
+    return x1
+
+
+def coil_b1_recon(u0, crec, coils, max_it=500, mu=2.0, params=None):
+    torch = _torch()
+    H, W = u0.shape
+    out = torch.empty((coils, H, W), dtype=torch.complex64, device=u0.device)
+    p = params or coil_default_params()
+    check(lib.avx_coil_b1_recon(W, H, coils, max_it, ctypes.c_float(mu), ctypes.byref(p), _cptr(u0), _cptr(crec),
+                                _cptr(out)))
+    return out
+
+
+def coil_construction(kdata, mask, params=None):
+    """PerformCoilConstruction: (u (C,H,W), b1 (C,H,W))."""
+    torch = _torch()
+    T, C, H, W = kdata.shape
+    u = torch.empty((C, H, W), dtype=torch.complex64, device=kdata.device)
+    b1 = torch.empty((C, H, W), dtype=torch.complex64, device=kdata.device)
+    pp = ctypes.byref(params) if params is not None else None
+    check(lib.avx_coil_construction(W, H, C, T, pp, _cptr(kdata), None if mask is None else _cptr(mask), _cptr(u),
+                                    _cptr(b1)))
+    return u, b1

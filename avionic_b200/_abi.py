@@ -26,6 +26,14 @@ class RunStats(C.Structure):
     ]
 
 
+class CoilParams(C.Structure):
+    _fields_ = [
+        ("uH1mu", F), ("uReg", F), ("uNrIt", U), ("uTau", F), ("uSigma", F), ("uSigmaTauRatio", F),
+        ("uAlpha0", F), ("uAlpha1", F), ("b1Reg", F), ("b1NrIt", U), ("b1Tau", F), ("b1Sigma", F),
+        ("b1SigmaTauRatio", F), ("b1FinalReg", F), ("b1FinalNrIt", U),
+    ]
+
+
 EXPORT_CB = C.CFUNCTYPE(None, C.c_char_p, C.c_char_p, VP, C.c_size_t, VP)
 
 # name -> (restype, argtypes)
@@ -69,6 +77,14 @@ SIGNATURES = {
     "avx_tv_norm_noalloc": (I, [VP, U, U, U, F, F, F, C.POINTER(D)]),
     "avx_ellipke": (F, [F]),
     "avx_time_space_weights": (I, [F, C.POINTER(F), C.POINTER(F)]),
+    "avx_coil_default_params": (I, [C.POINTER(CoilParams)]),
+    "avx_coil_time_averaged": (I, [U, U, U, U, VP, VP, VP, VP, I]),
+    "avx_coil_b1_from_u_h1": (I, [U, U, U, C.POINTER(CoilParams), VP, VP, VP]),
+    "avx_coil_utgv2": (I, [U, U, C.POINTER(CoilParams), VP, VP, VP, U, VP]),
+    "avx_coil_b1_recon": (I, [U, U, U, U, F, C.POINTER(CoilParams), VP, VP, VP]),
+    "avx_coil_construction": (I, [U, U, U, U, C.POINTER(CoilParams), VP, VP, VP, VP]),
+    "avx_coil_time_averaged_radial": (I, [U, U, U, U, U, VP, VP, VP, VP, VP, I]),
+    "avx_coil_construction_radial": (I, [U, U, U, U, U, C.POINTER(CoilParams), VP, VP, VP, VP, VP]),
     "avx_reconstruct_host": (I, [I, U, U, U, U, C.POINTER(PDParams), I, VP, VP, VP, VP, VP, C.POINTER(RunStats)]),
 }
 

@@ -1,4 +1,4 @@
-// avionic: command-line reconstruction of Cartesian 2D+t multi-coil data.
+// avionic: command-line reconstruction of Cartesian and radial 2D+t multi-coil data.
 //
 // Drop-in for the reference executable's Cartesian TV / TGV2 / ICTGV2 path
 // (CUDA/src/main.cpp:323-917): same flags, configuration keys, .bin inputs
@@ -57,39 +57,13 @@ void export_cb(const char* dir, const char* name, const avx_cf32* v, size_t n, v
     std::cout << "exported " << path << std::endl;
 }
 
-// Cartesian time-averaged coil-combined initial image:
-// u0 = sum_c conj(b1_c) F^-1( sum_t k_{t,c} / max(1, sum_t mask_t) )
-// (cartesian_coil_construction.cpp:23-86 forms the same average per coil).
-std::vector<cf> time_average_u0(const std::vector<cf>& k, const std::vector<float>& mask, const std::vector<cf>& b1,
-                                unsigned W, unsigned H, unsigned C, unsigned T) {
-  const size_t HW = (size_t)W * H;
-  std::vector<double> cnt(HW, 0.0);
-  for (unsigned t = 0; t < T; ++t)
-    for (size_t i = 0; i < HW; ++i) cnt[i] += mask[t * HW + i];
+// u0 = 0.5 sum_c conj(b1_c) crec_c from the time-averaged reconstruction
+// without phase (PerformInitalizationGivenB1, main.cpp:250-289)
+std::vector<cf> given_b1_u0(const std::vector<cf>& crec, const std::vector<cf>& b1, size_t HW, unsigned C) {
   std::vector<cf> u(HW, cf(0, 0));
-  std::vector<cd> avg(HW), tmp(HW);
-  for (unsigned c = 0; c < C; ++c) {
-    std::fill(avg.begin(), avg.end(), cd(0, 0));
-    for (unsigned t = 0; t < T; ++t)
-      for (size_t i = 0; i < HW; ++i) avg[i] += cd(k[((size_t)t * C + c) * HW + i]);
-    for (size_t i = 0; i < HW; ++i) avg[i] /= std::max(1.0, cnt[i]);
-    // unitary k-space -> image transform (e^{-2 pi i} kernel), separable DFT
-    for (unsigned y = 0; y < H; ++y)
-      for (unsigned x = 0; x < W; ++x) {
-        cd s(0, 0);
-        for (unsigned kx = 0; kx < W; ++kx)
-          s += avg[(size_t)y * W + kx] * std::polar(1.0, -2.0 * M_PI * ((double)kx * x / W));
-        tmp[(size_t)y * W + x] = s / std::sqrt((double)W);
-      }
-    for (unsigned x = 0; x < W; ++x)
-      for (unsigned y = 0; y < H; ++y) {
-        cd s(0, 0);
-        for (unsigned ky = 0; ky < H; ++ky)
-          s += tmp[(size_t)ky * W + x] * std::polar(1.0, -2.0 * M_PI * ((double)ky * y / H));
-        s /= std::sqrt((double)H);
-        u[(size_t)y * W + x] += cf(std::conj(cd(b1[c * HW + (size_t)y * W + x])) * s);
-      }
-  }
+  for (unsigned c = 0; c < C; ++c)
+    for (size_t i = 0; i < HW; ++i) u[i] += std::conj(b1[c * HW + i]) * crec[c * HW + i];
+  for (auto& v : u) v *= 0.5f;
   return u;
 }
 
@@ -123,19 +97,21 @@ int main(int argc, char** argv) {
   if (method < 0) return die("invalid method selected");
   if (method != AVX_METHOD_TV && method != AVX_METHOD_TGV2 && method != AVX_METHOD_ICTGV2)
     return die("method " + mname + " is not provided by this build (TV, TGV2, ICTGV2 are)");
-  if (o.nonuniform) return die("nonuniform (-n) data is not provided by this build");
   if (o.normalize) return die("data normalisation (-o) is not provided by this build");
   avx_pd_params p;
   if (!avcli::params_for_method(o, method, &p, err)) return die(err);
 
   const unsigned W = o.dims[0], H = o.dims[1], C = o.dims[6], T = o.dims[7];
-  const size_t HW = (size_t)W * H, N = HW * T, K = N * C;
+  const size_t HW = (size_t)W * H, N = HW * T;
   const std::string kfile = o.positional[0], mfile = o.positional[1], outfile = o.positional[2];
   const std::string outdir = avcli::parent_directory(outfile);
   if (o.gpu >= 0 && cudaSetDevice(o.gpu) != cudaSuccess) return die("cannot select GPU " + std::to_string(o.gpu));
 
   std::vector<cd> buf;
   bool cplx = false;
+  const unsigned nRO = o.dims[3], spf = o.dims[4];
+  const size_t S = (size_t)nRO * spf;                  // radial samples per frame
+  const size_t K = o.nonuniform ? S * C * T : N * C;   // k-space values
   if (avcli::file_extension(kfile) != ".bin") return die("k-space data must be a .bin vector file");
   if (!avcli::read_bin(kfile, buf, &cplx, &err)) return die(err);
   if (buf.size() != K) return die("k-space data holds " + std::to_string(buf.size()) + " values, dims require " +
@@ -144,41 +120,118 @@ int main(int argc, char** argv) {
   std::vector<cf> kdata(K);
   for (size_t i = 0; i < K; ++i) kdata[i] = cf(buf[i]);
   if (!avcli::read_bin(mfile, buf, &cplx, &err)) return die(err);
-  if (buf.size() != N) return die("mask holds " + std::to_string(buf.size()) + " values, dims require " + std::to_string(N));
-  std::cout << "Mask File " << mfile << " successfully loaded." << std::endl;
-  std::vector<float> mask(N);
-  for (size_t i = 0; i < N; ++i) mask[i] = (float)buf[i].real();
-  // zero the data outside the mask, per frame and coil (main.cpp:507-519)
-  for (unsigned t = 0; t < T; ++t)
-    for (unsigned c = 0; c < C; ++c)
-      for (size_t i = 0; i < HW; ++i) kdata[((size_t)t * C + c) * HW + i] *= mask[t * HW + i];
-
-  std::vector<cf> b1(HW * C, cf(1, 0)), u0(HW, cf(0, 0));
-  if (o.sens.empty()) return die("coil construction (no -s) is not provided by this build; pass -s b1.bin");
-  if (!avcli::read_bin(o.sens, buf, &cplx, &err)) return die(err);
-  if (buf.size() != HW * C) return die("coil sensitivities hold " + std::to_string(buf.size()) + " values");
-  for (size_t i = 0; i < HW * C; ++i) b1[i] = cf(buf[i]);
-  std::cout << "B1 File " << o.sens << " successfully loaded." << std::endl;
-  if (!o.u0.empty() && avcli::read_bin(o.u0, buf, &cplx, &err) && buf.size() == HW) {
-    for (size_t i = 0; i < HW; ++i) u0[i] = cf(buf[i]);
-    std::cout << " initial solution (u0) file " << o.u0 << " successfully loaded." << std::endl;
+  const size_t MN = o.nonuniform ? 2 * S * T : N;
+  if (buf.size() != MN)
+    return die(std::string(o.nonuniform ? "trajectory" : "mask") + " holds " + std::to_string(buf.size()) +
+               " values, dims require " + std::to_string(MN));
+  std::cout << (o.nonuniform ? "Trajectory" : "Mask") << " File " << mfile << " successfully loaded." << std::endl;
+  std::vector<float> mask(MN);
+  for (size_t i = 0; i < MN; ++i) mask[i] = (float)buf[i].real();
+  std::vector<float> dens;
+  if (o.nonuniform) {
+    if (o.dens.empty()) return die("Density compensation data could not be loaded!");
+    if (!avcli::read_bin(o.dens, buf, &cplx, &err)) return die(err);
+    if (buf.size() != S * T) return die("density compensation holds " + std::to_string(buf.size()) + " values");
+    dens.resize(S * T);
+    for (size_t i = 0; i < S * T; ++i) dens[i] = (float)buf[i].real();
+    // data *= sqrt(w) per frame and sample (main.cpp:546-570; the operator applies sqrt(w) itself)
+    for (unsigned t = 0; t < T; ++t)
+      for (unsigned c = 0; c < C; ++c)
+        for (size_t j = 0; j < S; ++j) kdata[((size_t)t * C + c) * S + j] *= std::sqrt(dens[(size_t)t * S + j]);
   } else {
-    std::cout << "no initial solution (u0) data provided! using the coil-combined time average" << std::endl;
-    u0 = time_average_u0(kdata, mask, b1, W, H, C, T);
+    // zero the data outside the mask, per frame and coil (main.cpp:507-519)
+    for (unsigned t = 0; t < T; ++t)
+      for (unsigned c = 0; c < C; ++c)
+        for (size_t i = 0; i < HW; ++i) kdata[((size_t)t * C + c) * HW + i] *= mask[t * HW + i];
   }
 
-  Dev dk, dm, db, dx;
-  if (cudaMalloc(&dk.p, K * sizeof(cf)) != cudaSuccess || cudaMalloc(&dm.p, N * sizeof(float)) != cudaSuccess ||
-      cudaMalloc(&db.p, HW * C * sizeof(cf)) != cudaSuccess || cudaMalloc(&dx.p, N * sizeof(cf)) != cudaSuccess)
+  Dev dk, dm, db, dx, dd, du, dc;
+  if (cudaMalloc(&dk.p, K * sizeof(cf)) != cudaSuccess || cudaMalloc(&dm.p, MN * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&db.p, HW * C * sizeof(cf)) != cudaSuccess || cudaMalloc(&dx.p, N * sizeof(cf)) != cudaSuccess ||
+      cudaMalloc(&du.p, HW * C * sizeof(cf)) != cudaSuccess || cudaMalloc(&dc.p, HW * C * sizeof(cf)) != cudaSuccess)
     return die("device allocation failed");
   cudaMemcpy(dk.p, kdata.data(), K * sizeof(cf), cudaMemcpyHostToDevice);
-  cudaMemcpy(dm.p, mask.data(), N * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemcpy(dm.p, mask.data(), MN * sizeof(float), cudaMemcpyHostToDevice);
+  if (o.nonuniform) {
+    if (cudaMalloc(&dd.p, S * T * sizeof(float)) != cudaSuccess) return die("device allocation failed");
+    cudaMemcpy(dd.p, dens.data(), S * T * sizeof(float), cudaMemcpyHostToDevice);
+  }
+
+  std::vector<cf> b1(HW * C, cf(1, 0)), u0(HW, cf(0, 0));
+  avx_coil_params cp;
+  avx_coil_default_params(&cp);
+  auto cfv = [&](const char* k, float def) { return o.conf.count(k) ? std::stof(o.conf[k]) : def; };
+  cp.uH1mu = cfv("coil.uH1mu", cp.uH1mu);
+  cp.uReg = cfv("coil.uReg", cp.uReg);
+  cp.uNrIt = (unsigned)cfv("coil.uNrIt", (float)cp.uNrIt);
+  cp.uTau = cfv("coil.uTau", cp.uTau);
+  cp.uSigma = cfv("coil.uSigma", cp.uSigma);
+  cp.uAlpha0 = cfv("coil.uAlpha0", cp.uAlpha0);
+  cp.uAlpha1 = cfv("coil.uAlpha1", cp.uAlpha1);
+  cp.b1Reg = cfv("coil.b1Reg", cp.b1Reg);
+  cp.b1NrIt = (unsigned)cfv("coil.b1NrIt", (float)cp.b1NrIt);
+  cp.b1Tau = cfv("coil.b1Tau", cp.b1Tau);
+  cp.b1Sigma = cfv("coil.b1Sigma", cp.b1Sigma);
+  cp.b1FinalReg = cfv("coil.b1FinalReg", cp.b1FinalReg);
+  cp.b1FinalNrIt = (unsigned)cfv("coil.b1FinalNrIt", (float)cp.b1FinalNrIt);
+  if (!o.sens.empty() && avcli::read_bin(o.sens, buf, &cplx, &err)) {
+    if (buf.size() != HW * C) return die("coil sensitivities hold " + std::to_string(buf.size()) + " values");
+    for (size_t i = 0; i < HW * C; ++i) b1[i] = cf(buf[i]);
+    std::cout << "B1 File " << o.sens << " successfully loaded." << std::endl;
+    if (!o.u0.empty() && avcli::read_bin(o.u0, buf, &cplx, &err) && buf.size() == HW) {
+      for (size_t i = 0; i < HW; ++i) u0[i] = cf(buf[i]);
+      std::cout << " initial solution (u0) file " << o.u0 << " successfully loaded." << std::endl;
+    } else {
+      std::cout << "no initial solution (u0) data provided!" << std::endl;
+      Dev tu;
+      cudaMalloc(&tu.p, HW * sizeof(cf));
+      const avx_status st =
+          o.nonuniform ? avx_coil_time_averaged_radial(W, H, C, T, (unsigned)S, (const float*)dm.p, (const float*)dd.p,
+                                                       (const avx_cf32*)dk.p, (avx_cf32*)tu.p, (avx_cf32*)dc.p, 0)
+                       : avx_coil_time_averaged(W, H, C, T, (const avx_cf32*)dk.p, (const float*)dm.p,
+                                                (avx_cf32*)tu.p, (avx_cf32*)dc.p, 0);
+      if (st != AVX_OK) return die(avx_last_error());
+      std::vector<cf> crec(HW * C);
+      cudaMemcpy(crec.data(), dc.p, HW * C * sizeof(cf), cudaMemcpyDeviceToHost);
+      u0 = given_b1_u0(crec, b1, HW, C);
+    }
+  } else {
+    std::cout << "Performing Coil Construction!" << std::endl;
+    const avx_status st =
+        o.nonuniform ? avx_coil_construction_radial(W, H, C, T, (unsigned)S, &cp, (const float*)dm.p,
+                                                    (const float*)dd.p, (const avx_cf32*)dk.p, (avx_cf32*)du.p,
+                                                    (avx_cf32*)db.p)
+                     : avx_coil_construction(W, H, C, T, &cp, (const avx_cf32*)dk.p, (const float*)dm.p,
+                                             (avx_cf32*)du.p, (avx_cf32*)db.p);
+    if (st != AVX_OK) return die(avx_last_error());
+    cudaMemcpy(b1.data(), db.p, HW * C * sizeof(cf), cudaMemcpyDeviceToHost);
+    cudaMemcpy(u0.data(), (cf*)du.p + (size_t)(C - 1) * HW, HW * sizeof(cf), cudaMemcpyDeviceToHost);
+    if (o.nonuniform)
+      for (auto& v : u0) v /= (float)T;  // main.cpp:636-640
+    std::vector<cd> e(HW);
+    for (size_t i = 0; i < HW; ++i) e[i] = cd(u0[i]);
+    avcli::write_bin(outdir + "/u0_reconstructed.bin", e, true, &err);
+    e.resize(HW * C);
+    for (size_t i = 0; i < HW * C; ++i) e[i] = cd(b1[i]);
+    avcli::write_bin(outdir + "/b1_reconstructed.bin", e, true, &err);
+  }
   cudaMemcpy(db.p, b1.data(), HW * C * sizeof(cf), cudaMemcpyHostToDevice);
   for (unsigned t = 0; t < T; ++t)
     cudaMemcpy((cf*)dx.p + t * HW, u0.data(), HW * sizeof(cf), cudaMemcpyHostToDevice);
 
   avx_operator* op = nullptr;
-  if (avx_cartesian_operator_create(W, H, C, T, (const float*)dm.p, 0, &op) != AVX_OK) return die(avx_last_error());
+  if (o.nonuniform) {
+    const float kw = o.conf.count("gpunufft.kernelWidth") ? std::stof(o.conf["gpunufft.kernelWidth"]) : 3.f;
+    const float sw = o.conf.count("gpunufft.sectorWidth") ? std::stof(o.conf["gpunufft.sectorWidth"]) : 8.f;
+    const float osf = o.conf.count("gpunufft.osf") ? std::stof(o.conf["gpunufft.osf"]) : 2.f;
+    std::cout << "Init NonCartesian Operator using kernelWidth:" << kw << " sectorWidth:" << sw << " OSF:" << osf
+              << std::endl;
+    if (avx_radial_operator_create(W, H, C, T, spf * T, nRO, spf, (const float*)dm.p, (const float*)dd.p, kw, sw,
+                                   osf, &op) != AVX_OK)
+      return die(avx_last_error());
+  } else if (avx_cartesian_operator_create(W, H, C, T, (const float*)dm.p, 0, &op) != AVX_OK) {
+    return die(avx_last_error());
+  }
   avx_solver* s = nullptr;
   if (avx_solver_create(method, W, H, C, T, &p, op, &s) != AVX_OK) return die(avx_last_error());
   avx_pd_params q;

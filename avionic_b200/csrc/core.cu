@@ -20,6 +20,8 @@
 #include <vector>
 
 #include "../../include/avionic.h"
+#include "coils.cuh"
+#include "fft2d.cuh"
 #include "pd_kernels.cuh"
 #include "radial.cuh"
 #include "utils_kernels.cuh"
@@ -148,6 +150,7 @@ avx_status configure_once() {
   if (g_configured) return AVX_OK;
   AVX_CK(avx::configure_kernels());
   AVX_CK(avx::configure_radial_kernels());
+  AVX_CK(avx::configure_fft2d_kernels());
   g_configured = true;
   return AVX_OK;
 }
@@ -819,6 +822,292 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
 }
 
 // ===========================================================================
+// Coil-sensitivity estimation (CUDA/src/coil_construction.cpp:55-556)
+// ===========================================================================
+
+namespace {
+
+struct Fft2dTables {
+  DevBuf<float2> twx, twy;
+  Fft2dPlan plan{};
+};
+
+avx_status make_fft2d(int W, int H, Fft2dTables& t) {
+  const std::vector<int> rx = fft_radices(W), ry = fft_radices(H);
+  if (rx.empty() || ry.empty()) return fail(AVX_E_UNSUPPORTED, "image size has no FFT plan (prime factor > 13)");
+  if (avx::fft2d_smem_bytes(std::max(W, H)) > 227 * 1024) return fail(AVX_E_UNSUPPORTED, "image too large for the FFT tile");
+  std::vector<float2> hx(W), hy(H);
+  for (int j = 0; j < W; ++j) hx[j] = make_float2((float)std::cos(2.0 * M_PI * j / W), (float)std::sin(2.0 * M_PI * j / W));
+  for (int j = 0; j < H; ++j) hy[j] = make_float2((float)std::cos(2.0 * M_PI * j / H), (float)std::sin(2.0 * M_PI * j / H));
+  AVX_CK(t.twx.alloc(W));
+  AVX_CK(t.twy.alloc(H));
+  AVX_CK(cudaMemcpy(t.twx.p, hx.data(), W * sizeof(float2), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(t.twy.p, hy.data(), H * sizeof(float2), cudaMemcpyHostToDevice));
+  t.plan.W = W;
+  t.plan.H = H;
+  t.plan.twx = t.twx.p;
+  t.plan.twy = t.twy.p;
+  t.plan.nradx = (int)rx.size();
+  t.plan.nrady = (int)ry.size();
+  for (int i = 0; i < 12; ++i) {
+    t.plan.radx[i] = i < t.plan.nradx ? rx[i] : 0;
+    t.plan.rady[i] = i < t.plan.nrady ? ry[i] : 0;
+  }
+  return AVX_OK;
+}
+
+avx_status coil_time_averaged(int W, int H, int C, int T, const float2* kdata, const float* mask, float2* u,
+                              float2* crec, int apply_phase, cudaStream_t s) {
+  Fft2dTables ft;
+  avx_status r = make_fft2d(W, H, ft);
+  if (r != AVX_OK) return r;
+  const int HW = W * H;
+  avx::launch_ta_sum(kdata, mask, crec, HW, C, T, s);
+  avx::launch_fft2d(ft.plan, crec, C, -1, s);  // unitary k-space -> image (e^{-2 pi i}), scaled below
+  avx::launch_ta_combine(crec, u, HW, C, (float)(1.0 / std::sqrt((double)HW)), apply_phase, s);
+  AVX_CK(cudaGetLastError());
+  AVX_CK(cudaStreamSynchronize(s));
+  return AVX_OK;
+}
+
+avx_status coil_b1_from_u_h1(int W, int H, int C, const avx_coil_params& p, const float2* u, const float2* crec,
+                             float2* absb1, cudaStream_t s) {
+  const int N = W * H;
+  DevBuf<double2> work;
+  DevBuf<double> muu;
+  AVX_CK(work.alloc((size_t)C * 4 * N));
+  AVX_CK(muu.alloc((size_t)C * N));
+  // the exact solution of the H1 system: FP64 CG to a relative residual of 1e-12
+  avx::launch_h1_cg(u, crec, p.uH1mu, W, H, C, 50000, 1e-12, work.p, muu.p, absb1, nullptr, s);
+  avx::launch_h1_normalize(absb1, N, C, s);
+  AVX_CK(cudaGetLastError());
+  AVX_CK(cudaStreamSynchronize(s));
+  return AVX_OK;
+}
+
+avx_status coil_utgv2(int W, int H, const avx_coil_params& p, const float2* b10, const float2* crec0,
+                      const std::vector<int>& inds, float2* x1, cudaStream_t s) {
+  const int N = W * H;
+  DevBuf<float2> buf;
+  DevBuf<int> dind;
+  AVX_CK(buf.alloc((size_t)11 * N));
+  AVX_CK(dind.alloc(inds.size()));
+  AVX_CK(cudaMemcpyAsync(dind.p, inds.data(), inds.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  AVX_CK(cudaMemsetAsync(buf.p, 0, (size_t)11 * N * sizeof(float2), s));
+  CoilPD a;
+  memset(&a, 0, sizeof(a));
+  a.W = W;
+  a.H = H;
+  a.sigma = p.uSigma;
+  a.tau = p.uTau;
+  a.s1 = (float)(1.0 / ((double)p.uAlpha1 * p.uReg));
+  a.s2 = (float)(1.0 / ((double)p.uAlpha0 * p.uReg));
+  a.x1 = x1;
+  a.x1n = x1;
+  a.ext1 = buf.p;
+  a.ext1n = buf.p;
+  for (int k = 0; k < 2; ++k) {
+    a.x2[k] = buf.p + (size_t)(1 + k) * N;
+    a.ext2[k] = buf.p + (size_t)(3 + k) * N;
+    a.ext2n[k] = a.ext2[k];
+    a.y1[k] = buf.p + (size_t)(5 + k) * N;
+  }
+  for (int k = 0; k < 3; ++k) a.y2[k] = buf.p + (size_t)(7 + k) * N;
+  float2* Lw = buf.p + (size_t)10 * N;
+  DevBuf<float2> Ib;
+  AVX_CK(Ib.alloc(N));
+  a.Lw = Lw;
+  a.Ib = Ib.p;
+  AVX_CK(cudaMemcpyAsync(a.ext1, x1, N * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+  avx::launch_utgv_prep(b10, crec0, dind.p, (int)inds.size(), p.uTau, N, Lw, Ib.p, s);
+  for (unsigned it = 0; it < p.uNrIt; ++it) avx::launch_utgv_iter(a, s);
+  AVX_CK(cudaGetLastError());
+  AVX_CK(cudaStreamSynchronize(s));
+  return AVX_OK;
+}
+
+avx_status coil_b1_recon(int W, int H, int coils, unsigned max_it, float mu, const avx_coil_params& p,
+                         const float2* u0, const float2* crec, float2* out, cudaStream_t s) {
+  const int N = W * H;
+  const size_t CN = (size_t)coils * N;
+  DevBuf<float2> buf;
+  DevBuf<unsigned> umax;
+  AVX_CK(buf.alloc(6 * CN));
+  AVX_CK(umax.alloc(1));
+  AVX_CK(cudaMemsetAsync(buf.p, 0, 6 * CN * sizeof(float2), s));
+  AVX_CK(cudaMemsetAsync(umax.p, 0, sizeof(unsigned), s));
+  CoilPD a;
+  memset(&a, 0, sizeof(a));
+  a.W = W;
+  a.H = H;
+  a.sigma = p.b1Sigma;
+  a.tau = p.b1Tau;
+  a.mu = mu;
+  a.x1 = a.x1n = buf.p;
+  a.ext1 = a.ext1n = buf.p + CN;
+  a.y1[0] = buf.p + 2 * CN;
+  a.y1[1] = buf.p + 3 * CN;
+  float2* Lw = buf.p + 4 * CN;
+  float2* Iu = buf.p + 5 * CN;
+  a.Lw = Lw;
+  a.Ib = Iu;
+  avx::launch_absmax(u0, N, umax.p, s);
+  avx::launch_b1r_prep(u0, umax.p, crec, coils, N, p.b1Tau, Lw, Iu, s);
+  for (unsigned it = 0; it < max_it; ++it) avx::launch_b1r_iter(a, coils, s);
+  avx::launch_b1r_normalize(a.x1, out, N, coils, s);
+  AVX_CK(cudaGetLastError());
+  AVX_CK(cudaStreamSynchronize(s));
+  return AVX_OK;
+}
+
+avx_status abs_sum(const float2* a, const float2* b, int N, cudaStream_t s, double* out) {
+  DevBuf<double> part;
+  AVX_CK(part.alloc(64));
+  avx::launch_abs_sum(a, b, N, part.p, 64, s);
+  std::vector<double> h(64);
+  AVX_CK(cudaMemcpyAsync(h.data(), part.p, 64 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  AVX_CK(cudaStreamSynchronize(s));
+  double acc = 0.0;
+  for (double v : h) acc += v;
+  *out = acc;
+  return AVX_OK;
+}
+
+__global__ void abs_inplace_kernel(float2* v, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = make_float2(sqrtf(cabs2(v[i])), 0.f);
+}
+
+// NoncartesianCoilConstruction::TimeAveragedReconstruction
+// (noncartesian_coil_construction.cpp:21-127): every frame's samples in one
+// gridding adjoint (kernel width 3, sector width 8, osf 2), per coil.
+avx_status coil_time_averaged_radial(int W, int H, int C, int T, int S, const float* traj, const float* dens,
+                                     const float2* kdata, float2* u, float2* crec, int apply_phase, cudaStream_t s) {
+  const size_t TS = (size_t)T * S;
+  std::vector<float> ht((size_t)T * 2 * S), hd(TS), ht1(2 * TS);
+  AVX_CK(cudaMemcpy(ht.data(), traj, ht.size() * sizeof(float), cudaMemcpyDeviceToHost));
+  AVX_CK(cudaMemcpy(hd.data(), dens, hd.size() * sizeof(float), cudaMemcpyDeviceToHost));
+  for (int f = 0; f < T; ++f)
+    for (int j = 0; j < S; ++j) {
+      ht1[(size_t)f * S + j] = ht[((size_t)f * 2 + 0) * S + j];
+      ht1[TS + (size_t)f * S + j] = ht[((size_t)f * 2 + 1) * S + j];
+    }
+  avx_operator op;
+  op.kind = 1;
+  op.W = W; op.H = H; op.C = 1; op.T = 1;
+  op.S = (int)TS;
+  op.spf = 1;
+  avx_status r = build_radial(&op, ht1.data(), hd.data(), 3.f, 8.f, 2.f);
+  if (r != AVX_OK) return r;
+  DevBuf<float2> ones, samp;
+  AVX_CK(ones.alloc((size_t)W * H));
+  AVX_CK(samp.alloc(TS));
+  std::vector<float2> h1((size_t)W * H, make_float2(1.f, 0.f));
+  AVX_CK(cudaMemcpy(ones.p, h1.data(), h1.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  RArgs ra = make_rargs(&op, ones.p, nullptr, nullptr);
+  for (int c = 0; c < C; ++c) {
+    // gather coil c's samples of all frames ([frame][coil][sample] -> [frame][sample])
+    for (int f = 0; f < T; ++f)
+      AVX_CK(cudaMemcpyAsync(samp.p + (size_t)f * S, kdata + ((size_t)f * C + c) * S, S * sizeof(float2),
+                             cudaMemcpyDeviceToDevice, s));
+    avx::launch_rad_spread(ra, samp.p, s);
+    avx::launch_rad_fft(ra, +1, s);
+    avx::launch_rad_crop(ra, crec + (size_t)c * W * H, s);
+  }
+  avx::launch_ta_combine(crec, u, W * H, C, 1.f, apply_phase, s);
+  AVX_CK(cudaGetLastError());
+  AVX_CK(cudaStreamSynchronize(s));
+  return AVX_OK;
+}
+
+// PerformCoilConstruction after the time-averaged reconstruction
+// (coil_construction.cpp:447-556): u0 (W*H, replaced by |u0|) and crec (C*W*H)
+avx_status coil_estimate(int W, int H, int C, const avx_coil_params& p, float2* u0p, float2* crecp, float2* u,
+                         float2* b1, cudaStream_t s) {
+  const int N = W * H;
+  DevBuf<float2> absb1, w, uin, cin, x1;
+  AVX_CK(absb1.alloc((size_t)C * N));
+  AVX_CK(w.alloc(N));
+  AVX_CK(uin.alloc(N));
+  AVX_CK(cin.alloc(N));
+  AVX_CK(x1.alloc(N));
+  struct {
+    float2* p;
+  } u0{u0p}, crec{crecp};
+  avx_status r;
+  abs_inplace_kernel<<<(N + 255) / 256, 256, 0, s>>>(u0.p, N);
+  r = coil_b1_from_u_h1(W, H, C, p, u0.p, crec.p, absb1.p, s);
+  if (r != AVX_OK) return r;
+  // FindMaximumSum (coil_construction.cpp:55-73)
+  std::vector<int> inds;
+  {
+    double best = -1.0;
+    int bi = 0;
+    for (int c = 0; c < C; ++c) {
+      double v;
+      r = abs_sum(crec.p + (size_t)c * N, nullptr, N, s, &v);
+      if (r != AVX_OK) return r;
+      if (v > best) {
+        best = v;
+        bi = c;
+      }
+    }
+    inds.push_back(bi);
+  }
+  AVX_CK(cudaMemsetAsync(b1, 0, (size_t)C * N * sizeof(float2), s));
+  AVX_CK(cudaMemsetAsync(u, 0, (size_t)C * N * sizeof(float2), s));
+  AVX_CK(cudaMemcpyAsync(b1 + (size_t)inds[0] * N, absb1.p + (size_t)inds[0] * N, N * sizeof(float2),
+                         cudaMemcpyDeviceToDevice, s));
+  r = coil_utgv2(W, H, p, b1, crec.p, inds, u, s);  // u[0] starts at zero
+  if (r != AVX_OK) return r;
+  AVX_CK(cudaMemsetAsync(w.p, 0, N * sizeof(float2), s));
+  float2* uMax = u;
+  for (int cnt = 1; cnt < C; ++cnt) {
+    const int prev = inds[cnt - 1];
+    avx::launch_weight_update(w.p, absb1.p + (size_t)prev * N, N, s);
+    double best = -1.0;
+    int mi = -1;
+    for (int k = 0; k < C; ++k) {
+      if (std::find(inds.begin(), inds.end(), k) != inds.end()) continue;
+      double v;
+      r = abs_sum(crec.p + (size_t)prev * N, crec.p + (size_t)k * N, N, s, &v);
+      if (r != AVX_OK) return r;
+      if (v > best) {
+        best = v;
+        mi = k;
+      }
+    }
+    inds.push_back(mi);
+    avx::launch_greedy_inputs(absb1.p + (size_t)mi * N, u + (size_t)(cnt - 1) * N, w.p, crec.p + (size_t)mi * N,
+                              uin.p, cin.p, N, s);
+    r = coil_b1_recon(W, H, 1, p.b1NrIt, p.b1Reg, p, uin.p, cin.p, x1.p, s);
+    if (r != AVX_OK) return r;
+    avx::launch_phase_apply(absb1.p + (size_t)mi * N, x1.p, b1 + (size_t)mi * N, N, s);
+    uMax = u + (size_t)cnt * N;
+    AVX_CK(cudaMemcpyAsync(uMax, u + (size_t)(cnt - 1) * N, N * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+    r = coil_utgv2(W, H, p, b1, crec.p, inds, uMax, s);
+    if (r != AVX_OK) return r;
+  }
+  // final correction of all coils (coil_construction.cpp:555)
+  r = coil_b1_recon(W, H, C, p.b1FinalNrIt, p.b1FinalReg, p, uMax, crec.p, b1, s);
+  if (r != AVX_OK) return r;
+  AVX_CK(cudaGetLastError());
+  return AVX_OK;
+}
+
+avx_status coil_construction(int W, int H, int C, int T, const avx_coil_params& p, const float2* kdata,
+                             const float* mask, float2* u, float2* b1, cudaStream_t s) {
+  DevBuf<float2> u0, crec;
+  AVX_CK(u0.alloc((size_t)W * H));
+  AVX_CK(crec.alloc((size_t)C * W * H));
+  avx_status r = coil_time_averaged(W, H, C, T, kdata, mask, u0.p, crec.p, 1, s);
+  if (r != AVX_OK) return r;
+  return coil_estimate(W, H, C, p, u0.p, crec.p, u, b1, s);
+}
+
+}  // namespace
+
+// ===========================================================================
 // C ABI
 // ===========================================================================
 
@@ -1312,6 +1601,101 @@ avx_status avx_time_space_weights(float tsw, float* ds, float* dt) {
   *ds = (float)a;
   *dt = (float)b;
   return AVX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// coil-sensitivity estimation
+// ---------------------------------------------------------------------------
+
+avx_status avx_coil_default_params(avx_coil_params* p) {
+  if (!p) return fail(AVX_E_ARG, "null params");
+  p->uH1mu = 1e-5f;
+  p->uReg = 0.2f;
+  p->uNrIt = 100;
+  p->uSigmaTauRatio = 1.f;
+  p->uSigma = (float)std::sqrt(1.0 / 12.0);
+  p->uTau = (float)std::sqrt(1.0 / 12.0);
+  p->uAlpha0 = (float)std::sqrt(2.0);
+  p->uAlpha1 = 1.f;
+  p->b1Reg = 2.f;
+  p->b1NrIt = 500;
+  p->b1SigmaTauRatio = 1.f;
+  p->b1Sigma = (float)std::sqrt(1.0 / 8.0);
+  p->b1Tau = (float)std::sqrt(1.0 / 8.0);
+  p->b1FinalReg = 0.1f;
+  p->b1FinalNrIt = 1000;
+  return AVX_OK;
+}
+
+avx_status avx_coil_time_averaged(unsigned W, unsigned H, unsigned C, unsigned T, const avx_cf32* d_kdata,
+                                  const float* d_mask, avx_cf32* d_u, avx_cf32* d_crec, int apply_phase) {
+  if (!d_kdata || !d_u || !d_crec) return fail(AVX_E_ARG, "null argument");
+  avx_status r = configure_once();
+  if (r != AVX_OK) return r;
+  return coil_time_averaged((int)W, (int)H, (int)C, (int)T, reinterpret_cast<const float2*>(d_kdata), d_mask,
+                            reinterpret_cast<float2*>(d_u), reinterpret_cast<float2*>(d_crec), apply_phase, 0);
+}
+
+avx_status avx_coil_b1_from_u_h1(unsigned W, unsigned H, unsigned C, const avx_coil_params* p, const avx_cf32* d_u,
+                                 const avx_cf32* d_crec, avx_cf32* d_absb1) {
+  if (!p || !d_u || !d_crec || !d_absb1) return fail(AVX_E_ARG, "null argument");
+  return coil_b1_from_u_h1((int)W, (int)H, (int)C, *p, reinterpret_cast<const float2*>(d_u),
+                           reinterpret_cast<const float2*>(d_crec), reinterpret_cast<float2*>(d_absb1), 0);
+}
+
+avx_status avx_coil_utgv2(unsigned W, unsigned H, const avx_coil_params* p, const avx_cf32* d_b1,
+                          const avx_cf32* d_crec, const int* h_inds, unsigned ninds, avx_cf32* d_x1) {
+  if (!p || !d_b1 || !d_crec || !h_inds || !ninds || !d_x1) return fail(AVX_E_ARG, "null argument");
+  std::vector<int> inds(h_inds, h_inds + ninds);
+  return coil_utgv2((int)W, (int)H, *p, reinterpret_cast<const float2*>(d_b1), reinterpret_cast<const float2*>(d_crec),
+                    inds, reinterpret_cast<float2*>(d_x1), 0);
+}
+
+avx_status avx_coil_b1_recon(unsigned W, unsigned H, unsigned coils, unsigned max_it, float mu,
+                             const avx_coil_params* p, const avx_cf32* d_u0, const avx_cf32* d_crec, avx_cf32* d_b1) {
+  if (!p || !d_u0 || !d_crec || !d_b1) return fail(AVX_E_ARG, "null argument");
+  return coil_b1_recon((int)W, (int)H, (int)coils, max_it, mu, *p, reinterpret_cast<const float2*>(d_u0),
+                       reinterpret_cast<const float2*>(d_crec), reinterpret_cast<float2*>(d_b1), 0);
+}
+
+avx_status avx_coil_time_averaged_radial(unsigned W, unsigned H, unsigned C, unsigned T, unsigned S,
+                                         const float* d_traj, const float* d_dens, const avx_cf32* d_kdata,
+                                         avx_cf32* d_u, avx_cf32* d_crec, int apply_phase) {
+  if (!d_traj || !d_dens || !d_kdata || !d_u || !d_crec) return fail(AVX_E_ARG, "null argument");
+  avx_status r = configure_once();
+  if (r != AVX_OK) return r;
+  return coil_time_averaged_radial((int)W, (int)H, (int)C, (int)T, (int)S, d_traj, d_dens,
+                                   reinterpret_cast<const float2*>(d_kdata), reinterpret_cast<float2*>(d_u),
+                                   reinterpret_cast<float2*>(d_crec), apply_phase, 0);
+}
+
+avx_status avx_coil_construction_radial(unsigned W, unsigned H, unsigned C, unsigned T, unsigned S,
+                                        const avx_coil_params* p, const float* d_traj, const float* d_dens,
+                                        const avx_cf32* d_kdata, avx_cf32* d_u, avx_cf32* d_b1) {
+  if (!d_traj || !d_dens || !d_kdata || !d_u || !d_b1) return fail(AVX_E_ARG, "null argument");
+  avx_status r = configure_once();
+  if (r != AVX_OK) return r;
+  avx_coil_params dp;
+  avx_coil_default_params(&dp);
+  DevBuf<float2> u0, crec;
+  AVX_CK(u0.alloc((size_t)W * H));
+  AVX_CK(crec.alloc((size_t)C * W * H));
+  r = coil_time_averaged_radial((int)W, (int)H, (int)C, (int)T, (int)S, d_traj, d_dens,
+                                reinterpret_cast<const float2*>(d_kdata), u0.p, crec.p, 1, 0);
+  if (r != AVX_OK) return r;
+  return coil_estimate((int)W, (int)H, (int)C, p ? *p : dp, u0.p, crec.p, reinterpret_cast<float2*>(d_u),
+                       reinterpret_cast<float2*>(d_b1), 0);
+}
+
+avx_status avx_coil_construction(unsigned W, unsigned H, unsigned C, unsigned T, const avx_coil_params* p,
+                                 const avx_cf32* d_kdata, const float* d_mask, avx_cf32* d_u, avx_cf32* d_b1) {
+  if (!d_kdata || !d_u || !d_b1) return fail(AVX_E_ARG, "null argument");
+  avx_status r = configure_once();
+  if (r != AVX_OK) return r;
+  avx_coil_params dp;
+  avx_coil_default_params(&dp);
+  return coil_construction((int)W, (int)H, (int)C, (int)T, p ? *p : dp, reinterpret_cast<const float2*>(d_kdata),
+                           d_mask, reinterpret_cast<float2*>(d_u), reinterpret_cast<float2*>(d_b1), 0);
 }
 
 // ---------------------------------------------------------------------------

@@ -249,6 +249,69 @@ float avx_ellipke(float m);
 avx_status avx_time_space_weights(float time_space_weight, float* ds, float* dt);
 
 /* ------------------------------------------------------------------ */
+/* Coil-sensitivity estimation (CoilConstruction,                       */
+/* CUDA/src/coil_construction.cpp, cartesian_coil_construction.cpp)     */
+/* ------------------------------------------------------------------ */
+
+/* CoilConstructionParams (CUDA/include/coil_construction.h:19-41) */
+typedef struct avx_coil_params {
+  float uH1mu, uReg;
+  unsigned uNrIt;
+  float uTau, uSigma, uSigmaTauRatio, uAlpha0, uAlpha1;
+  float b1Reg;
+  unsigned b1NrIt;
+  float b1Tau, b1Sigma, b1SigmaTauRatio, b1FinalReg;
+  unsigned b1FinalNrIt;
+} avx_coil_params;
+
+/* CoilConstruction::InitParams (coil_construction.cpp:22-48) */
+avx_status avx_coil_default_params(avx_coil_params* p);
+
+/* CartesianCoilConstruction::TimeAveragedReconstruction
+ * (cartesian_coil_construction.cpp:23-86), uncentred transform:
+ * crec_c = F^-1(sum_t k_{t,c} / max(1, sum_t mask_t)); u = sqrt(sum_c
+ * |crec_c|^2), times the phase of sum_c crec_c when apply_phase.
+ * d_mask may be NULL (all ones).  d_u: W*H, d_crec: W*H*C. */
+avx_status avx_coil_time_averaged(unsigned W, unsigned H, unsigned C, unsigned T, const avx_cf32* d_kdata,
+                                  const float* d_mask, avx_cf32* d_u, avx_cf32* d_crec, int apply_phase);
+
+/* B1FromUH1 (coil_construction.cpp:363-445): per coil the solution of
+ * (uH1mu |u|^2 - Laplace_periodic) b = conj(u) uH1mu |crec_c|, normalised
+ * over coils; returns |b1|.  Solved by FP64 conjugate gradients to a relative
+ * residual of 1e-12 (the reference stops at 800 FP32 iterations). */
+avx_status avx_coil_b1_from_u_h1(unsigned W, unsigned H, unsigned C, const avx_coil_params* p, const avx_cf32* d_u,
+                                 const avx_cf32* d_crec, avx_cf32* d_absb1);
+
+/* UTGV2Recon (coil_construction.cpp:75-215) on the coils listed in h_inds;
+ * d_x1 (W*H) is the initial image and receives the result. */
+avx_status avx_coil_utgv2(unsigned W, unsigned H, const avx_coil_params* p, const avx_cf32* d_b1,
+                          const avx_cf32* d_crec, const int* h_inds, unsigned ninds, avx_cf32* d_x1);
+
+/* B1Recon (coil_construction.cpp:217-361) for `coils` coil images. */
+avx_status avx_coil_b1_recon(unsigned W, unsigned H, unsigned coils, unsigned max_it, float mu,
+                             const avx_coil_params* p, const avx_cf32* d_u0, const avx_cf32* d_crec, avx_cf32* d_b1);
+
+/* PerformCoilConstruction (coil_construction.cpp:447-556), Cartesian data:
+ * d_u receives the C image estimates (W*H*C, the last is the initial image
+ * the CLI uses, main.cpp:634), d_b1 the coil maps (W*H*C).  p may be NULL. */
+avx_status avx_coil_construction(unsigned W, unsigned H, unsigned C, unsigned T, const avx_coil_params* p,
+                                 const avx_cf32* d_kdata, const float* d_mask, avx_cf32* d_u, avx_cf32* d_b1);
+
+/* NoncartesianCoilConstruction::TimeAveragedReconstruction
+ * (noncartesian_coil_construction.cpp:21-127): all frames' samples through
+ * one radial gridding adjoint (kernel width 3, sector width 8, osf 2) per
+ * coil.  d_traj/d_dens/d_kdata as for avx_radial_operator_create and the
+ * radial k-space layout; S samples per frame. */
+avx_status avx_coil_time_averaged_radial(unsigned W, unsigned H, unsigned C, unsigned T, unsigned S,
+                                         const float* d_traj, const float* d_dens, const avx_cf32* d_kdata,
+                                         avx_cf32* d_u, avx_cf32* d_crec, int apply_phase);
+
+/* PerformCoilConstruction for radial data (main.cpp:210-248). */
+avx_status avx_coil_construction_radial(unsigned W, unsigned H, unsigned C, unsigned T, unsigned S,
+                                        const avx_coil_params* p, const float* d_traj, const float* d_dens,
+                                        const avx_cf32* d_kdata, avx_cf32* d_u, avx_cf32* d_b1);
+
+/* ------------------------------------------------------------------ */
 /* Host-buffer reconstruction (the CLI path, main.cpp:507-839)         */
 /* ------------------------------------------------------------------ */
 

@@ -181,12 +181,35 @@ def b1_recon(u0, crec, coils, max_it, mu, p):
     return x1 / nrm[None]
 
 
+def time_averaged_radial(kdata, traj, dens, W, H, apply_phase=True):
+    """NoncartesianCoilConstruction::TimeAveragedReconstruction
+    (noncartesian_coil_construction.cpp:21-127): all frames' samples through
+    one gridding adjoint (kernel width 3, sector width 8, osf 2) per coil,
+    with the gridding of oracle/radial.py.  kdata (T,C,S)."""
+    from .radial import RadialOperator
+    T, C, S = kdata.shape
+    tr = np.concatenate([traj[f] for f in range(T)], axis=1)[None]      # (1, 2, T S)
+    de = dens.reshape(1, T * S)
+    op = RadialOperator(W, H, 1, 1, tr, de, 3.0, 8.0, 2.0)
+    ones = np.ones((1, H, W), complex)
+    crec = np.stack([op.forward(kdata[:, c, :].reshape(1, 1, T * S), ones)[0] for c in range(C)])
+    u = np.sqrt(np.sum(np.abs(crec) ** 2, axis=0)).astype(complex)
+    if apply_phase:
+        u = u * np.exp(1j * np.angle(np.sum(crec, axis=0)))
+    return u, crec
+
+
 def perform_coil_construction(kdata, mask, p=None, centered=False):
     """PerformCoilConstruction (coil_construction.cpp:447-556).  Returns
     (u (C,H,W) the sequence of image estimates, b1 (C,H,W))."""
-    p = p or default_params()
-    C = kdata.shape[1]
     u0, crec = time_averaged_reconstruction(kdata, mask, centered)
+    return estimate_from(u0, crec, p)
+
+
+def estimate_from(u0, crec, p=None):
+    """The part of PerformCoilConstruction after the time average."""
+    p = p or default_params()
+    C = crec.shape[0]
     u0 = np.abs(u0).astype(complex)
     absb1 = b1_from_u_h1(u0, crec, p)
     H, W = u0.shape

@@ -117,3 +117,49 @@ def test_cli_reconstruction_matches_oracle(tmp_path, method):
     if method == "ICTGV2":
         assert binfmt.read_bin(str(tmp_path / "x3_component")).size == T * H * W
         assert binfmt.read_bin(str(tmp_path / "ICTGVnorm")).size == len(tr["ICTGVnorm"])
+
+
+@needs_exe
+@pytest.mark.gpu
+def test_cli_radial_with_coil_construction(tmp_path):
+    """-n radial data without -s: coil construction, u0/b1 exports, then TGV2."""
+    from oracle import coils as co
+    from oracle import radial as rd
+    from oracle import solvers as so
+    from tests.test_radial import _problem
+    pr = _problem(13, W=20, H=20, C=3, T=3, nfe=40, spf=7)
+    T, C, S = pr["k"].shape
+    W, H = pr["W"], pr["H"]
+    raw = pr["k"] / np.sqrt(pr["dens"])[:, None, :]  # the CLI weights by sqrt(w) itself
+    paths = {"kdata": str(tmp_path / "k.bin"), "traj": str(tmp_path / "traj.bin"), "dens": str(tmp_path / "w.bin")}
+    binfmt.write_bin(paths["kdata"], raw.astype(np.complex64).astype(np.complex128))
+    binfmt.write_bin(paths["traj"], pr["traj"].astype(np.float32).astype(np.float64))
+    binfmt.write_bin(paths["dens"], pr["dens"].astype(np.float32).astype(np.float64))
+    cfg = tmp_path / "run.cfg"
+    cfg.write_text("maxIt = 40\n[coil]\nuNrIt = 20\nb1NrIt = 30\nb1FinalNrIt = 40\n[tgv2]\nlambda = 4.0\n"
+                   "sigma = 0.3333\ntau = 0.3333\ntimeSpaceWeight = 1.4\nalpha0 = 1.41421356\nalpha1 = 1.0\n"
+                   "[gpunufft]\nkernelWidth = 3\nsectorWidth = 8\nosf = 1.5\n")
+    out = str(tmp_path / "recon.bin")
+    dims = "%d:%d:0:%d:%d:0:%d:%d" % (W, H, pr["nfe"], pr["spf"], C, T)
+    r = run(["-n", "-m", "TGV2", "-p", str(cfg), "-g", "0", "-w", paths["dens"], "-d", dims, paths["kdata"],
+             paths["traj"], out])
+    assert r.returncode == 0, r.stderr + r.stdout
+    b1 = binfmt.read_bin(str(tmp_path / "b1_reconstructed.bin")).reshape(C, H, W)
+    u0 = binfmt.read_bin(str(tmp_path / "u0_reconstructed.bin")).reshape(H, W)
+    x = binfmt.read_bin(out).reshape(T, H, W)
+    # oracle: same pipeline
+    k32 = (raw.astype(np.complex64) * np.sqrt(pr["dens"].astype(np.float32))[:, None, :]).astype(complex)
+    tr, de = pr["traj"].astype(np.float32).astype(float), pr["dens"].astype(np.float32).astype(float)
+    p = co.default_params()
+    p["uNrIt"], p["b1NrIt"], p["b1FinalNrIt"] = 20, 30, 40
+    ua, crec = co.time_averaged_radial(k32, tr, de, W, H)
+    uo, bo = co.estimate_from(ua, crec, p)
+    assert np.linalg.norm(b1 - bo) / np.linalg.norm(bo) < 1e-4
+    u0o = uo[C - 1] / T
+    assert np.linalg.norm(u0 - u0o) / np.linalg.norm(u0o) < 1e-4
+    op = rd.RadialOperator(W, H, C, T, tr, de, 3.0, 8.0, 1.5)
+    q = so.init_params("TGV2")
+    q.maxIt, q.lam, q.sigma, q.tau, q.timeSpaceWeight, q.alpha0 = 40, 4.0, 0.3333, 0.3333, 1.4, 1.41421356
+    xo = so.tgv2(k32, np.repeat(u0.astype(np.complex64).astype(complex)[None], T, axis=0),
+                 b1.astype(np.complex64).astype(complex), op, q)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-4
