@@ -205,8 +205,9 @@ class Solver:
         check(lib.avx_solver_set_timing(self.handle, int(on)))
 
     def kernel_times(self):
-        """Mean ms of the (dual, k-space, primal) kernels of the last timed run."""
-        arr = (ctypes.c_float * 3)()
+        """Mean ms of the five stages (dual, forward transform, k-space rows,
+        adjoint, primal) of the iterations of the last timed run."""
+        arr = (ctypes.c_float * 5)()
         n = ctypes.c_uint()
         check(lib.avx_solver_kernel_times(self.handle, arr, ctypes.byref(n)))
         return list(arr), n.value

@@ -57,6 +57,7 @@ struct DevState {
   int ngap;               // records written to the gap history
   int iters;              // iterations started (dual_kernel increments it)
   int err;                // non-zero when a device-side check failed
+  double d_off;           // energy of the data outside the sampled rows (gap constant)
 };
 
 // Number of FP64 partial-sum slots a reduction writes per block.

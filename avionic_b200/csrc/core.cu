@@ -16,6 +16,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -183,7 +184,8 @@ struct avx_operator {
   RadialGeomDev rg{};
   DevBuf<float> r_traj, r_sqrtw, r_ipx, r_ipy;
   DevBuf<int> r_order, r_secstart;
-  DevBuf<float2> r_twgx, r_twgy, r_grid, r_khz;
+  DevBuf<float2> r_twgx, r_twgy, r_grid;
+  DevBuf<float2> r_khz;  // K^H z image (T x H x W), both operator kinds
   bool has_mask = false, binary = true;
   std::vector<int> rows, row_off;
   int R = 0;
@@ -248,6 +250,7 @@ static avx_status build_operator(avx_operator* op, const float* h_mask) {
   AVX_CK(op->d_twx.alloc(W));
   AVX_CK(op->d_twy.alloc(H));
   AVX_CK(op->d_qp.alloc((size_t)op->C * std::max(op->R, 1) * W));
+  AVX_CK(op->r_khz.alloc((size_t)T * H * W));
   if (op->R) AVX_CK(cudaMemcpy(op->d_rows.p, op->rows.data(), op->R * sizeof(int), cudaMemcpyHostToDevice));
   AVX_CK(cudaMemcpy(op->d_row_off.p, op->row_off.data(), (T + 1) * sizeof(int), cudaMemcpyHostToDevice));
   if (!mrow.empty()) AVX_CK(cudaMemcpy(op->d_mrow.p, mrow.data(), mrow.size() * sizeof(float), cudaMemcpyHostToDevice));
@@ -429,6 +432,36 @@ static avx_status check_dims(unsigned W, unsigned H, unsigned C, unsigned T) {
   return AVX_OK;
 }
 
+
+// Cached device state of avx_reconstruct_host: the operator, solver, CUDA
+// graphs and device buffers of the last call are reused while the problem
+// (device, method, sizes, parameters, debug step and mask contents) is
+// unchanged; the data, coil maps and initial image are copied every call.
+struct avx_solver;
+struct HostPlan {
+  int device = -1, method = -1, debugstep = 0;
+  unsigned W = 0, H = 0, C = 0, T = 0;
+  avx_pd_params params{};      // as given by the caller
+  avx_pd_params run_params{};  // as the solver holds them before its first run
+  bool has_mask = false;
+  std::vector<float> mask;
+  DevBuf<float2> dk, db1, dx;
+  DevBuf<float> dm;
+  avx_operator* op = nullptr;
+  avx_solver* s = nullptr;
+  cudaStream_t stream = nullptr;
+  bool matches(int dev, int m, unsigned w, unsigned h, unsigned c, unsigned t, int ds, const avx_pd_params* p,
+               const float* h_mask) const {
+    if (!s || dev != device || m != method || w != W || h != H || c != C || t != T || ds != debugstep) return false;
+    if (memcmp(p, &params, sizeof(params)) != 0) return false;
+    if ((h_mask != nullptr) != has_mask) return false;
+    return !h_mask || memcmp(h_mask, mask.data(), mask.size() * sizeof(float)) == 0;
+  }
+  void release();
+};
+static std::mutex g_plan_mu;
+static HostPlan g_plan;
+
 // ===========================================================================
 // Solver
 // ===========================================================================
@@ -456,7 +489,7 @@ struct avx_solver {
   // timing mode
   bool timing = false;
   std::vector<cudaEvent_t> events;
-  float kmean[3] = {0.f, 0.f, 0.f};
+  float kmean[AVX_NSTAGE] = {};
   unsigned kcount = 0;
 
   ~avx_solver() {
@@ -533,6 +566,7 @@ static PDArgs make_pdargs(avx_solver* s) {
   a.alpha = s->p.alpha;
   a.ic_a = (float)(alpha / m);
   a.ic_b = (float)((1.0 - alpha) / m);
+  a.khz = s->op->r_khz.p;
   a.st = s->st.p;
   return a;
 }
@@ -558,7 +592,6 @@ static avx::GapConst make_gapconst(avx_solver* s) {
   avx::GapConst gc;
   const double alpha = s->p.alpha, m = std::min(alpha, 1.0 - alpha);
   gc.lam = s->p.lambda;
-  gc.d_off_energy = s->d_off_energy;
   gc.N = (double)s->N();
   gc.stop_gap = s->p.stopPDGap;
   gc.alpha0 = s->p.alpha0;
@@ -576,7 +609,7 @@ static bool gap_due(const avx_solver* s, unsigned k) {
 
 static unsigned shape_launches(int kind, int shape) {
   if (kind == 1) return 10u + ((shape & 1) ? 7u : 0u) + ((shape & 2) ? 10u : 0u);
-  return 3u + ((shape & 1) ? 4u : 0u) + ((shape & 2) ? 3u : 0u);
+  return 5u + ((shape & 1) ? 5u : 0u) + ((shape & 2) ? 5u : 0u);
 }
 
 static RArgs solver_rargs(avx_solver* s, const float2* b1, const float2* in, const float2* in2) {
@@ -590,29 +623,32 @@ static RArgs solver_rargs(avx_solver* s, const float2* b1, const float2* in, con
 }
 
 // radial operator pass: K u (mode 0 z prox, 1 norm, 2 gap sums) and, for modes
-// 0 and 2, K^H z into the operator's K^H z image
-static void radial_pass(avx_solver* s, int mode, const float2* b1, const float2* in, const float2* in2) {
+// 0 and 2, K^H z into the operator's K^H z image.  ev (optional) receives
+// events after the forward FFT, the interpolation and the adjoint.
+static void radial_pass(avx_solver* s, int mode, const float2* b1, const float2* in, const float2* in2,
+                        cudaEvent_t* ev = nullptr) {
   RArgs r = solver_rargs(s, b1, in, in2);
   avx::launch_rad_pad(r, s->stream);
   avx::launch_rad_fft(r, -1, s->stream);
+  if (ev) cudaEventRecord(ev[0], s->stream);
   avx::launch_rad_interp(r, mode, s->stream);
+  if (ev) cudaEventRecord(ev[1], s->stream);
   if (mode == 1) return;
   avx::launch_rad_spread(r, s->z.p, s->stream);
   avx::launch_rad_fft(r, +1, s->stream);
   avx::launch_rad_crop(r, s->op->r_khz.p, s->stream);
+  if (ev) cudaEventRecord(ev[2], s->stream);
 }
 
 static void enqueue_shape_radial(avx_solver* s, int shape, const float2* b1, cudaEvent_t* ev) {
-  PDArgs a = make_pdargs(s);
-  a.khz = s->op->r_khz.p;
+  const PDArgs a = make_pdargs(s);
   const KArgs kdummy = make_kargs(s, b1, s->extc(0), nullptr);
   if (ev) cudaEventRecord(ev[0], s->stream);
   avx::launch_dual(s->method, a, s->stream);
   if (ev) cudaEventRecord(ev[1], s->stream);
-  radial_pass(s, 0, b1, s->extc(0), nullptr);
-  if (ev) cudaEventRecord(ev[2], s->stream);
-  avx::launch_primal(s->method, a, kdummy, s->stream, false);
-  if (ev) cudaEventRecord(ev[3], s->stream);
+  radial_pass(s, 0, b1, s->extc(0), nullptr, ev ? ev + 2 : nullptr);
+  avx::launch_primal(s->method, a, s->stream);
+  if (ev) cudaEventRecord(ev[5], s->stream);
   const int nk = avx::radial_interp_blocks(s->op->rg);
   if (shape & 1) {
     avx::Ptr8 e;
@@ -627,8 +663,7 @@ static void enqueue_shape_radial(avx_solver* s, int shape, const float2* b1, cud
     double* h = s->hist.p;
     const bool ic = s->method == AVX_METHOD_ICTGV2;
     avx::launch_gap_tail(s->method, a, kdummy, s->pimg.p, s->pk.p, nk, make_gapconst(s), h,
-                         ic ? h + (s->cap + 1) : nullptr, ic ? h + 2 * (s->cap + 1) : nullptr, s->cap, 0, false,
-                         s->stream);
+                         ic ? h + (s->cap + 1) : nullptr, ic ? h + 2 * (s->cap + 1) : nullptr, s->cap, 0, s->stream);
   }
 }
 
@@ -639,17 +674,7 @@ static void enqueue_shape(avx_solver* s, int shape, const float2* b1, cudaEvent_
   }
   const PDArgs a = make_pdargs(s);
   const KArgs ks = make_kargs(s, b1, s->extc(0), nullptr);
-  if (ev) {
-    cudaEventRecord(ev[0], s->stream);
-    avx::launch_dual(s->method, a, s->stream);
-    cudaEventRecord(ev[1], s->stream);
-    avx::launch_kspace(ks, 0, s->stream);
-    cudaEventRecord(ev[2], s->stream);
-    avx::launch_primal(s->method, a, ks, s->stream);
-    cudaEventRecord(ev[3], s->stream);
-  } else {
-    avx::launch_iteration(s->method, a, ks, s->stream);
-  }
+  avx::launch_iteration(s->method, a, ks, s->op->r_khz.p, s->stream, ev);
   if (shape & 1) {
     avx::Ptr8 e;
     const int P = method_P(s->method);
@@ -661,8 +686,8 @@ static void enqueue_shape(avx_solver* s, int shape, const float2* b1, cudaEvent_
     const KArgs kx = make_kargs(s, b1, s->primc(0), nullptr);
     double* h = s->hist.p;
     const bool ic = s->method == AVX_METHOD_ICTGV2;
-    avx::launch_gap(s->method, a, kx, s->pimg.p, s->pk.p, make_gapconst(s), h, ic ? h + (s->cap + 1) : nullptr,
-                    ic ? h + 2 * (s->cap + 1) : nullptr, s->cap, 0, s->stream);
+    avx::launch_gap(s->method, a, kx, s->op->r_khz.p, s->pimg.p, s->pk.p, make_gapconst(s), h,
+                    ic ? h + (s->cap + 1) : nullptr, ic ? h + 2 * (s->cap + 1) : nullptr, s->cap, 0, s->stream);
   }
 }
 
@@ -699,6 +724,7 @@ static avx_status prepare_run(avx_solver* s, const float2* data, const float2* x
   DevState h{};
   h.sigma = s->p.sigma;
   h.tau = s->p.tau;
+  h.d_off = s->d_off_energy;
   AVX_CK(cudaMemcpyAsync(s->st.p, &h, sizeof(h), cudaMemcpyHostToDevice, s->stream));
   AVX_CK(cudaStreamSynchronize(s->stream));
   return AVX_OK;
@@ -732,22 +758,26 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
       a.khz = s->op->r_khz.p;
       radial_pass(s, 2, b1, s->primc(0), nullptr);
       avx::launch_gap_tail(s->method, a, kx, s->pimg.p, s->pk.p, avx::radial_interp_blocks(s->op->rg),
-                           make_gapconst(s), h, h + (s->cap + 1), h + 2 * (s->cap + 1), s->cap, 1, false, s->stream);
+                           make_gapconst(s), h, h + (s->cap + 1), h + 2 * (s->cap + 1), s->cap, 1, s->stream);
     } else {
-      avx::launch_gap(s->method, a, kx, s->pimg.p, s->pk.p, make_gapconst(s), h, h + (s->cap + 1),
+      avx::launch_gap(s->method, a, kx, s->op->r_khz.p, s->pimg.p, s->pk.p, make_gapconst(s), h, h + (s->cap + 1),
                       h + 2 * (s->cap + 1), s->cap, 1, s->stream);
     }
     AVX_CK(cudaGetLastError());
   }
-  // graphs depend on every pointer and scalar baked into the launches
+  // graphs depend on every pointer and scalar baked into the launches; the
+  // step sizes and the data-energy constant live in DevState and are not baked
+  avx_pd_params pk = s->p;
+  pk.sigma = pk.tau = 0.f;
   const size_t key = (size_t)b1 ^ ((size_t)s->prim.p << 1) ^ ((size_t)s->op << 2) ^
-                     std::hash<std::string>()(std::string((const char*)&s->p, sizeof(s->p))) ^ (size_t)s->d_off_energy;
+                     std::hash<std::string>()(std::string((const char*)&pk, sizeof(pk)));
   if (key != s->graph_key) {
     s->drop_graphs();
     s->graph_key = key;
   }
-  if (s->timing && s->events.size() < (size_t)4 * s->p.maxIt) {
-    const size_t need = (size_t)4 * s->p.maxIt;
+  constexpr size_t NEV = AVX_NSTAGE + 1;  // events per timed iteration
+  if (s->timing && s->events.size() < NEV * s->p.maxIt) {
+    const size_t need = NEV * s->p.maxIt;
     while (s->events.size() < need) {
       cudaEvent_t e;
       AVX_CK(cudaEventCreate(&e));
@@ -761,7 +791,7 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
     const int shape = (step_due(k) ? 1 : 0) | (gap_due(s, k) ? 2 : 0);
     launches += shape_launches(s->op->kind, shape);
     if (s->timing) {
-      enqueue_shape(s, shape, b1, &s->events[(size_t)4 * k]);
+      enqueue_shape(s, shape, b1, &s->events[NEV * k]);
       AVX_CK(cudaGetLastError());
       continue;
     }
@@ -792,17 +822,17 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ev0, ev1);
   s->kcount = 0;
-  s->kmean[0] = s->kmean[1] = s->kmean[2] = 0.f;
+  for (int j = 0; j < AVX_NSTAGE; ++j) s->kmean[j] = 0.f;
   if (s->timing) {
-    double acc[3] = {0, 0, 0};
+    double acc[AVX_NSTAGE] = {};
     for (unsigned i = 0; i < k; ++i)
-      for (int j = 0; j < 3; ++j) {
+      for (int j = 0; j < AVX_NSTAGE; ++j) {
         float t = 0.f;
-        cudaEventElapsedTime(&t, s->events[(size_t)4 * i + j], s->events[(size_t)4 * i + j + 1]);
+        cudaEventElapsedTime(&t, s->events[NEV * i + j], s->events[NEV * i + j + 1]);
         acc[j] += t;
       }
     s->kcount = k;
-    for (int j = 0; j < 3; ++j) s->kmean[j] = k ? (float)(acc[j] / k) : 0.f;
+    for (int j = 0; j < AVX_NSTAGE; ++j) s->kmean[j] = k ? (float)(acc[j] / k) : 0.f;
   }
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
@@ -1205,6 +1235,7 @@ avx_status avx_operator_backward(avx_operator* op, const avx_cf32* d_x, avx_cf32
   k.b1 = reinterpret_cast<const float2*>(d_b1);
   k.in = reinterpret_cast<const float2*>(d_x);
   k.dense_out = reinterpret_cast<float2*>(d_k);
+  k.qp = op->d_qp.p;  // y-transformed rows between the two kernels
   if (op->R) avx::launch_kspace(k, 3, 0);
   AVX_CK(cudaGetLastError());
   AVX_CK(cudaDeviceSynchronize());
@@ -1398,10 +1429,10 @@ avx_status avx_solver_compute_gap(avx_solver* s, const avx_cf32* const* d_x, con
     nk = avx::radial_interp_blocks(s->op->rg);
     radial_pass(s, 2, reinterpret_cast<const float2*>(d_b1), s->primc(0), nullptr);
     avx::launch_gap_tail(s->method, a, kx, s->pimg.p, s->pk.p, nk, gc, h, h + (s->cap + 1), h + 2 * (s->cap + 1),
-                         s->cap, 0, false, s->stream);
+                         s->cap, 0, s->stream);
   } else {
-    avx::launch_gap(s->method, a, kx, s->pimg.p, s->pk.p, gc, h, h + (s->cap + 1), h + 2 * (s->cap + 1), s->cap, 0,
-                    s->stream);
+    avx::launch_gap(s->method, a, kx, s->op->r_khz.p, s->pimg.p, s->pk.p, gc, h, h + (s->cap + 1),
+                    h + 2 * (s->cap + 1), s->cap, 0, s->stream);
   }
   AVX_CK(cudaGetLastError());
   const int nimg = avx::gap_img_blocks(s->W, s->H, s->T);
@@ -1468,12 +1499,31 @@ avx_status avx_solver_set_timing(avx_solver* s, int on) {
 
 avx_status avx_solver_kernel_times(const avx_solver* s, float* mean_ms, unsigned* count) {
   if (!s || !mean_ms) return fail(AVX_E_ARG, "null argument");
-  for (int j = 0; j < 3; ++j) mean_ms[j] = s->kmean[j];
+  for (int j = 0; j < AVX_NSTAGE; ++j) mean_ms[j] = s->kmean[j];
   if (count) *count = s->kcount;
   return AVX_OK;
 }
 
 void avx_solver_destroy(avx_solver* s) { delete s; }
+
+}  // extern "C"
+
+void HostPlan::release() {
+  if (s) avx_solver_destroy(s);
+  if (op) avx_operator_destroy(op);
+  if (stream) cudaStreamDestroy(stream);
+  s = nullptr;
+  op = nullptr;
+  stream = nullptr;
+  dk.release();
+  db1.release();
+  dx.release();
+  dm.release();
+  mask.clear();
+  device = method = -1;
+}
+
+extern "C" {
 
 // ---------------------------------------------------------------------------
 // utils
@@ -1708,50 +1758,73 @@ avx_status avx_reconstruct_host(int method, unsigned W, unsigned H, unsigned C, 
   if (!h_kdata || !h_b1 || !h_x) return fail(AVX_E_ARG, "null argument");
   avx_status r = check_dims(W, H, C, T);
   if (r != AVX_OK) return r;
-  const size_t N = (size_t)W * H * T, K = N * C, HW = (size_t)W * H;
-  DevBuf<float2> dk, db1, dx;
-  DevBuf<float> dm;
-  AVX_CK(dk.alloc(K));
-  AVX_CK(db1.alloc(HW * C));
-  AVX_CK(dx.alloc(N));
-  AVX_CK(cudaMemcpy(dk.p, h_kdata, K * sizeof(float2), cudaMemcpyHostToDevice));
-  AVX_CK(cudaMemcpy(db1.p, h_b1, HW * C * sizeof(float2), cudaMemcpyHostToDevice));
-  if (h_mask) {
-    AVX_CK(dm.alloc(N));
-    AVX_CK(cudaMemcpy(dm.p, h_mask, N * sizeof(float), cudaMemcpyHostToDevice));
+  avx_pd_params defaults;
+  if (!params) {
+    r = avx_default_params(method, &defaults);
+    if (r != AVX_OK) return r;
+    params = &defaults;
   }
+  std::lock_guard<std::mutex> lock(g_plan_mu);
+  HostPlan& pl = g_plan;
+  const size_t N = (size_t)W * H * T, K = N * C, HW = (size_t)W * H;
+  int dev = 0;
+  AVX_CK(cudaGetDevice(&dev));
+  if (!pl.matches(dev, method, W, H, C, T, debugstep, params, h_mask)) {
+    pl.release();
+    AVX_CK(pl.dk.alloc(K));
+    AVX_CK(pl.db1.alloc(HW * C));
+    AVX_CK(pl.dx.alloc(N));
+    if (h_mask) {
+      AVX_CK(pl.dm.alloc(N));
+      AVX_CK(cudaMemcpy(pl.dm.p, h_mask, N * sizeof(float), cudaMemcpyHostToDevice));
+      pl.mask.assign(h_mask, h_mask + N);
+    }
+    r = avx_cartesian_operator_create(W, H, C, T, h_mask ? pl.dm.p : nullptr, 0, &pl.op);
+    if (r != AVX_OK) return r;
+    r = avx_solver_create(method, W, H, C, T, params, pl.op, &pl.s);
+    if (r != AVX_OK) {
+      pl.release();
+      return r;
+    }
+    AVX_CK(cudaStreamCreateWithFlags(&pl.stream, cudaStreamNonBlocking));
+    avx_solver_set_stream(pl.s, pl.stream);
+    avx_solver_set_debug(pl.s, debugstep > 0, debugstep);
+    pl.device = dev;
+    pl.method = method;
+    pl.W = W; pl.H = H; pl.C = C; pl.T = T;
+    pl.debugstep = debugstep;
+    pl.params = *params;
+    pl.has_mask = h_mask != nullptr;
+    avx_solver_get_params(pl.s, &pl.run_params);  // lambda adapted by the solver, if asked
+  }
+  // every call restarts from the parameters of a fresh solver (a run adapts sigma and tau)
+  avx_solver_set_params(pl.s, &pl.run_params);
+  cudaStream_t st = pl.stream;
+  AVX_CK(cudaMemcpyAsync(pl.dk.p, h_kdata, K * sizeof(float2), cudaMemcpyHostToDevice, st));
+  AVX_CK(cudaMemcpyAsync(pl.db1.p, h_b1, HW * C * sizeof(float2), cudaMemcpyHostToDevice, st));
   for (unsigned t = 0; t < T; ++t) {
     if (h_u0)
-      AVX_CK(cudaMemcpy(dx.p + t * HW, h_u0, HW * sizeof(float2), cudaMemcpyHostToDevice));
+      AVX_CK(cudaMemcpyAsync(pl.dx.p + t * HW, h_u0, HW * sizeof(float2), cudaMemcpyHostToDevice, st));
     else
-      AVX_CK(cudaMemset(dx.p + t * HW, 0, HW * sizeof(float2)));
+      AVX_CK(cudaMemsetAsync(pl.dx.p + t * HW, 0, HW * sizeof(float2), st));
   }
-  avx_operator* op = nullptr;
-  r = avx_cartesian_operator_create(W, H, C, T, h_mask ? dm.p : nullptr, 0, &op);
-  if (r != AVX_OK) return r;
   // zero the data outside the mask (main.cpp:507-519): the compact rows only
   // read sampled rows, and the rest enter the gap's data term as zeros.
-  if (h_mask) {
-    avx::launch_dense_rowidft(op->geom(), dk.p, op->d_qp.p, dm.p, 0);  // masks dk in place
-    AVX_CK(cudaDeviceSynchronize());
-  }
-  avx_solver* s = nullptr;
-  r = avx_solver_create(method, W, H, C, T, params, op, &s);
-  if (r != AVX_OK) {
-    avx_operator_destroy(op);
-    return r;
-  }
-  avx_solver_set_debug(s, debugstep > 0, debugstep);
-  r = avx_solver_run(s, reinterpret_cast<avx_cf32*>(dk.p), reinterpret_cast<avx_cf32*>(dx.p),
-                     reinterpret_cast<avx_cf32*>(db1.p));
+  if (h_mask) avx::launch_dense_rowidft(pl.op->geom(), pl.dk.p, pl.op->d_qp.p, pl.dm.p, st);  // masks dk in place
+  AVX_CK(cudaGetLastError());
+  r = avx_solver_run(pl.s, reinterpret_cast<avx_cf32*>(pl.dk.p), reinterpret_cast<avx_cf32*>(pl.dx.p),
+                     reinterpret_cast<avx_cf32*>(pl.db1.p));
   if (r == AVX_OK) {
-    cudaError_t e = cudaMemcpy(h_x, dx.p, N * sizeof(float2), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) r = fail(AVX_E_CUDA, cudaGetErrorString(e));
-    if (stats) *stats = s->stats;
+    AVX_CK(cudaMemcpyAsync(h_x, pl.dx.p, N * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    AVX_CK(cudaStreamSynchronize(st));
+    if (stats) *stats = pl.s->stats;
   }
-  avx_solver_destroy(s);
-  avx_operator_destroy(op);
   return r;
+}
+
+void avx_reconstruct_host_release(void) {
+  std::lock_guard<std::mutex> lock(g_plan_mu);
+  g_plan.release();
 }
 
 }  // extern "C"

@@ -1,15 +1,19 @@
 // Primal-dual kernels of the AVIONIC B200 reconstruction core.
 //
 // One PD iteration of TV / TGV2 / ICTGV2 (reference loops: CUDA/src/tv.cpp:137-198,
-// tgv2.cpp:234-335, ictgv2.cpp:334-490) runs as three kernels:
+// tgv2.cpp:234-335, ictgv2.cpp:334-490) with the Cartesian operator runs as
+// five kernels:
 //   dual_kernel    y <- prox(y + sigma * K_reg xbar)        (pointwise + stencils)
-//   kspace_kernel  z <- prox(z + sigma (K xbar - d)); Q' = row-IDFT(mask z)
-//                  one CTA per (coil, frame), compact sampled rows only
-//   primal_kernel  K^H z (column IDFT of Q', coil combine) fused with the
-//                  divergence stencils, the primal update and the extragradient
+//   ydft_kernel    y-transform of b1 xbar onto the sampled rows (all coils)
+//   rows_kernel    x-FFT of those rows, z <- prox(z + sigma (K xbar - d)),
+//                  Q' = row-IFFT(mask z); one CTA per (coil, frame)
+//   coladj_kernel  K^H z = sum_c conj(b1_c) column-IDFT(Q'_c)
+//   primal_kernel  divergence stencils, primal update and extragradient
 // The step-size rule (pd_recon.cpp:40-61) and the primal-dual gap
 // (tv.cpp:202-235, tgv2.cpp:130-176, ictgv2.cpp:163-249) are FP64 block
 // reductions plus a one-block finaliser that updates device-resident scalars.
+#include <algorithm>
+
 #include "pd_kernels.cuh"
 #include "stencil.cuh"
 #include "fft.cuh"
@@ -100,57 +104,46 @@ __global__ void __launch_bounds__(256) dual_kernel(PDArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// k-space kernel: one CTA per (coil, frame), sampled rows in chunks of KC.
-//
-// For a chunk of compact rows k (ky_k):
-//   P[k][x]  = 1/sqrt(H) sum_y  e^{+2 pi i (ky_k-sy)(y-sy)/H} b1[c,y,x] u[t,y,x]
-//   X[k][kx] = 1/sqrt(W) sum_x  e^{+2 pi i (kx-sx)(x-sx)/W} P[k][x]
-// which is the unitary image -> k-space transform of the reference restricted
-// to the kept rows (see oracle/cartesian.py for the sign).  Then, by mode:
-//   0  PD step:   z <- mask * (z + sigma mask X - sigma d) / (1 + sigma/lambda)
-//                 (tgv2.cpp:254-264 followed by the in-place masking of
-//                 ForwardOperation, cartesian_operator.cpp:83-88), and
-//                 Q'[k][x] = 1/sqrt(W) sum_kx e^{-2 pi i ..} z[k][kx]
-//   1  step rule: sum |mask X|^2 of u = in - in2
-//   2  gap:       sum |mask X - d|^2, Re<d,z>, |z|^2, then z <- mask z and Q'
-//   3  apply:     dense_out[t,c,ky,kx] = mask X
+// y-transform: frame t, a strip of YD_XS image columns, every coil.
+//   P[t,c,k,x] = 1/sqrt(H) sum_y e^{+2 pi i (ky_k-sy)(y-sy)/H} b1[c,y,x] u[t,y,x]
+// (u = in - in2 when in2 is given), written into k.qp in the compact layout
+// of z.  The strip of u is staged in shared memory once; coefficient rows
+// are staged in chunks of KC compact rows.  Thread (x, cs) handles the
+// coils cs, cs + YD_CG, ...
 // ---------------------------------------------------------------------------
 
 template <int KC>
-__global__ void __launch_bounds__(256) kspace_kernel(KArgs a, int mode) {
-  if (a.st && a.st->stop && mode != 3) return;
+__global__ void __launch_bounds__(YD_XS* YD_CG) ydft_kernel(KArgs a) {
+  if (a.st && a.st->stop) return;
   constexpr int KCP = KC + 2;  // padded row stride (keeps 16-byte alignment)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const CartGeomDev& g = a.g;
   const int W = g.W, H = g.H, C = g.C;
-  const int c = blockIdx.x % C;
-  const int t = blockIdx.x / C;
+  const int t = blockIdx.y;
+  const int x0 = blockIdx.x * YD_XS;
+  const int tx = threadIdx.x, cs = threadIdx.y;
+  const int tid = tx + YD_XS * cs, nt = YD_XS * YD_CG;
   const int r0 = g.row_off[t], r1 = g.row_off[t + 1];
   const int S = r1 - r0;
+  if (S == 0) return;
   const long long HW = (long long)W * H;
-  const long long zb = kbase(g, t, c, r0, r1);
-
-  float2* coefY = reinterpret_cast<float2*>(smem_raw);   // [H][KCP]
-  float2* P = coefY + (size_t)H * KCP;                     // [W][KCP]
-  float2* X = P + (size_t)W * KCP;                         // [W][KCP]
-  float2* twx = X + (size_t)W * KCP;                       // [W]
-  double* red = reinterpret_cast<double*>(twx + W);        // [32*3]
-
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int j = tid; j < W; j += nt) twx[j] = g.twx[j];
-
-  const float sig = a.st ? (float)a.st->sigma : 0.f;
-  const float zscale = (mode == 0) ? (float)(1.0 / (1.0 + a.st->sigma / (double)a.lam)) : 1.f;
-  double acc_r[3] = {0.0, 0.0, 0.0};
-
-  const float2* __restrict__ b1 = a.b1 + (long long)c * HW;
+  float2* su = reinterpret_cast<float2*>(smem_raw);  // [H][YD_XS]
+  float2* coef = su + (size_t)H * YD_XS;            // [H][KCP]
   const float2* __restrict__ u = a.in + (long long)t * HW;
   const float2* __restrict__ u2 = a.in2 ? a.in2 + (long long)t * HW : nullptr;
-
+  for (int e = tid; e < H * YD_XS; e += nt) {
+    const int y = e / YD_XS, x = x0 + e % YD_XS;
+    float2 v = czero();
+    if (x < W) {
+      v = u[(long long)y * W + x];
+      if (u2) v = csub(v, u2[(long long)y * W + x]);
+    }
+    su[e] = v;
+  }
+  const int x = x0 + tx;
   for (int k0 = 0; k0 < S; k0 += KC) {
     const int kc = min(KC, S - k0);
     __syncthreads();
-    // column coefficients of this chunk
     for (int e = tid; e < H * KC; e += nt) {
       const int y = e / KC, kk = e % KC;
       float2 v = czero();
@@ -159,65 +152,118 @@ __global__ void __launch_bounds__(256) kspace_kernel(KArgs a, int mode) {
         const int a1 = (ky - g.sy + H) % H, a2 = (y - g.sy + H) % H;
         v = cscale(g.twy[(a1 * a2) % H], g.inv_sqrt_h);
       }
-      coefY[y * KCP + kk] = v;
+      coef[y * KCP + kk] = v;
     }
     __syncthreads();
-    // partial DFT along y: thread per x
-    for (int x = tid; x < W; x += nt) {
+    if (x >= W) continue;
+    for (int c = cs; c < C; c += YD_CG) {
+      const float2* __restrict__ bc = a.b1 + (long long)c * HW + x;
       float2 acc[KC];
 #pragma unroll
       for (int kk = 0; kk < KC; ++kk) acc[kk] = czero();
 #pragma unroll 4
       for (int y = 0; y < H; ++y) {
-        float2 v = u[(long long)y * W + x];
-        if (u2) v = csub(v, u2[(long long)y * W + x]);
-        v = cmul(__ldg(b1 + (long long)y * W + x), v);
-        const float4* cy = reinterpret_cast<const float4*>(coefY + y * KCP);
+        const float2 v = cmul(__ldg(bc + (long long)y * W), su[y * YD_XS + tx]);
+        const float4* cy = reinterpret_cast<const float4*>(coef + y * KCP);
 #pragma unroll
         for (int kk = 0; kk < KC; kk += 2) {
-          float4 q = cy[kk >> 1];
+          const float4 q = cy[kk >> 1];
           cfma(acc[kk], make_float2(q.x, q.y), v);
           cfma(acc[kk + 1], make_float2(q.z, q.w), v);
         }
       }
-      // with the FFT, sequence position n holds x = n + sx (the ifftshift of
-      // the centred transform); the dense DFT indexes x directly
-      const int xs = g.nrad ? (x - g.sx + W) % W : x;
-      float4* pr = reinterpret_cast<float4*>(P + xs * KCP);
+      float2* out = a.qp + kbase(g, t, c, r0, r1) + (long long)k0 * W + x;
 #pragma unroll
-      for (int kk = 0; kk < KC; kk += 2)
-        pr[kk >> 1] = make_float4(acc[kk].x, acc[kk].y, acc[kk + 1].x, acc[kk + 1].y);
+      for (int kk = 0; kk < KC; ++kk)
+        if (kk < kc) out[(long long)kk * W] = acc[kk];
+    }
+  }
+}
+
+size_t ydft_smem_bytes(int H) { return sizeof(float2) * (size_t)H * (YD_XS + KSPACE_KC + 2); }
+
+// ---------------------------------------------------------------------------
+// Row kernel: one CTA per (coil, frame), compact rows in chunks of KC.  For
+// the chunk's y-transformed rows P (from ydft_kernel, in k.qp):
+//   X[k][kx] = 1/sqrt(W) sum_x e^{+2 pi i (kx-sx)(x-sx)/W} P[k][x]
+// which completes the unitary image -> k-space transform of the reference
+// restricted to the kept rows (see oracle/cartesian.py for the sign).  Then,
+// by mode:
+//   0  PD step:   z <- mask * (z + sigma mask X - sigma d) / (1 + sigma/lambda)
+//                 (tgv2.cpp:254-264 followed by the in-place masking of
+//                 ForwardOperation, cartesian_operator.cpp:83-88), and
+//                 Q'[k][x] = 1/sqrt(W) sum_kx e^{-2 pi i ..} z[k][kx] into k.qp
+//   1  step rule: sum |mask X|^2
+//   2  gap:       sum |mask X - d|^2, Re<d,z>, |z|^2, then z <- mask z and Q'
+//   3  apply:     dense_out[t,c,ky,kx] = mask X
+// Each CTA reads and rewrites only its own block of k.qp.
+// ---------------------------------------------------------------------------
+
+template <int KC>
+__global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
+  if (a.st && a.st->stop && mode != 3) return;
+  constexpr int KCP = KC + 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const CartGeomDev& g = a.g;
+  const int W = g.W, C = g.C;
+  const int c = blockIdx.x % C;
+  const int t = blockIdx.x / C;
+  const int r0 = g.row_off[t], r1 = g.row_off[t + 1];
+  const int S = r1 - r0;
+  const long long zb = kbase(g, t, c, r0, r1);
+
+  float2* P = reinterpret_cast<float2*>(smem_raw);  // [W][KCP]
+  float2* X = P + (size_t)W * KCP;                   // [W][KCP]
+  float2* twx = X + (size_t)W * KCP;                 // [W]
+  double* red = reinterpret_cast<double*>(twx + W);  // [32*3]
+
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int j = tid; j < W; j += nt) twx[j] = g.twx[j];
+
+  const float sig = a.st ? (float)a.st->sigma : 0.f;
+  const float zscale = (mode == 0) ? (float)(1.0 / (1.0 + a.st->sigma / (double)a.lam)) : 1.f;
+  double acc_r[3] = {0.0, 0.0, 0.0};
+
+  for (int k0 = 0; k0 < S; k0 += KC) {
+    const int kc = min(KC, S - k0);
+    __syncthreads();
+    // with the FFT, sequence position n holds x = n + sx (the ifftshift of the
+    // centred transform); the dense DFT indexes x directly
+    for (int e = tid; e < KC * W; e += nt) {
+      const int kk = e / W, x = e % W;
+      const int xs = g.nrad ? (x - g.sx + W) % W : x;
+      P[xs * KCP + kk] = kk < kc ? a.qp[zb + (long long)(k0 + kk) * W + x] : czero();
     }
     __syncthreads();
     float2* Xb = X;  // buffer holding the row transform, index (kx - sx) mod W with the FFT
     if (g.nrad) {
       Xb = row_fft<KC>(P, X, twx, W, g.nrad, g.rad, +1);
     } else {
-    // dense DFT along x: thread per kx
-    for (int kx = tid; kx < W; kx += nt) {
-      float2 acc[KC];
+      // dense DFT along x: thread per kx
+      for (int kx = tid; kx < W; kx += nt) {
+        float2 acc[KC];
 #pragma unroll
-      for (int kk = 0; kk < KC; ++kk) acc[kk] = czero();
-      const int step = (kx - g.sx + W) % W;
-      int jj = (step * ((W - g.sx) % W)) % W;  // index for x = 0
-      for (int x = 0; x < W; ++x) {
-        const float2 tw = twx[jj];
-        const float4* pr = reinterpret_cast<const float4*>(P + x * KCP);
+        for (int kk = 0; kk < KC; ++kk) acc[kk] = czero();
+        const int step = (kx - g.sx + W) % W;
+        int jj = (step * ((W - g.sx) % W)) % W;  // index for x = 0
+        for (int x = 0; x < W; ++x) {
+          const float2 tw = twx[jj];
+          const float4* pr = reinterpret_cast<const float4*>(P + x * KCP);
 #pragma unroll
-        for (int kk = 0; kk < KC; kk += 2) {
-          float4 q = pr[kk >> 1];
-          cfma(acc[kk], tw, make_float2(q.x, q.y));
-          cfma(acc[kk + 1], tw, make_float2(q.z, q.w));
+          for (int kk = 0; kk < KC; kk += 2) {
+            float4 q = pr[kk >> 1];
+            cfma(acc[kk], tw, make_float2(q.x, q.y));
+            cfma(acc[kk + 1], tw, make_float2(q.z, q.w));
+          }
+          jj += step;
+          if (jj >= W) jj -= W;
         }
-        jj += step;
-        if (jj >= W) jj -= W;
-      }
-      float4* xr = reinterpret_cast<float4*>(X + kx * KCP);
+        float4* xr = reinterpret_cast<float4*>(X + kx * KCP);
 #pragma unroll
-      for (int kk = 0; kk < KC; kk += 2)
-        xr[kk >> 1] = make_float4(acc[kk].x, acc[kk].y, acc[kk + 1].x, acc[kk + 1].y);
-    }
-    __syncthreads();
+        for (int kk = 0; kk < KC; kk += 2)
+          xr[kk >> 1] = make_float4(acc[kk].x, acc[kk].y, acc[kk + 1].x, acc[kk + 1].y);
+      }
+      __syncthreads();
     }
     // pointwise stage on the kept samples; Xb[n] holds kx = n + sx (FFT) or kx
     for (int e = tid; e < kc * W; e += nt) {
@@ -249,7 +295,7 @@ __global__ void __launch_bounds__(256) kspace_kernel(KArgs a, int mode) {
         Xb[n * KCP + kk] = zm;
       } else {
         const int ky = g.rows[r0 + k0 + kk];
-        a.dense_out[(((long long)t * C + c) * H + ky) * W + kx] = mX;
+        a.dense_out[(((long long)t * C + c) * g.H + ky) * W + kx] = mX;
       }
     }
     if (mode == 1 || mode == 3) continue;
@@ -284,8 +330,9 @@ __global__ void __launch_bounds__(256) kspace_kernel(KArgs a, int mode) {
         jj += step;
         if (jj >= W) jj -= W;
       }
-      for (int kk = 0; kk < kc; ++kk)
-        a.qp[zb + (long long)(k0 + kk) * W + x] = cscale(acc[kk], g.inv_sqrt_w);
+#pragma unroll
+      for (int kk = 0; kk < KC; ++kk)
+        if (kk < kc) a.qp[zb + (long long)(k0 + kk) * W + x] = cscale(acc[kk], g.inv_sqrt_w);
     }
   }
   if (mode == 1 || mode == 2) {
@@ -299,116 +346,111 @@ __global__ void __launch_bounds__(256) kspace_kernel(KArgs a, int mode) {
   }
 }
 
-size_t kspace_smem_bytes(int W, int H) {
+size_t rows_smem_bytes(int W) {
   const int KCP = KSPACE_KC + 2;
-  return sizeof(float2) * ((size_t)H * KCP + 2 * (size_t)W * KCP + W) + sizeof(double) * 32 * 3;
+  return sizeof(float2) * (2 * (size_t)W * KCP + W) + sizeof(double) * 32 * 3;
 }
 
+size_t kspace_smem_bytes(int W, int H) { return std::max(ydft_smem_bytes(H), rows_smem_bytes(W)); }
+
 // ---------------------------------------------------------------------------
-// Column adjoint of the compact rows for a 32 x 16 pixel tile of frame t:
-//   acc[y,x] = sum_c conj(b1[c,y,x]) 1/sqrt(H) sum_k e^{-2 pi i (ky_k-sy)(y-sy)/H} Q'[t,c,k,x]
-// which completes K^H (cartesian_operator.cpp:65-111) from Q'.
+// Column adjoint of the compact rows (completes K^H, cartesian_operator.cpp:65-111):
+//   img[t,y,x] = sum_c conj(b1[c,y,x]) 1/sqrt(H) sum_k e^{-2 pi i (ky_k-sy)(y-sy)/H} Q'[t,c,k,x]
+// CTA tile 2 CA_TX columns x CA_TY CA_YP rows of frame t; thread (tx, ty)
+// owns columns x0+tx, x0+tx+CA_TX and rows y0+ty*CA_YP .. +CA_YP-1, a 2 x
+// CA_YP register tile.  Coefficients are staged per chunk of CA_KQ rows;
+// Q' is read from global memory (L2 resident), one value per column and row.
 // ---------------------------------------------------------------------------
 
-struct __align__(16) AdjSmem {
-  float2 q[ADJ_KQ * ADJ_TX];
-  float2 cf[ADJ_KQ * ADJ_TH];
-};
-
-AVX_D void adjoint_tile(const KArgs& k, int t, int x0, int y0, float2 (&acc)[ADJ_YP], AdjSmem& sm) {
+__global__ void __launch_bounds__(CA_TX* CA_TY) coladj_kernel(KArgs k, float2* img) {
+  if (k.st && k.st->stop) return;
+  constexpr int TH = CA_TY * CA_YP;
+  __shared__ __align__(16) float2 sg[CA_KQ * TH];  // [kk][y] conjugated coefficients
   const CartGeomDev& g = k.g;
-  const int W = g.W, H = g.H;
+  const int W = g.W, H = g.H, C = g.C;
+  const int t = blockIdx.z;
+  const int x0 = blockIdx.x * 2 * CA_TX, y0 = blockIdx.y * TH;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int tid = tx + ADJ_TX * ty;
-  const int nthr = ADJ_TX * ADJ_TY;
+  const int tid = tx + CA_TX * ty, nt = CA_TX * CA_TY;
   const int r0 = g.row_off[t], r1 = g.row_off[t + 1];
   const int S = r1 - r0;
-  const int x = x0 + tx;
   const long long HW = (long long)W * H;
+  const int xa = x0 + tx, xb = x0 + tx + CA_TX;
+  const bool va = xa < W, vb = xb < W;
+  float2 acc[2][CA_YP];
 #pragma unroll
-  for (int j = 0; j < ADJ_YP; ++j) acc[j] = czero();
-  for (int c = 0; c < g.C; ++c) {
-    float2 racc[ADJ_YP];
+  for (int j = 0; j < CA_YP; ++j) acc[0][j] = acc[1][j] = czero();
+  for (int k0 = 0; k0 < S; k0 += CA_KQ) {
+    const int kc = min(CA_KQ, S - k0);
+    __syncthreads();
+    for (int e = tid; e < CA_KQ * TH; e += nt) {
+      const int kk = e / TH, yy = e % TH;
+      float2 v = czero();
+      if (kk < kc && y0 + yy < H) {
+        const int ky = g.rows[r0 + k0 + kk];
+        const int a1 = (ky - g.sy + H) % H, a2 = (y0 + yy - g.sy + H) % H;
+        const float2 w = g.twy[(a1 * a2) % H];
+        v = make_float2(w.x * g.inv_sqrt_h, -w.y * g.inv_sqrt_h);
+      }
+      sg[e] = v;
+    }
+    __syncthreads();
+    for (int c = 0; c < C; ++c) {
+      const float2* __restrict__ q = k.qp + kbase(g, t, c, r0, r1) + (long long)k0 * W;
+      float2 racc[2][CA_YP];
 #pragma unroll
-    for (int j = 0; j < ADJ_YP; ++j) racc[j] = czero();
-    const long long base = kbase(g, t, c, r0, r1);
-    for (int k0 = 0; k0 < S; k0 += ADJ_KQ) {
-      const int kc = min(ADJ_KQ, S - k0);
-      __syncthreads();
-      for (int e = tid; e < ADJ_KQ * ADJ_TX; e += nthr) {
-        const int kk = e / ADJ_TX, xx = e % ADJ_TX;
-        sm.q[e] = (kk < kc && x0 + xx < W) ? k.qp[base + (long long)(k0 + kk) * W + x0 + xx] : czero();
-      }
-      for (int e = tid; e < ADJ_KQ * ADJ_TH; e += nthr) {
-        const int kk = e / ADJ_TH, yy = e % ADJ_TH;
-        float2 v = czero();
-        if (kk < kc && y0 + yy < H) {
-          const int ky = g.rows[r0 + k0 + kk];
-          const int a1 = (ky - g.sy + H) % H, a2 = (y0 + yy - g.sy + H) % H;
-          const float2 w = g.twy[(a1 * a2) % H];
-          v = make_float2(w.x * g.inv_sqrt_h, -w.y * g.inv_sqrt_h);
-        }
-        sm.cf[e] = v;
-      }
-      __syncthreads();
+      for (int j = 0; j < CA_YP; ++j) racc[0][j] = racc[1][j] = czero();
+#pragma unroll 4
       for (int kk = 0; kk < kc; ++kk) {
-        const float2 q = sm.q[kk * ADJ_TX + tx];
-        const float4* cf4 = reinterpret_cast<const float4*>(sm.cf + kk * ADJ_TH + ty * ADJ_YP);
+        const float2 qa = va ? __ldg(q + (long long)kk * W + xa) : czero();
+        const float2 qb = vb ? __ldg(q + (long long)kk * W + xb) : czero();
+        const float4* gy = reinterpret_cast<const float4*>(sg + kk * TH + ty * CA_YP);
 #pragma unroll
-        for (int j = 0; j < ADJ_YP; j += 2) {
-          const float4 c2 = cf4[j >> 1];
-          cfma(racc[j], make_float2(c2.x, c2.y), q);
-          cfma(racc[j + 1], make_float2(c2.z, c2.w), q);
+        for (int j = 0; j < CA_YP; j += 2) {
+          const float4 c2 = gy[j >> 1];
+          const float2 g0 = make_float2(c2.x, c2.y), g1 = make_float2(c2.z, c2.w);
+          cfma(racc[0][j], g0, qa);
+          cfma(racc[0][j + 1], g1, qa);
+          cfma(racc[1][j], g0, qb);
+          cfma(racc[1][j + 1], g1, qb);
         }
       }
-    }
-    if (x < W) {
+      const float2* __restrict__ bc = k.b1 + (long long)c * HW;
 #pragma unroll
-      for (int j = 0; j < ADJ_YP; ++j) {
-        const int y = y0 + ty * ADJ_YP + j;
-        if (y < H) acc[j] = cadd(acc[j], cmulc(__ldg(k.b1 + c * HW + (long long)y * W + x), racc[j]));
+      for (int j = 0; j < CA_YP; ++j) {
+        const int y = y0 + ty * CA_YP + j;
+        if (y >= H) break;
+        if (va) acc[0][j] = cadd(acc[0][j], cmulc(__ldg(bc + (long long)y * W + xa), racc[0][j]));
+        if (vb) acc[1][j] = cadd(acc[1][j], cmulc(__ldg(bc + (long long)y * W + xb), racc[1][j]));
       }
     }
   }
-}
-
-// k-space -> image (operator apply): img[t] = K^H from Q'.
-__global__ void __launch_bounds__(ADJ_TX* ADJ_TY) adjoint_kernel(KArgs k, float2* img) {
-  __shared__ AdjSmem sm;
-  const int t = blockIdx.z;
-  const int x0 = blockIdx.x * ADJ_TX, y0 = blockIdx.y * ADJ_TH;
-  float2 acc[ADJ_YP];
-  adjoint_tile(k, t, x0, y0, acc, sm);
-  const int x = x0 + threadIdx.x;
-  if (x >= k.g.W) return;
+  float2* out = img + (long long)t * HW;
 #pragma unroll
-  for (int j = 0; j < ADJ_YP; ++j) {
-    const int y = y0 + threadIdx.y * ADJ_YP + j;
-    if (y < k.g.H) img[((long long)t * k.g.H + y) * k.g.W + x] = acc[j];
+  for (int j = 0; j < CA_YP; ++j) {
+    const int y = y0 + ty * CA_YP + j;
+    if (y >= H) break;
+    if (va) out[(long long)y * W + xa] = acc[0][j];
+    if (vb) out[(long long)y * W + xb] = acc[1][j];
   }
 }
 
 // ---------------------------------------------------------------------------
-// primal update fused with K^H z
+// primal update; K^H z is read from the image a.khz (column adjoint or
+// gridding adjoint)
 // ---------------------------------------------------------------------------
 
-template <int M, bool CART>
-__global__ void __launch_bounds__(ADJ_TX* ADJ_TY) primal_kernel(PDArgs a, KArgs k) {
+template <int M>
+__global__ void __launch_bounds__(ADJ_TX* ADJ_TY) primal_kernel(PDArgs a) {
   if (a.st->stop) return;
-  __shared__ AdjSmem sm;
   const int t = blockIdx.z;
   const int x0 = blockIdx.x * ADJ_TX, y0 = blockIdx.y * ADJ_TH;
   float2 kh[ADJ_YP];
-  if (CART) {
-    adjoint_tile(k, t, x0, y0, kh, sm);
-  } else {
-    // K^H z supplied as an image by the operator (radial)
 #pragma unroll
-    for (int j = 0; j < ADJ_YP; ++j) {
-      const int y = y0 + threadIdx.y * ADJ_YP + j;
-      const int x = x0 + threadIdx.x;
-      kh[j] = (x < a.W && y < a.H) ? a.khz[((long long)t * a.H + y) * a.W + x] : czero();
-    }
+  for (int j = 0; j < ADJ_YP; ++j) {
+    const int y = y0 + threadIdx.y * ADJ_YP + j;
+    const int x = x0 + threadIdx.x;
+    kh[j] = (x < a.W && y < a.H) ? a.khz[((long long)t * a.H + y) * a.W + x] : czero();
   }
   const int x = x0 + threadIdx.x;
   if (x >= a.W) return;
@@ -568,28 +610,23 @@ __global__ void step_finalize_kernel(DevState* st, const double* pimg, int nimg,
 }
 
 // ---------------------------------------------------------------------------
-// primal-dual gap, image side (needs K^H z from a fresh Q').
+// primal-dual gap, image side (needs a fresh K^H z image in a.khz).
 // slots: 0 g3 = |K^H z - div y1|_1, 1 g4, 2 g5, 3 g6,
 //        4..7 regulariser L1 sums n1..n4 (see gap_finalize_kernel)
 // ---------------------------------------------------------------------------
 
-template <int M, bool CART>
-__global__ void __launch_bounds__(ADJ_TX* ADJ_TY) gap_img_kernel(PDArgs a, KArgs k, double* partial) {
+template <int M>
+__global__ void __launch_bounds__(ADJ_TX* ADJ_TY) gap_img_kernel(PDArgs a, double* partial) {
   if (a.st->stop) return;
-  __shared__ AdjSmem sm;
   __shared__ double red[32 * 8];
   const int t = blockIdx.z;
   const int x0 = blockIdx.x * ADJ_TX, y0 = blockIdx.y * ADJ_TH;
   float2 kh[ADJ_YP];
-  if (CART) {
-    adjoint_tile(k, t, x0, y0, kh, sm);
-  } else {
 #pragma unroll
-    for (int j = 0; j < ADJ_YP; ++j) {
-      const int y = y0 + threadIdx.y * ADJ_YP + j;
-      const int x = x0 + threadIdx.x;
-      kh[j] = (x < a.W && y < a.H) ? a.khz[((long long)t * a.H + y) * a.W + x] : czero();
-    }
+  for (int j = 0; j < ADJ_YP; ++j) {
+    const int y = y0 + threadIdx.y * ADJ_YP + j;
+    const int x = x0 + threadIdx.x;
+    kh[j] = (x < a.W && y < a.H) ? a.khz[((long long)t * a.H + y) * a.W + x] : czero();
   }
   double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const int x = x0 + threadIdx.x;
@@ -665,7 +702,7 @@ __global__ void gap_finalize_kernel(DevState* st, const double* pk, int nk, cons
   block_sum<11>(v, red);
   if (threadIdx.x != 0) return;
   const double lam = gc.lam;
-  const double res2 = v[0] + gc.d_off_energy;
+  const double res2 = v[0] + st->d_off;
   const double g1 = 0.5 * lam * res2;
   const double g2 = v[1] + v[2] / (2.0 * lam);
   const double g36 = v[3] + v[4] + v[5] + v[6];
@@ -754,34 +791,8 @@ __global__ void dense_rowidft_kernel(CartGeomDev g, float2* dense, float2* qp, c
 // explicit template instantiations and launch helpers
 // ---------------------------------------------------------------------------
 
-template <int M>
-static void launch_iteration_impl(const PDArgs& a, const KArgs& k, cudaStream_t s) {
-  const int HW = a.W * a.H;
-  dim3 gd((HW + 255) / 256, a.T);
-  dual_kernel<M><<<gd, 256, 0, s>>>(a);
-  kspace_kernel<KSPACE_KC><<<k.g.C * k.g.T, 256, kspace_smem_bytes(a.W, a.H), s>>>(k, 0);
-  dim3 gp((a.W + ADJ_TX - 1) / ADJ_TX, (a.H + ADJ_TH - 1) / ADJ_TH, a.T);
-  primal_kernel<M, true><<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(a, k);
-}
-
-void launch_iteration(int method, const PDArgs& a, const KArgs& k, cudaStream_t s) {
-  if (method == AVX_M_TV) launch_iteration_impl<AVX_M_TV>(a, k, s);
-  else if (method == AVX_M_TGV2) launch_iteration_impl<AVX_M_TGV2>(a, k, s);
-  else launch_iteration_impl<AVX_M_ICTGV2>(a, k, s);
-}
-
-void launch_primal(int method, const PDArgs& a, const KArgs& k, cudaStream_t s, bool cart) {
-  dim3 gp((a.W + ADJ_TX - 1) / ADJ_TX, (a.H + ADJ_TH - 1) / ADJ_TH, a.T);
-  dim3 bl(ADJ_TX, ADJ_TY);
-  if (cart) {
-    if (method == AVX_M_TV) primal_kernel<AVX_M_TV, true><<<gp, bl, 0, s>>>(a, k);
-    else if (method == AVX_M_TGV2) primal_kernel<AVX_M_TGV2, true><<<gp, bl, 0, s>>>(a, k);
-    else primal_kernel<AVX_M_ICTGV2, true><<<gp, bl, 0, s>>>(a, k);
-  } else {
-    if (method == AVX_M_TV) primal_kernel<AVX_M_TV, false><<<gp, bl, 0, s>>>(a, k);
-    else if (method == AVX_M_TGV2) primal_kernel<AVX_M_TGV2, false><<<gp, bl, 0, s>>>(a, k);
-    else primal_kernel<AVX_M_ICTGV2, false><<<gp, bl, 0, s>>>(a, k);
-  }
+static void rec(cudaEvent_t* ev, int i, cudaStream_t s) {
+  if (ev) cudaEventRecord(ev[i], s);
 }
 
 void launch_dual(int method, const PDArgs& a, cudaStream_t s) {
@@ -791,13 +802,45 @@ void launch_dual(int method, const PDArgs& a, cudaStream_t s) {
   else dual_kernel<AVX_M_ICTGV2><<<gd, 256, 0, s>>>(a);
 }
 
+void launch_primal(int method, const PDArgs& a, cudaStream_t s) {
+  dim3 gp((a.W + ADJ_TX - 1) / ADJ_TX, (a.H + ADJ_TH - 1) / ADJ_TH, a.T);
+  dim3 bl(ADJ_TX, ADJ_TY);
+  if (method == AVX_M_TV) primal_kernel<AVX_M_TV><<<gp, bl, 0, s>>>(a);
+  else if (method == AVX_M_TGV2) primal_kernel<AVX_M_TGV2><<<gp, bl, 0, s>>>(a);
+  else primal_kernel<AVX_M_ICTGV2><<<gp, bl, 0, s>>>(a);
+}
+
+void launch_ydft(const KArgs& k, cudaStream_t s) {
+  dim3 gr((k.g.W + YD_XS - 1) / YD_XS, k.g.T);
+  ydft_kernel<KSPACE_KC><<<gr, dim3(YD_XS, YD_CG), ydft_smem_bytes(k.g.H), s>>>(k);
+}
+
+void launch_rows(const KArgs& k, int mode, cudaStream_t s) {
+  rows_kernel<KSPACE_KC><<<k.g.C * k.g.T, 256, rows_smem_bytes(k.g.W), s>>>(k, mode);
+}
+
 void launch_kspace(const KArgs& k, int mode, cudaStream_t s) {
-  kspace_kernel<KSPACE_KC><<<k.g.C * k.g.T, 256, kspace_smem_bytes(k.g.W, k.g.H), s>>>(k, mode);
+  launch_ydft(k, s);
+  launch_rows(k, mode, s);
 }
 
 void launch_adjoint(const KArgs& k, float2* img, cudaStream_t s) {
-  dim3 gp((k.g.W + ADJ_TX - 1) / ADJ_TX, (k.g.H + ADJ_TH - 1) / ADJ_TH, k.g.T);
-  adjoint_kernel<<<gp, dim3(ADJ_TX, ADJ_TY), 0, s>>>(k, img);
+  dim3 gr((k.g.W + 2 * CA_TX - 1) / (2 * CA_TX), (k.g.H + CA_TY * CA_YP - 1) / (CA_TY * CA_YP), k.g.T);
+  coladj_kernel<<<gr, dim3(CA_TX, CA_TY), 0, s>>>(k, img);
+}
+
+void launch_iteration(int method, const PDArgs& a, const KArgs& k, float2* khz, cudaStream_t s, cudaEvent_t* ev) {
+  rec(ev, 0, s);
+  launch_dual(method, a, s);
+  rec(ev, 1, s);
+  launch_ydft(k, s);
+  rec(ev, 2, s);
+  launch_rows(k, 0, s);
+  rec(ev, 3, s);
+  launch_adjoint(k, khz, s);
+  rec(ev, 4, s);
+  launch_primal(method, a, s);
+  rec(ev, 5, s);
 }
 
 int gap_img_blocks(int W, int H, int T) {
@@ -818,19 +861,19 @@ void launch_step_finalize(const PDArgs& a, double* pimg, double* pk, int nk, dou
 void launch_step(int method, const PDArgs& a, const KArgs& k_e, const Ptr8& e_dev, int P,
                  double* pimg, double* pk, double ratio, cudaStream_t s) {
   launch_step_img(method, a, e_dev, P, pimg, s);
-  kspace_kernel<KSPACE_KC><<<k_e.g.C * k_e.g.T, 256, kspace_smem_bytes(k_e.g.W, k_e.g.H), s>>>(k_e, 1);
+  launch_kspace(k_e, 1, s);
   launch_step_finalize(a, pimg, pk, k_e.g.C * k_e.g.T, ratio, s);
 }
 
 void launch_gap_tail(int method, const PDArgs& a, const KArgs& k_x, double* pimg, double* pk, int nk,
-                     const GapConst& gc, double* hg, double* hn, double* hf, int cap, int init_only, bool cart,
+                     const GapConst& gc, double* hg, double* hn, double* hf, int cap, int init_only,
                      cudaStream_t s) {
+  (void)k_x;
   dim3 gp((a.W + ADJ_TX - 1) / ADJ_TX, (a.H + ADJ_TH - 1) / ADJ_TH, a.T);
   dim3 bl(ADJ_TX, ADJ_TY);
   const int nimg = gap_img_blocks(a.W, a.H, a.T);
-#define GAP_IMG(MM)                                                        \
-  if (cart) gap_img_kernel<MM, true><<<gp, bl, 0, s>>>(a, k_x, pimg);     \
-  else gap_img_kernel<MM, false><<<gp, bl, 0, s>>>(a, k_x, pimg);         \
+#define GAP_IMG(MM)                                              \
+  gap_img_kernel<MM><<<gp, bl, 0, s>>>(a, pimg);                \
   gap_finalize_kernel<MM><<<1, 256, 0, s>>>(a.st, pk, nk, pimg, nimg, gc, hg, hn, hf, cap, init_only);
   if (method == AVX_M_TV) {
     GAP_IMG(AVX_M_TV)
@@ -842,10 +885,13 @@ void launch_gap_tail(int method, const PDArgs& a, const KArgs& k_x, double* pimg
 #undef GAP_IMG
 }
 
-void launch_gap(int method, const PDArgs& a, const KArgs& k_x, double* pimg, double* pk, const GapConst& gc,
-                double* hg, double* hn, double* hf, int cap, int init_only, cudaStream_t s) {
-  kspace_kernel<KSPACE_KC><<<k_x.g.C * k_x.g.T, 256, kspace_smem_bytes(k_x.g.W, k_x.g.H), s>>>(k_x, 2);
-  launch_gap_tail(method, a, k_x, pimg, pk, k_x.g.C * k_x.g.T, gc, hg, hn, hf, cap, init_only, true, s);
+void launch_gap(int method, const PDArgs& a, const KArgs& k_x, float2* khz, double* pimg, double* pk,
+                const GapConst& gc, double* hg, double* hn, double* hf, int cap, int init_only, cudaStream_t s) {
+  launch_kspace(k_x, 2, s);
+  launch_adjoint(k_x, khz, s);
+  PDArgs ag = a;
+  ag.khz = khz;
+  launch_gap_tail(method, ag, k_x, pimg, pk, k_x.g.C * k_x.g.T, gc, hg, hn, hf, cap, init_only, s);
 }
 
 void launch_gather_rows(const CartGeomDev& g, const float2* dense, float2* compact, int apply_mask, cudaStream_t s) {
@@ -858,7 +904,9 @@ void launch_dense_rowidft(const CartGeomDev& g, float2* dense, float2* qp, const
 
 cudaError_t configure_kernels() {
   // opt in to the full 227 KB of dynamic shared memory per CTA (sm_100)
-  return cudaFuncSetAttribute(kspace_kernel<KSPACE_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(ydft_kernel<KSPACE_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(rows_kernel<KSPACE_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 }
 
 }  // namespace avx

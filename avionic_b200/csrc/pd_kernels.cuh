@@ -3,12 +3,20 @@
 
 #include "pd_args.cuh"
 
-#define KSPACE_KC 16  // compact k-space rows per chunk in kspace_kernel
-#define ADJ_TX 32     // tile width (x) of the column-adjoint / primal kernels
+#define KSPACE_KC 16  // compact k-space rows per chunk (y-transform and row kernels)
+#define YD_XS 16      // image columns per CTA of the y-transform
+#define YD_CG 16      // coil slots per CTA of the y-transform
+#define CA_TX 16      // column-adjoint threads along x (two columns each, 16 apart)
+#define CA_TY 8       // column-adjoint threads along y
+#define CA_YP 8       // column-adjoint rows per thread
+#define CA_KQ 32      // compact rows per coefficient chunk of the column adjoint
+#define ADJ_TX 32     // tile width (x) of the primal / gap kernels
 #define ADJ_TY 4      // thread rows per tile
 #define ADJ_YP 4      // pixels per thread along y
 #define ADJ_TH (ADJ_TY * ADJ_YP)
-#define ADJ_KQ 32     // compact rows staged per chunk in the adjoint
+
+// timed stages of one iteration (avx_solver_kernel_times)
+#define AVX_NSTAGE 5
 
 namespace avx {
 
@@ -17,28 +25,35 @@ struct Ptr8 {
 };
 
 struct GapConst {
-  double lam, d_off_energy, N, stop_gap;
+  double lam, N, stop_gap;  // the data-energy constant is DevState::d_off
   double alpha0, alpha1, ic_a, ic_b;
 };
 
-size_t kspace_smem_bytes(int W, int H);
+size_t kspace_smem_bytes(int W, int H);  // largest dynamic shared memory of the transform kernels
 int gap_img_blocks(int W, int H, int T);
 cudaError_t configure_kernels();
 
-void launch_iteration(int method, const PDArgs& a, const KArgs& k, cudaStream_t s);
+// one Cartesian iteration: dual, y-transform, rows, column adjoint, primal;
+// ev (optional) receives AVX_NSTAGE + 1 events around the stages
+void launch_iteration(int method, const PDArgs& a, const KArgs& k, float2* khz, cudaStream_t s,
+                      cudaEvent_t* ev = nullptr);
 void launch_dual(int method, const PDArgs& a, cudaStream_t s);
-void launch_primal(int method, const PDArgs& a, const KArgs& k, cudaStream_t s, bool cart = true);
+void launch_primal(int method, const PDArgs& a, cudaStream_t s);
+void launch_ydft(const KArgs& k, cudaStream_t s);
+void launch_rows(const KArgs& k, int mode, cudaStream_t s);
 void launch_step_img(int method, const PDArgs& a, const Ptr8& e_dev, int P, double* pimg, cudaStream_t s);
 void launch_step_finalize(const PDArgs& a, double* pimg, double* pk, int nk, double ratio, cudaStream_t s);
 void launch_gap_tail(int method, const PDArgs& a, const KArgs& k_x, double* pimg, double* pk, int nk,
-                     const GapConst& gc, double* hg, double* hn, double* hf, int cap, int init_only, bool cart,
+                     const GapConst& gc, double* hg, double* hn, double* hf, int cap, int init_only,
                      cudaStream_t s);
+// y-transform followed by the row kernel in the given mode (0 PD step, 1 step-rule norm, 2 gap, 3 apply)
 void launch_kspace(const KArgs& k, int mode, cudaStream_t s);
+// img[t] = sum_c conj(b1_c) column-IDFT of the compact rows in k.qp
 void launch_adjoint(const KArgs& k, float2* img, cudaStream_t s);
 void launch_step(int method, const PDArgs& a, const KArgs& k_e, const Ptr8& e_dev, int P,
                  double* pimg, double* pk, double ratio, cudaStream_t s);
-void launch_gap(int method, const PDArgs& a, const KArgs& k_x, double* pimg, double* pk, const GapConst& gc,
-                double* hg, double* hn, double* hf, int cap, int init_only, cudaStream_t s);
+void launch_gap(int method, const PDArgs& a, const KArgs& k_x, float2* khz, double* pimg, double* pk,
+                const GapConst& gc, double* hg, double* hn, double* hf, int cap, int init_only, cudaStream_t s);
 void launch_gather_rows(const CartGeomDev& g, const float2* dense, float2* compact, int apply_mask,
                         cudaStream_t s);
 void launch_dense_rowidft(const CartGeomDev& g, float2* dense, float2* qp, const float* mask_dense,

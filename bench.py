@@ -54,18 +54,23 @@ def cfg_params(av):
 
 
 def algorithmic_bytes(W, H, T, C, R):
-    """Compulsory bytes per ICTGV2 iteration by kernel (complex64 = 8 B).
-    N = W*H*T pixels; S = C*R*W sampled k-space values (R compact rows)."""
+    """Compulsory bytes per ICTGV2 iteration by stage (complex64 = 8 B).
+    N = W*H*T pixels; S = C*R*W compact k-space values (R sampled rows over
+    all frames)."""
     N = W * H * T
     S = C * R * W
     P, D = 8, 18
     return {
         # read xbar (P), read + write y (2D)
         "dual": 8 * N * (P + 2 * D),
-        # read xbar1 + b1, read z, d, write z, Q'
-        "kspace": 8 * (N + C * W * H) + 8 * 4 * S + 4 * R * W,
-        # read Q', b1, x (P), y (D); write x, xbar (2P)
-        "primal": 8 * S + 8 * C * W * H + 8 * N * (3 * P + D),
+        # read xbar1, b1; write the y-transformed rows
+        "ydft": 8 * N + 8 * C * W * H + 8 * S,
+        # read rows, z, d, mask; write z, Q'
+        "rows": 8 * 5 * S + 4 * R * W,
+        # read Q', b1; write K^H z
+        "coladj": 8 * S + 8 * C * W * H + 8 * N,
+        # read K^H z, x (P), y (D); write x, xbar (2P)
+        "primal": 8 * N * (1 + 3 * P + D),
         # the whole iteration, the formula of the scope table: 8 [4PN + 2DN + 3CS] + 8 C W H + 4 S
         "iteration": 8 * (4 * P * N + 2 * D * N + 3 * S) + 8 * C * W * H + 4 * R * W,
     }
@@ -250,8 +255,8 @@ def main():
     solver.set_debug(False, 0)
     R = int(np.count_nonzero(prob["mask"].any(axis=2)))
 
-    # warm-up (graphs are not used in timing mode; kernels and buffers are set up here)
-    solver.set_timing(True)
+    # warm-up: kernels, buffers and the CUDA graphs of the iteration shapes are set up here
+    solver.set_timing(False)
     for _ in range(args.warmup):
         x.copy_(x0)
         solver.run(kd, x, b1)
@@ -262,7 +267,6 @@ def main():
     torch.cuda.synchronize()
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    kt = np.zeros(3)
     launches = 0
     lat = []
     e0.record()
@@ -274,8 +278,6 @@ def main():
         s1 = torch.cuda.Event(enable_timing=True)
         s1.record()
         lat.append((s0, s1))
-        t, n = solver.kernel_times()
-        kt += np.array(t)
         launches += solver.stats().kernel_launches + 3  # + row gather and two set-up reductions
     e1.record()
     torch.cuda.synchronize()
@@ -288,21 +290,34 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
     value = world * args.steps * ITERS / (ms / 1000.0)
-    kmean = kt / args.steps
+
+    # per-stage durations: one more reconstruction with CUDA events between the
+    # stages of every iteration (kernels launched directly, not from graphs)
+    solver.set_timing(True)
+    x.copy_(x0)
+    solver.run(kd, x, b1)
+    torch.cuda.synchronize()
+    t_stage, n_timed = solver.kernel_times()
+    solver.set_timing(False)
+    kmean = np.array(t_stage)
 
     # roofline of the dominant kernel (largest mean duration per iteration)
     ab = algorithmic_bytes(W, H, T, C, R)
-    names = ["dual", "kspace", "primal"]
+    names = ["dual", "ydft", "rows", "coladj", "primal"]
     dom = int(np.argmax(kmean))
     peak, peak_kind = load_peaks()
     achieved = ab[names[dom]] / (kmean[dom] / 1000.0) / 1e9
     traffic = load_traffic().get(names[dom])
     iter_ms = float(np.sum(kmean))
-    roof = {"bound": "hbm", "kernel": names[dom] + "_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
+    kern = {"dual": "dual_kernel", "ydft": "ydft_kernel", "rows": "rows_kernel", "coladj": "coladj_kernel",
+            "primal": "primal_kernel"}
+    roof = {"bound": "hbm", "kernel": kern[names[dom]], "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"
             if peak_kind == "measured" else "fallback 6650 GB/s", "traffic": traffic,
             "algorithmic_bytes_per_launch": ab[names[dom]],
             "kernel_ms": {n: float(kmean[i]) for i, n in enumerate(names)},
+            "kernel_ms_source": "CUDA events around each stage, %d iterations of one extra reconstruction "
+                                "after the timed region" % n_timed,
             "iteration_algorithmic_bytes": ab["iteration"],
             "iteration_frac": ab["iteration"] / (iter_ms / 1000.0) / 1e9 / peak}
 
@@ -338,6 +353,7 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ems = float(tt.item())
     e2e_value = world * args.steps * ITERS / (ems / 1000.0)
+    av.lib.avx_reconstruct_host_release()
     h2d = pk.numel() * 8 + pm.numel() * 4 + pb.numel() * 8 + pu.numel() * 8
     d2h = px.numel() * 8
 
@@ -361,7 +377,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (complex64)", "data": "synthetic",
         "config": {"workload": WORKLOAD, "parallelism": "one independent reconstruction per GPU",
-                   "l2": "inputs larger than L2 (working set ~0.4 GB per GPU)", "graphs": False,
+                   "l2": "inputs larger than L2 (working set ~0.4 GB per GPU)", "graphs": True,
                    "recons_per_s": value / ITERS,
                    "recon_latency_ms": {"p50": float(np.percentile(step_ms, 50)),
                                         "p99": float(np.percentile(step_ms, 99))}},

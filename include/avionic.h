@@ -193,11 +193,19 @@ avx_status avx_solver_compute_gap(avx_solver* s, const avx_cf32* const* d_x, con
 avx_status avx_solver_export(avx_solver* s, const char* output_dir, avx_export_cb cb, void* user);
 avx_status avx_solver_get_stats(const avx_solver* s, avx_run_stats* stats);
 
-/* Per-kernel timing: with timing on, a run launches its kernels directly
- * (not from CUDA graphs) with CUDA events around the dual, k-space and primal
- * kernels of every iteration on the solver's stream.  avx_solver_kernel_times
- * returns their mean durations in ms of the last run ([0] dual, [1] k-space,
- * [2] primal) and how many launches of each were timed. */
+/* Per-stage timing: with timing on, a run launches its kernels directly
+ * (not from CUDA graphs) with CUDA events between the five stages of every
+ * iteration on the solver's stream.  avx_solver_kernel_times writes the mean
+ * durations in ms of the last run to mean_ms[0..4]:
+ *   [0] dual update
+ *   [1] forward transform: y-DFT of b1 x onto the sampled rows (Cartesian),
+ *       zero-pad + oversampled FFT (radial)
+ *   [2] k-space: row FFT, data prox, inverse row FFT (Cartesian),
+ *       interpolation + data prox (radial)
+ *   [3] adjoint: column IDFT + coil combine (Cartesian), spreading + FFT +
+ *       crop (radial)
+ *   [4] primal update
+ * and to *count how many iterations were timed. */
 avx_status avx_solver_set_timing(avx_solver* s, int on);
 avx_status avx_solver_kernel_times(const avx_solver* s, float* mean_ms, unsigned* count);
 void avx_solver_destroy(avx_solver* s);
@@ -319,11 +327,19 @@ avx_status avx_coil_construction_radial(unsigned W, unsigned H, unsigned C, unsi
  * replicates u0 over the frames (main.cpp:775-779), runs the method and
  * copies the image back.  h_mask may be NULL (all ones); h_u0 is one frame
  * (W*H) or NULL (zeros).  debugstep > 0 enables the gap history
- * (options_parser.cpp:79).  stats may be NULL. */
+ * (options_parser.cpp:79).  stats may be NULL.  The operator, solver,
+ * device buffers and CUDA graphs of the last call are kept and reused while
+ * the device, method, sizes, parameters, debug step and mask contents stay
+ * the same (calls are serialised by a lock); every call copies the data,
+ * coil maps and u0 and starts from the given parameters.  No reference
+ * counterpart: the reference's main builds everything per run. */
 avx_status avx_reconstruct_host(int method, unsigned width, unsigned height, unsigned coils, unsigned frames,
                                 const avx_pd_params* params, int debugstep, const avx_cf32* h_kdata,
                                 const float* h_mask, const avx_cf32* h_b1, const avx_cf32* h_u0,
                                 avx_cf32* h_x, avx_run_stats* stats);
+
+/* Frees the state kept by avx_reconstruct_host (no reference counterpart). */
+void avx_reconstruct_host_release(void);
 
 #ifdef __cplusplus
 }

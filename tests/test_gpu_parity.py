@@ -181,3 +181,32 @@ def test_reconstruct_host_matches_device_path(av):
     xo, _, _ = _oracle_run("TGV2", prob, 60)
     assert rel(x, xo) < REL_IMG
     assert st.iterations == 60
+
+
+def test_reconstruct_host_reuses_state_correctly(av):
+    """Repeated host calls (the kept operator/solver/graphs) give the same image
+    as the first call, and a changed mask or parameter set rebuilds the state."""
+    from avionic_b200 import synth
+    prob = synth.small(4)
+    p = av.default_params(av.TGV2)
+    p.maxIt = 40
+    x1, _ = av.reconstruct_host("TGV2", prob["kdata"], prob["mask"], prob["b1"], params=p)
+    x2, _ = av.reconstruct_host("TGV2", prob["kdata"], prob["mask"], prob["b1"], params=p)
+    assert np.array_equal(x1, x2)
+    # another mask: must match the oracle for that mask, not the cached one
+    prob2 = dict(prob)
+    m2 = prob["mask"].copy()
+    m2[:, 1::3, :] = 0.0
+    prob2["mask"] = m2
+    prob2["kdata"] = prob["kdata"] * m2[:, None]
+    x3, _ = av.reconstruct_host("TGV2", prob2["kdata"], prob2["mask"], prob2["b1"], params=p)
+    xo, _, _ = _oracle_run("TGV2", prob2, 40)
+    assert rel(x3, xo) < REL_IMG
+    # another lambda
+    q = av.default_params(av.TGV2)
+    q.maxIt = 40
+    q.adaptLambda = 0
+    q.lambda_ = 3.0
+    x4, _ = av.reconstruct_host("TGV2", prob["kdata"], prob["mask"], prob["b1"], params=q)
+    assert rel(x4, x1) > 1e-4
+    av.lib.avx_reconstruct_host_release()
