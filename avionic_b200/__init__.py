@@ -91,6 +91,10 @@ def to_device(a, dtype=None):
     return torch.from_numpy(np.ascontiguousarray(a.astype(dtype))).cuda()
 
 
+DFT_FP32 = 0            # fp32 CUDA-core transform along y
+DFT_SPLIT_BF16X3 = 1    # tcgen05 tensor-core transform, operands split into three bf16 pieces
+
+
 class CartesianOperator:
     """``CartesianOperator`` (CUDA/src/cartesian_operator.cpp:3-168).
 
@@ -103,6 +107,17 @@ class CartesianOperator:
         mptr = _cptr(mask) if mask is not None else None
         check(lib.avx_cartesian_operator_create(width, height, coils, frames, mptr, int(centered),
                                                 ctypes.byref(self.handle)))
+
+    @property
+    def dft_mode(self):
+        """DFT_FP32 or DFT_SPLIT_BF16X3: arithmetic of the transform along y."""
+        m = ctypes.c_int()
+        check(lib.avx_operator_get_dft_mode(self.handle, ctypes.byref(m)))
+        return m.value
+
+    @dft_mode.setter
+    def dft_mode(self, mode):
+        check(lib.avx_operator_set_dft_mode(self.handle, int(mode)))
 
     def backward(self, x, b1, out=None):
         """image (T,H,W) -> k-space (T,C,H,W) (BackwardOperation)."""

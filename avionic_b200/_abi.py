@@ -87,6 +87,8 @@ SIGNATURES = {
     "avx_coil_construction_radial": (I, [U, U, U, U, U, C.POINTER(CoilParams), VP, VP, VP, VP, VP]),
     "avx_reconstruct_host": (I, [I, U, U, U, U, C.POINTER(PDParams), I, VP, VP, VP, VP, VP, C.POINTER(RunStats)]),
     "avx_reconstruct_host_release": (None, []),
+    "avx_operator_set_dft_mode": (I, [VP, I]),
+    "avx_operator_get_dft_mode": (I, [VP, C.POINTER(I)]),
 }
 
 

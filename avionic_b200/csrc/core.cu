@@ -25,6 +25,7 @@
 #include "fft2d.cuh"
 #include "pd_kernels.cuh"
 #include "radial.cuh"
+#include "tc_dft.cuh"
 #include "utils_kernels.cuh"
 
 
@@ -145,14 +146,19 @@ avx_status sum_sq(const float2* v, long long n, cudaStream_t s, double* out) {
   return AVX_OK;
 }
 
-bool g_configured = false;
+// kernel attributes are per device: one bit per configured device
+unsigned long long g_configured = 0;
 
 avx_status configure_once() {
-  if (g_configured) return AVX_OK;
+  int dev = 0;
+  AVX_CK(cudaGetDevice(&dev));
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (g_configured & bit) return AVX_OK;
   AVX_CK(avx::configure_kernels());
   AVX_CK(avx::configure_radial_kernels());
   AVX_CK(avx::configure_fft2d_kernels());
-  g_configured = true;
+  AVX_CK(avx::configure_tc_kernels());
+  g_configured |= bit;
   return AVX_OK;
 }
 
@@ -193,6 +199,10 @@ struct avx_operator {
   DevBuf<int> d_rows, d_row_off;
   DevBuf<float> d_mrow, d_mask;
   DevBuf<float2> d_twx, d_twy, d_qp;
+  // split-BF16x3 tensor-core y-transform
+  int dft_mode = AVX_DFT_FP32;
+  int tc_np = 0;  // MMA N of the y-transform = MMA K of the column adjoint; 0: split form not available
+  DevBuf<uint4> tc_ytab, tc_ctab;
 
   CartGeomDev geom() const {
     CartGeomDev g;
@@ -259,6 +269,25 @@ static avx_status build_operator(avx_operator* op, const float* h_mask) {
   if (op->has_mask) {
     AVX_CK(op->d_mask.alloc((size_t)T * H * W));
     AVX_CK(cudaMemcpy(op->d_mask.p, h_mask, (size_t)T * H * W * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  // coefficient table of the tensor-core y-transform (at most 64 rows per frame)
+  int max_rows = 0;
+  for (int t = 0; t < T; ++t) max_rows = std::max(max_rows, op->row_off[t + 1] - op->row_off[t]);
+  const int np = std::max(16, (2 * max_rows + 15) / 16 * 16);
+  op->tc_np = 0;
+  op->dft_mode = AVX_DFT_FP32;
+  if (max_rows > 0 && np <= TC_MAX_NP) {
+    std::vector<unsigned short> tab(avx::tc_ytab_bytes(H, T, np) / 2);
+    avx::tc_build_ytab(W, H, T, op->centered ? W / 2 : 0, op->centered ? H / 2 : 0, op->rows.data(),
+                       op->row_off.data(), np, tab.data());
+    AVX_CK(op->tc_ytab.alloc(tab.size() * 2 / sizeof(uint4)));
+    AVX_CK(cudaMemcpy(op->tc_ytab.p, tab.data(), tab.size() * 2, cudaMemcpyHostToDevice));
+    std::vector<unsigned short> ctab(avx::tc_ctab_bytes(H, T, np) / 2);
+    avx::tc_build_ctab(H, T, op->centered ? H / 2 : 0, op->rows.data(), op->row_off.data(), np, ctab.data());
+    AVX_CK(op->tc_ctab.alloc(ctab.size() * 2 / sizeof(uint4)));
+    AVX_CK(cudaMemcpy(op->tc_ctab.p, ctab.data(), ctab.size() * 2, cudaMemcpyHostToDevice));
+    op->tc_np = np;
+    op->dft_mode = AVX_DFT_SPLIT_BF16X3;
   }
   return AVX_OK;
 }
@@ -571,6 +600,14 @@ static PDArgs make_pdargs(avx_solver* s) {
   return a;
 }
 
+static void set_tc(KArgs* k, const avx_operator* op) {
+  const bool on = op->kind == 0 && op->dft_mode == AVX_DFT_SPLIT_BF16X3 && op->tc_np > 0;
+  k->tc_ytab = on ? op->tc_ytab.p : nullptr;
+  k->tc_np = on ? op->tc_np : 0;
+  k->tc_ctab = on ? op->tc_ctab.p : nullptr;
+  k->tc_kc = on ? op->tc_np : 0;
+}
+
 static KArgs make_kargs(avx_solver* s, const float2* b1, const float2* in, const float2* in2) {
   KArgs k;
   memset(&k, 0, sizeof(k));
@@ -585,6 +622,7 @@ static KArgs make_kargs(avx_solver* s, const float2* b1, const float2* in, const
   k.binary_mask = s->op->binary ? 1 : 0;
   k.st = s->st.p;
   k.partial = s->pk.p;
+  set_tc(&k, s->op);
   return k;
 }
 
@@ -770,7 +808,7 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
   avx_pd_params pk = s->p;
   pk.sigma = pk.tau = 0.f;
   const size_t key = (size_t)b1 ^ ((size_t)s->prim.p << 1) ^ ((size_t)s->op << 2) ^
-                     std::hash<std::string>()(std::string((const char*)&pk, sizeof(pk)));
+                     ((size_t)s->op->dft_mode << 7) ^ std::hash<std::string>()(std::string((const char*)&pk, sizeof(pk)));
   if (key != s->graph_key) {
     s->drop_graphs();
     s->graph_key = key;
@@ -1170,6 +1208,21 @@ avx_status avx_cartesian_operator_create(unsigned width, unsigned height, unsign
   return AVX_OK;
 }
 
+avx_status avx_operator_set_dft_mode(avx_operator* op, int mode) {
+  if (!op) return fail(AVX_E_ARG, "null operator");
+  if (mode != AVX_DFT_FP32 && mode != AVX_DFT_SPLIT_BF16X3) return fail(AVX_E_ARG, "unknown DFT mode");
+  if (mode == AVX_DFT_SPLIT_BF16X3 && (op->kind != 0 || op->tc_np == 0))
+    return fail(AVX_E_UNSUPPORTED, "split-BF16x3 transform needs a Cartesian operator with <= 64 rows per frame");
+  op->dft_mode = mode;
+  return AVX_OK;
+}
+
+avx_status avx_operator_get_dft_mode(const avx_operator* op, int* mode) {
+  if (!op || !mode) return fail(AVX_E_ARG, "null argument");
+  *mode = op->kind == 0 ? op->dft_mode : AVX_DFT_FP32;
+  return AVX_OK;
+}
+
 avx_status avx_radial_operator_create(unsigned width, unsigned height, unsigned coils, unsigned frames,
                                       unsigned nSpokes, unsigned nFE, unsigned spokesPerFrame, const float* d_traj,
                                       const float* d_dens, float kernelWidth, float sectorWidth, float osf,
@@ -1236,6 +1289,7 @@ avx_status avx_operator_backward(avx_operator* op, const avx_cf32* d_x, avx_cf32
   k.in = reinterpret_cast<const float2*>(d_x);
   k.dense_out = reinterpret_cast<float2*>(d_k);
   k.qp = op->d_qp.p;  // y-transformed rows between the two kernels
+  set_tc(&k, op);
   if (op->R) avx::launch_kspace(k, 3, 0);
   AVX_CK(cudaGetLastError());
   AVX_CK(cudaDeviceSynchronize());
@@ -1258,6 +1312,7 @@ avx_status avx_operator_forward(avx_operator* op, avx_cf32* d_k, avx_cf32* d_x, 
   k.g = op->geom();
   k.b1 = reinterpret_cast<const float2*>(d_b1);
   k.qp = op->d_qp.p;
+  set_tc(&k, op);
   avx::launch_dense_rowidft(k.g, reinterpret_cast<float2*>(d_k), op->d_qp.p, op->has_mask ? op->d_mask.p : nullptr, 0);
   avx::launch_adjoint(k, reinterpret_cast<float2*>(d_x), 0);
   AVX_CK(cudaGetLastError());

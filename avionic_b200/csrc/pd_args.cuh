@@ -60,4 +60,10 @@ struct KArgs {
   int binary_mask;      // 1 when every mask value is 0 or 1
   DevState* st;
   double* partial;      // [slots * gridBlocks]
+  // split-BF16x3 tensor-core y-transform (null: fp32 CUDA-core kernels)
+  const uint4* tc_ytab; // coefficient pieces, tc_dft.cuh
+  int tc_np;            // MMA N (2 x rows per frame, rounded up to 16)
+  // split-BF16x3 tensor-core column adjoint (null: fp32 CUDA-core kernel)
+  const uint4* tc_ctab; // conjugate coefficient pieces, tc_dft.cuh
+  int tc_kc;            // MMA K (2 x rows per frame, rounded up to 16)
 };

@@ -17,6 +17,7 @@
 #include "pd_kernels.cuh"
 #include "stencil.cuh"
 #include "fft.cuh"
+#include "tc_dft.cuh"
 
 namespace avx {
 
@@ -811,6 +812,10 @@ void launch_primal(int method, const PDArgs& a, cudaStream_t s) {
 }
 
 void launch_ydft(const KArgs& k, cudaStream_t s) {
+  if (k.tc_ytab) {
+    launch_ydft_tc(k, s);
+    return;
+  }
   dim3 gr((k.g.W + YD_XS - 1) / YD_XS, k.g.T);
   ydft_kernel<KSPACE_KC><<<gr, dim3(YD_XS, YD_CG), ydft_smem_bytes(k.g.H), s>>>(k);
 }
@@ -825,6 +830,10 @@ void launch_kspace(const KArgs& k, int mode, cudaStream_t s) {
 }
 
 void launch_adjoint(const KArgs& k, float2* img, cudaStream_t s) {
+  if (k.tc_ctab) {
+    launch_coladj_tc(k, img, s);
+    return;
+  }
   dim3 gr((k.g.W + 2 * CA_TX - 1) / (2 * CA_TX), (k.g.H + CA_TY * CA_YP - 1) / (CA_TY * CA_YP), k.g.T);
   coladj_kernel<<<gr, dim3(CA_TX, CA_TY), 0, s>>>(k, img);
 }

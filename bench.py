@@ -219,6 +219,8 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=2)
     ap.add_argument("--cpu-iters", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--dft", default="split", choices=["split", "fp32"],
+                    help="arithmetic of the y-transforms: split-BF16x3 tensor cores or fp32 CUDA cores")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -251,6 +253,7 @@ def main():
     x0 = av.to_device(np.repeat(prob["u0"][None], T, axis=0))
     x = torch.empty_like(x0)
     op = av.CartesianOperator(W, H, C, T, mask=md, centered=False)
+    op.dft_mode = av.DFT_SPLIT_BF16X3 if args.dft == "split" else av.DFT_FP32
     solver = av.Solver(av.ICTGV2, op, cfg_params(av))
     solver.set_debug(False, 0)
     R = int(np.count_nonzero(prob["mask"].any(axis=2)))
@@ -290,6 +293,31 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
     value = world * args.steps * ITERS / (ms / 1000.0)
+
+    # the other arithmetic of the y-transforms, same problem and schedule (reported beside the headline)
+    other = None
+    if args.dft == "split" and op.dft_mode == av.DFT_SPLIT_BF16X3:
+        op.dft_mode = av.DFT_FP32
+        for _ in range(2):
+            x.copy_(x0)
+            solver.run(kd, x, b1)
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record()
+        for _ in range(args.steps):
+            x.copy_(x0)
+            solver.run(kd, x, b1)
+        g1.record()
+        torch.cuda.synchronize()
+        x_fp32 = x.clone()
+        other = {"dft": "fp32 CUDA cores", "value": world * args.steps * ITERS / (g0.elapsed_time(g1) / 1000.0),
+                 "unit": UNIT}
+        op.dft_mode = av.DFT_SPLIT_BF16X3
+        x.copy_(x0)
+        solver.run(kd, x, b1)
+        torch.cuda.synchronize()
+        other["rel_l2_split_vs_fp32"] = float(torch.linalg.vector_norm(x - x_fp32) /
+                                              torch.linalg.vector_norm(x_fp32))
 
     # per-stage durations: one more reconstruction with CUDA events between the
     # stages of every iteration (kernels launched directly, not from graphs)
@@ -375,10 +403,14 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32 (complex64)", "data": "synthetic",
+        "vs_baseline": None,
+        "dtype": ("bf16x3-split y-DFTs on tensor cores (fp32 accumulate), f32 elsewhere" if args.dft == "split"
+                  else "f32 (complex64)"),
+        "data": "synthetic",
         "config": {"workload": WORKLOAD, "parallelism": "one independent reconstruction per GPU",
                    "l2": "inputs larger than L2 (working set ~0.4 GB per GPU)", "graphs": True,
                    "recons_per_s": value / ITERS,
+                   "dft": args.dft, "other_dft_form": other,
                    "recon_latency_ms": {"p50": float(np.percentile(step_ms, 50)),
                                         "p99": float(np.percentile(step_ms, 99))}},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},

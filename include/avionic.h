@@ -109,6 +109,19 @@ const char* avx_last_error(void);
 avx_status avx_cartesian_operator_create(unsigned width, unsigned height, unsigned coils, unsigned frames,
                                          const float* d_mask, int centered, avx_operator** op);
 
+/* Arithmetic of the Cartesian operator's transform along y (no reference
+ * counterpart; the reference applies cuFFT in fp32):
+ *   AVX_DFT_FP32           fp32 CUDA-core partial DFT
+ *   AVX_DFT_SPLIT_BF16X3   tcgen05 tensor-core partial DFT with operands split
+ *                          into three bf16 pieces (six piece products, fp32
+ *                          accumulation; fp32-level accuracy)
+ * The split form needs at most 64 sampled rows per frame; otherwise
+ * AVX_E_UNSUPPORTED is returned and the mode is unchanged.  New operators
+ * use the split form when it applies.  The radial operator ignores this. */
+typedef enum avx_dft_mode { AVX_DFT_FP32 = 0, AVX_DFT_SPLIT_BF16X3 = 1 } avx_dft_mode;
+avx_status avx_operator_set_dft_mode(avx_operator* op, int mode);
+avx_status avx_operator_get_dft_mode(const avx_operator* op, int* mode);
+
 /* NoncartesianOperator(width, height, coils, frames, nSpokes, nFE,
  * spokesPerFrame, kTraj, dens, kernelWidth, sectorWidth, osf)
  * (CUDA/src/noncartesian_operator.cpp:3-86): the radial gridding operator.

@@ -60,12 +60,18 @@ def _mask(kind, T, H, W, rng):
     return m * rng.uniform(0.3, 1.7, size=(T, H, W)).astype(np.float32)
 
 
+DFT_MODES = [0, 1]  # DFT_FP32, DFT_SPLIT_BF16X3
+
+
+@pytest.mark.parametrize("dft", DFT_MODES)
 @pytest.mark.parametrize("W,H,C,T,kind,centered", CASES)
-def test_operator_matches_oracle(av, W, H, C, T, kind, centered):
+def test_operator_matches_oracle(av, W, H, C, T, kind, centered, dft):
     rng = np.random.default_rng(W * 1000 + H)
     mask = _mask(kind, T, H, W, rng)
     x, b1, k = cplx(rng, (T, H, W)), cplx(rng, (C, H, W)), cplx(rng, (T, C, H, W))
     op = av.CartesianOperator(W, H, C, T, mask=None if mask is None else av.to_device(mask), centered=centered)
+    op.dft_mode = dft
+    assert op.dft_mode == dft
     oop = OCart(W, H, C, T, mask=mask, centered=centered)
     kg = op.backward(av.to_device(x), av.to_device(b1)).cpu().numpy()
     ko = oop.backward(x.astype(complex), b1.astype(complex))
@@ -79,8 +85,9 @@ def test_operator_matches_oracle(av, W, H, C, T, kind, centered):
     assert rel(kd.cpu().numpy(), kref) < 1e-6 or np.linalg.norm(kref) == 0
 
 
+@pytest.mark.parametrize("dft", DFT_MODES)
 @pytest.mark.parametrize("W,H,C,T,kind,centered", CASES)
-def test_operator_adjointness(av, W, H, C, T, kind, centered):
+def test_operator_adjointness(av, W, H, C, T, kind, centered, dft):
     """test_adjointness.m:1-13 / cartesian_operator.cc:150-200 on the device."""
     rng = np.random.default_rng(7 + W)
     mask = _mask(kind, T, H, W, rng)
@@ -88,6 +95,7 @@ def test_operator_adjointness(av, W, H, C, T, kind, centered):
         mask = (mask != 0).astype(np.float32)  # K^H is the adjoint for a 0/1 mask
     x, b1, z = cplx(rng, (T, H, W)), cplx(rng, (C, H, W)), cplx(rng, (T, C, H, W))
     op = av.CartesianOperator(W, H, C, T, mask=None if mask is None else av.to_device(mask), centered=centered)
+    op.dft_mode = dft
     kx = op.backward(av.to_device(x), av.to_device(b1)).cpu().numpy().astype(complex)
     khz = op.forward(av.to_device(z), av.to_device(b1)).cpu().numpy().astype(complex)
     lhs = np.vdot(kx, z.astype(complex))
@@ -110,10 +118,12 @@ def _oracle_run(method, prob, iters, debugstep=0, stop=0.0, centered=False, u0=N
     return x, tr, p
 
 
-def _gpu_run(av, method, prob, iters, debugstep=0, stop=0.0, centered=False, u0=None):
+def _gpu_run(av, method, prob, iters, debugstep=0, stop=0.0, centered=False, u0=None, dft=None):
     import torch
     T, C, H, W = prob["kdata"].shape
     op = av.CartesianOperator(W, H, C, T, mask=av.to_device(prob["mask"]), centered=centered)
+    if dft is not None:
+        op.dft_mode = dft
     s = av.Solver(method, op)
     p = s.params
     p.maxIt = iters
@@ -126,13 +136,14 @@ def _gpu_run(av, method, prob, iters, debugstep=0, stop=0.0, centered=False, u0=
     return x.cpu().numpy(), s
 
 
+@pytest.mark.parametrize("dft", DFT_MODES)
 @pytest.mark.parametrize("method", ["TV", "TGV2", "ICTGV2"])
 @pytest.mark.parametrize("binary", [True, False])
-def test_solver_matches_oracle_small(av, method, binary):
+def test_solver_matches_oracle_small(av, method, binary, dft):
     from avionic_b200 import synth
     prob = synth.small(11, binary=binary)
     xo, tro, _ = _oracle_run(method, prob, 120, debugstep=10)
-    xg, s = _gpu_run(av, method, prob, 120, debugstep=10)
+    xg, s = _gpu_run(av, method, prob, 120, debugstep=10, dft=dft)
     assert rel(xg, xo) < REL_IMG, rel(xg, xo)
     st = s.stats()
     assert st.iterations == 120
@@ -210,3 +221,34 @@ def test_reconstruct_host_reuses_state_correctly(av):
     x4, _ = av.reconstruct_host("TGV2", prob["kdata"], prob["mask"], prob["b1"], params=q)
     assert rel(x4, x1) > 1e-4
     av.lib.avx_reconstruct_host_release()
+
+
+def test_split_dft_matches_fp32_config1_shape(av):
+    """The split-BF16x3 tensor-core y-transform agrees with the fp32 CUDA-core
+    one at the benchmark shape (192 x 192, 16 coils, 16 rows per frame)."""
+    import torch
+    from avionic_b200 import synth
+    prob = synth.config1(2, T=4)
+    T, C, H, W = prob["kdata"].shape
+    rng = np.random.default_rng(3)
+    x = av.to_device(cplx(rng, (T, H, W)))
+    b1 = av.to_device(prob["b1"])
+    op = av.CartesianOperator(W, H, C, T, mask=av.to_device(prob["mask"]), centered=False)
+    assert op.dft_mode == av.DFT_SPLIT_BF16X3
+    ks = op.backward(x, b1).cpu().numpy()
+    op.dft_mode = av.DFT_FP32
+    kf = op.backward(x, b1).cpu().numpy()
+    oop = OCart(W, H, C, T, mask=prob["mask"], centered=False)
+    ko = oop.backward(x.cpu().numpy().astype(complex), prob["b1"].astype(complex))
+    assert rel(kf, ko) < REL_OP
+    assert rel(ks, ko) < REL_OP
+    # the adjoint (column transform + coil combine) in both forms
+    z = cplx(rng, (T, C, H, W)) * prob["mask"][:, None]
+    io = oop.forward(z.astype(complex), prob["b1"].astype(complex))
+    op.dft_mode = av.DFT_SPLIT_BF16X3
+    i_s = op.forward(av.to_device(z), b1).cpu().numpy()
+    op.dft_mode = av.DFT_FP32
+    i_f = op.forward(av.to_device(z), b1).cpu().numpy()
+    assert rel(i_f, io) < REL_OP
+    assert rel(i_s, io) < REL_OP
+    torch.cuda.synchronize()
