@@ -26,7 +26,7 @@ AVX_D void small_dft(const float2* src, float2* dst, const float2* tw, int j, in
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const float2 s0 = src[(j + r * nb) * KCP + kk];
-    v[r] = r ? cmul(s0, tw_sign(tw, (r * k * tws) % W, sign)) : s0;
+    v[r] = r ? cmul(s0, tw_sign(tw, r * k * tws, sign)) : s0;
   }
 #pragma unroll
   for (int q = 0; q < R; ++q) {
@@ -37,28 +37,37 @@ AVX_D void small_dft(const float2* src, float2* dst, const float2* tw, int j, in
   }
 }
 
+// floor(j / d) for j < 2^16 and 1 <= d < 2^16 from m = ceil(2^32 / d) (m = 0 for d = 1):
+// j m = j 2^32 / d + j e / d with e = m d - 2^32 < d, and j e < 2^32, so the
+// high word is exact.
+AVX_D unsigned div_magic(unsigned d) { return d == 1u ? 0u : 0xFFFFFFFFu / d + 1u; }
+AVX_D int fast_div(int j, unsigned d, unsigned m) { return d == 1u ? j : (int)__umulhi((unsigned)j, m); }
+
 template <int KC>
 __device__ float2* row_fft(float2* src, float2* dst, const float2* tw, int W, int nrad, const int* rad, int sign) {
   constexpr int KCP = KC + 2;
   int Ns = 1;
+  // kk is fixed per thread when the block size is a multiple of KC
   for (int p = 0; p < nrad; ++p) {
     const int R = rad[p];
     const int nb = W / R;
-    const int tws = W / (Ns * R);
+    const int tws = W / (Ns * R);  // r k tws < W for r < R, k < Ns: twiddle indices need no reduction
+    const unsigned mNs = div_magic((unsigned)Ns);
     for (int e = threadIdx.x; e < nb * KC; e += blockDim.x) {
       const int kk = e % KC, j = e / KC;
-      const int k = j % Ns;
-      const int idxD = (j / Ns) * Ns * R + k;
+      const int q = fast_div(j, (unsigned)Ns, mNs);
+      const int k = j - q * Ns;
+      const int idxD = q * Ns * R + k;
       if (R == 2) {
         const float2 v0 = src[j * KCP + kk];
-        const float2 v1 = cmul(src[(j + nb) * KCP + kk], tw_sign(tw, (k * tws) % W, sign));
+        const float2 v1 = cmul(src[(j + nb) * KCP + kk], tw_sign(tw, k * tws, sign));
         dst[idxD * KCP + kk] = cadd(v0, v1);
         dst[(idxD + Ns) * KCP + kk] = csub(v0, v1);
       } else if (R == 4) {
         const float2 v0 = src[j * KCP + kk];
-        const float2 v1 = cmul(src[(j + nb) * KCP + kk], tw_sign(tw, (k * tws) % W, sign));
-        const float2 v2 = cmul(src[(j + 2 * nb) * KCP + kk], tw_sign(tw, (2 * k * tws) % W, sign));
-        const float2 v3 = cmul(src[(j + 3 * nb) * KCP + kk], tw_sign(tw, (3 * k * tws) % W, sign));
+        const float2 v1 = cmul(src[(j + nb) * KCP + kk], tw_sign(tw, k * tws, sign));
+        const float2 v2 = cmul(src[(j + 2 * nb) * KCP + kk], tw_sign(tw, 2 * k * tws, sign));
+        const float2 v3 = cmul(src[(j + 3 * nb) * KCP + kk], tw_sign(tw, 3 * k * tws, sign));
         const float2 a0 = cadd(v0, v2), a1 = csub(v0, v2);
         const float2 b0 = cadd(v1, v3), b1 = csub(v1, v3);
         // i*sign*b1
@@ -69,8 +78,8 @@ __device__ float2* row_fft(float2* src, float2* dst, const float2* tw, int W, in
         dst[(idxD + 3 * Ns) * KCP + kk] = csub(a1, ib1);
       } else if (R == 3) {
         const float2 v0 = src[j * KCP + kk];
-        const float2 v1 = cmul(src[(j + nb) * KCP + kk], tw_sign(tw, (k * tws) % W, sign));
-        const float2 v2 = cmul(src[(j + 2 * nb) * KCP + kk], tw_sign(tw, (2 * k * tws) % W, sign));
+        const float2 v1 = cmul(src[(j + nb) * KCP + kk], tw_sign(tw, k * tws, sign));
+        const float2 v2 = cmul(src[(j + 2 * nb) * KCP + kk], tw_sign(tw, 2 * k * tws, sign));
         const float2 t1 = cadd(v1, v2);
         const float2 t2 = make_float2(v0.x - 0.5f * t1.x, v0.y - 0.5f * t1.y);
         const float2 d = csub(v1, v2);

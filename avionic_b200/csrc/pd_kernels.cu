@@ -220,6 +220,7 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
 
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int j = tid; j < W; j += nt) twx[j] = g.twx[j];
+  const unsigned mW = div_magic((unsigned)W);  // e < KC W < 2^16
 
   const float sig = a.st ? (float)a.st->sigma : 0.f;
   const float zscale = (mode == 0) ? (float)(1.0 / (1.0 + a.st->sigma / (double)a.lam)) : 1.f;
@@ -231,8 +232,12 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
     // with the FFT, sequence position n holds x = n + sx (the ifftshift of the
     // centred transform); the dense DFT indexes x directly
     for (int e = tid; e < KC * W; e += nt) {
-      const int kk = e / W, x = e % W;
-      const int xs = g.nrad ? (x - g.sx + W) % W : x;
+      const int kk = fast_div(e, (unsigned)W, mW), x = e - kk * W;
+      int xs = x;
+      if (g.nrad) {
+        xs = x - g.sx;
+        if (xs < 0) xs += W;
+      }
       P[xs * KCP + kk] = kk < kc ? a.qp[zb + (long long)(k0 + kk) * W + x] : czero();
     }
     __syncthreads();
@@ -268,8 +273,12 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
     }
     // pointwise stage on the kept samples; Xb[n] holds kx = n + sx (FFT) or kx
     for (int e = tid; e < kc * W; e += nt) {
-      const int kk = e / W, kx = e % W;
-      const int n = g.nrad ? (kx - g.sx + W) % W : kx;
+      const int kk = fast_div(e, (unsigned)W, mW), kx = e - kk * W;
+      int n = kx;
+      if (g.nrad) {
+        n = kx - g.sx;
+        if (n < 0) n += W;
+      }
       const long long gi = zb + (long long)(k0 + kk) * W + kx;
       const float m = g.mrow[(long long)(r0 + k0 + kk) * W + kx];
       const float2 Xv = cscale(Xb[n * KCP + kk], g.inv_sqrt_w);
@@ -305,8 +314,9 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
       // inverse row FFT; Xb position n holds kx = n + sx, the result position n holds x = n + sx
       float2* Qb = row_fft<KC>(Xb, Xb == X ? P : X, twx, W, g.nrad, g.rad, -1);
       for (int e = tid; e < kc * W; e += nt) {
-        const int kk = e / W, x = e % W;
-        const int n = (x - g.sx + W) % W;
+        const int kk = fast_div(e, (unsigned)W, mW), x = e - kk * W;
+        int n = x - g.sx;
+        if (n < 0) n += W;
         a.qp[zb + (long long)(k0 + kk) * W + x] = cscale(Qb[n * KCP + kk], g.inv_sqrt_w);
       }
       continue;
@@ -461,50 +471,40 @@ __global__ void __launch_bounds__(ADJ_TX* ADJ_TY) primal_kernel(PDArgs a) {
     const int y = y0 + threadIdx.y * ADJ_YP + j;
     if (y >= a.H) continue;
     const PixCoord p = make_pix(x, y, t, a.W, a.H, a.T);
-    // x1 <- x1 - tau (K^H z - div y1)
+    // every load of the pixel first (the stores below would otherwise order them)
     const float2 dv1 = div3(a.y[0], a.y[1], a.y[2], p, a.w1);
-    {
-      const float2 xo = a.x[0][p.i];
-      const float2 r = csub(kh[j], dv1);
-      const float2 xn = make_float2(xo.x - tau * r.x, xo.y - tau * r.y);
-      a.x[0][p.i] = xn;
-      a.xb[0][p.i] = make_float2(2.f * xn.x - xo.x, 2.f * xn.y - xo.y);
-    }
-    if (M == AVX_M_TV) continue;
-    // x2 <- x2 + tau (y1 + symdiv y2)
-    {
-      float2 sd[3];
-      symdiv(a.y + 3, p, a.w1, sd);
+    float2 sd1[3], y1[3], sd2[3], y3[3], xo[8];
+    float2 dv3 = czero();
+    if (M != AVX_M_TV) {
+      symdiv(a.y + 3, p, a.w1, sd1);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float2 r = cadd(ldc(a.y[c], p.i), sd[c]);
-        const float2 xo = a.x[1 + c][p.i];
-        const float2 xn = make_float2(xo.x + tau * r.x, xo.y + tau * r.y);
-        a.x[1 + c][p.i] = xn;
-        a.xb[1 + c][p.i] = make_float2(2.f * xn.x - xo.x, 2.f * xn.y - xo.y);
-      }
+      for (int c = 0; c < 3; ++c) y1[c] = ldc(a.y[c], p.i);
     }
     if (M == AVX_M_ICTGV2) {
-      // x3 <- x3 - tau (div1 y1 - div2 y3)
-      const float2 dv3 = div3(a.y[9], a.y[10], a.y[11], p, a.w2);
-      {
-        const float2 r = csub(dv1, dv3);
-        const float2 xo = a.x[4][p.i];
-        const float2 xn = make_float2(xo.x - tau * r.x, xo.y - tau * r.y);
-        a.x[4][p.i] = xn;
-        a.xb[4][p.i] = make_float2(2.f * xn.x - xo.x, 2.f * xn.y - xo.y);
-      }
-      // x4 <- x4 + tau (y3 + symdiv2 y4)
-      float2 sd[3];
-      symdiv(a.y + 12, p, a.w2, sd);
+      dv3 = div3(a.y[9], a.y[10], a.y[11], p, a.w2);
+      symdiv(a.y + 12, p, a.w2, sd2);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float2 r = cadd(ldc(a.y[9 + c], p.i), sd[c]);
-        const float2 xo = a.x[5 + c][p.i];
-        const float2 xn = make_float2(xo.x + tau * r.x, xo.y + tau * r.y);
-        a.x[5 + c][p.i] = xn;
-        a.xb[5 + c][p.i] = make_float2(2.f * xn.x - xo.x, 2.f * xn.y - xo.y);
-      }
+      for (int c = 0; c < 3; ++c) y3[c] = ldc(a.y[9 + c], p.i);
+    }
+    constexpr int P = M == AVX_M_TV ? 1 : (M == AVX_M_TGV2 ? 4 : 8);
+#pragma unroll
+    for (int c = 0; c < P; ++c) xo[c] = a.x[c][p.i];
+    // updates: x' = x + tau r, xbar = 2 x' - x
+    float2 r[8];
+    r[0] = csub(dv1, kh[j]);                       // x1 <- x1 - tau (K^H z - div y1)
+    if (M != AVX_M_TV)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) r[1 + c] = cadd(y1[c], sd1[c]);  // x2 <- x2 + tau (y1 + symdiv y2)
+    if (M == AVX_M_ICTGV2) {
+      r[4] = csub(dv3, dv1);                       // x3 <- x3 - tau (div1 y1 - div2 y3)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) r[5 + c] = cadd(y3[c], sd2[c]);  // x4 <- x4 + tau (y3 + symdiv2 y4)
+    }
+#pragma unroll
+    for (int c = 0; c < P; ++c) {
+      const float2 xn = make_float2(xo[c].x + tau * r[c].x, xo[c].y + tau * r[c].y);
+      a.x[c][p.i] = xn;
+      a.xb[c][p.i] = make_float2(2.f * xn.x - xo[c].x, 2.f * xn.y - xo[c].y);
     }
   }
 }
