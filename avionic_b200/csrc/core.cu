@@ -203,6 +203,7 @@ struct avx_operator {
   int dft_mode = AVX_DFT_FP32;
   int tc_np = 0;  // MMA N of the y-transform = MMA K of the column adjoint; 0: split form not available
   DevBuf<uint4> tc_ytab, tc_ctab;
+  DevBuf<float2> tc_b1t;  // coil maps in column-tile order for operator applies
 
   CartGeomDev geom() const {
     CartGeomDev g;
@@ -506,6 +507,7 @@ struct avx_solver {
   cudaStream_t stream = 0;
   // device state
   DevBuf<float2> prim, ext, dual, escr, z, d;
+  DevBuf<float2> b1t;  // coil maps in column-tile order (tensor-core adjoint)
   DevBuf<DevState> st;
   DevBuf<double> pimg, pk, hist;
   int cap = 0;
@@ -623,7 +625,17 @@ static KArgs make_kargs(avx_solver* s, const float2* b1, const float2* in, const
   k.st = s->st.p;
   k.partial = s->pk.p;
   set_tc(&k, s->op);
+  k.b1t = s->b1t.p;
   return k;
+}
+
+// the tensor-core adjoint reads the coil maps in column-tile order
+static avx_status prepare_b1t(avx_solver* s, const float2* b1) {
+  if (s->op->kind != 0 || s->op->dft_mode != AVX_DFT_SPLIT_BF16X3 || s->op->tc_np == 0) return AVX_OK;
+  AVX_CK(s->b1t.alloc(avx::b1t_count(s->W, s->H, s->C)));
+  avx::launch_b1_tile_transpose(b1, s->b1t.p, s->W, s->H, s->C, s->stream);
+  AVX_CK(cudaGetLastError());
+  return AVX_OK;
 }
 
 static avx::GapConst make_gapconst(avx_solver* s) {
@@ -787,6 +799,8 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
   AVX_CK(cudaEventRecord(evin, s->user_stream));
   AVX_CK(cudaStreamWaitEvent(s->stream, evin, 0));
   r = prepare_run(s, data, x);
+  if (r != AVX_OK) return r;
+  r = prepare_b1t(s, b1);
   if (r != AVX_OK) return r;
   if (s->method == AVX_METHOD_ICTGV2 && s->debug) {
     PDArgs a = make_pdargs(s);
@@ -1313,6 +1327,11 @@ avx_status avx_operator_forward(avx_operator* op, avx_cf32* d_k, avx_cf32* d_x, 
   k.b1 = reinterpret_cast<const float2*>(d_b1);
   k.qp = op->d_qp.p;
   set_tc(&k, op);
+  if (k.tc_ctab) {
+    AVX_CK(op->tc_b1t.alloc(avx::b1t_count(op->W, op->H, op->C)));
+    avx::launch_b1_tile_transpose(k.b1, op->tc_b1t.p, op->W, op->H, op->C, 0);
+    k.b1t = op->tc_b1t.p;
+  }
   avx::launch_dense_rowidft(k.g, reinterpret_cast<float2*>(d_k), op->d_qp.p, op->has_mask ? op->d_mask.p : nullptr, 0);
   avx::launch_adjoint(k, reinterpret_cast<float2*>(d_x), 0);
   AVX_CK(cudaGetLastError());
@@ -1464,6 +1483,8 @@ avx_status avx_solver_compute_gap(avx_solver* s, const avx_cf32* const* d_x, con
   const int P = method_P(s->method), D = method_D(s->method);
   const size_t N = (size_t)s->N();
   r = prepare_run(s, reinterpret_cast<const float2*>(d_data), nullptr);
+  if (r != AVX_OK) return r;
+  r = prepare_b1t(s, reinterpret_cast<const float2*>(d_b1));
   if (r != AVX_OK) return r;
   for (int c = 0; c < P; ++c)
     AVX_CK(cudaMemcpyAsync(s->primc(c), d_x[c], N * sizeof(float2), cudaMemcpyDeviceToDevice, s->stream));

@@ -66,4 +66,5 @@ struct KArgs {
   // split-BF16x3 tensor-core column adjoint (null: fp32 CUDA-core kernel)
   const uint4* tc_ctab; // conjugate coefficient pieces, tc_dft.cuh
   int tc_kc;            // MMA K (2 x rows per frame, rounded up to 16)
+  const float2* b1t;    // b1 in column-tile order for the tensor-core adjoint (tc_dft.cuh)
 };

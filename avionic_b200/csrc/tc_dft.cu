@@ -13,6 +13,7 @@
 #include <cuda_bf16.h>
 
 #include <cmath>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -507,10 +508,11 @@ __global__ void __launch_bounds__(TC_THREADS) coladj_tc_kernel(KArgs k, float2* 
       // b1 of the first two coils while the MMAs run
       float2 pbA[XH], pbB[XH];
       auto load_b1 = [&](int cc, float2 (&pb)[XH]) {
-        const float2* bc = k.b1 + (long long)cc * HW + (long long)y * W + xe;
+        // column-tile order: consecutive rows y of one column are adjacent
+        const float2* bc = k.b1t + (((long long)blockIdx.x * C + cc) * XT + XH * half) * H + y;
 #pragma unroll
         for (int i = 0; i < XH; ++i)
-          pb[i] = (cc < c0 + ncc && y < H && xe + i < W) ? __ldg(bc + i) : make_float2(0.f, 0.f);
+          pb[i] = (cc < c0 + ncc && y < H) ? __ldg(bc + (long long)i * H) : make_float2(0.f, 0.f);
       };
       auto combine = [&](int cl, const float2 (&pb)[XH]) {
         float v[XT];
@@ -543,6 +545,28 @@ __global__ void __launch_bounds__(TC_THREADS) coladj_tc_kernel(KArgs k, float2* 
     for (int i = 0; i < XH; ++i)
       if (xe + i < W) out[i] = acc[i];
   }
+}
+
+size_t b1t_count(int W, int H, int C) { return (size_t)((W + CA_TC_XT - 1) / CA_TC_XT) * C * CA_TC_XT * H; }
+
+__global__ void b1_tile_transpose_kernel(const float2* __restrict__ b1, float2* __restrict__ b1t, int W, int H,
+                                         int C, long long n) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(e % H);
+    long long r = e / H;
+    const int xs = (int)(r % CA_TC_XT);
+    r /= CA_TC_XT;
+    const int c = (int)(r % C);
+    const int tx = (int)(r / C);
+    const int x = tx * CA_TC_XT + xs;
+    b1t[e] = x < W ? b1[((long long)c * H + y) * W + x] : make_float2(0.f, 0.f);
+  }
+}
+
+void launch_b1_tile_transpose(const float2* b1, float2* b1t, int W, int H, int C, cudaStream_t s) {
+  const long long n = (long long)b1t_count(W, H, C);
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
+  b1_tile_transpose_kernel<<<blocks, 256, 0, s>>>(b1, b1t, W, H, C, n);
 }
 
 cudaError_t configure_tc_kernels() {

@@ -46,7 +46,14 @@ AVX_HD int tc_ytiles(int H) { return (H + TC_M - 1) / TC_M; }
 size_t tc_ctab_bytes(int H, int T, int kc);
 void tc_build_ctab(int H, int T, int sy, const int* rows, const int* row_off, int kc, unsigned short* out);
 size_t tc_coladj_smem_bytes(int kc);
-// img[t] = sum_c conj(b1_c) column-IDFT(Q'_c), Q' (k.qp) split on the fly
+// img[t] = sum_c conj(b1_c) column-IDFT(Q'_c), Q' (k.qp) split on the fly;
+// needs k.b1t (below)
 void launch_coladj_tc(const KArgs& k, float2* img, cudaStream_t s);
+
+// b1 in column-tile order: b1t[((tx C + c) CA_TC_XT + xs) H + y] = b1[c][y][tx CA_TC_XT + xs]
+// (zero past the last column), so that the adjoint's threads, one per image
+// row, read consecutive addresses.  Elements: b1t_count(W, H, C).
+size_t b1t_count(int W, int H, int C);
+void launch_b1_tile_transpose(const float2* b1, float2* b1t, int W, int H, int C, cudaStream_t s);
 
 }  // namespace avx
