@@ -361,6 +361,96 @@ def reconstruct_host(method, kdata, mask, b1, u0=None, params=None, debugstep=0)
 
 
 # ---------------------------------------------------------------------------
+# batched / served reconstructions
+# ---------------------------------------------------------------------------
+
+Request = _abi.Request
+Completion = _abi.Completion
+
+
+def cartesian_request(method, data, x, b1, mask=None, params=None, centered=False, dft_mode=DFT_SPLIT_BF16X3,
+                      tag=0):
+    """avx_request for a Cartesian reconstruction.  data (T,C,H,W), x (T,H,W)
+    initial image in / result out, b1 (C,H,W), mask (T,H,W) float32 or None:
+    CUDA tensors that must stay alive until the completion is polled."""
+    if isinstance(method, str):
+        method = METHODS[method.upper()]
+    T, C, H, W = data.shape
+    r = Request()
+    r.method, r.op_kind = method, 0
+    r.width, r.height, r.coils, r.frames = W, H, C, T
+    r.params = params if params is not None else default_params(method)
+    r.dft_mode = int(dft_mode)
+    r.d_mask = _cptr(mask) if mask is not None else None
+    r.centered = int(centered)
+    r.d_data, r.d_x, r.d_b1 = _cptr(data), _cptr(x), _cptr(b1)
+    r.tag = int(tag)
+    return r
+
+
+def radial_request(method, data, x, b1, traj, dens, spokes_per_frame, n_fe, params=None, kernel_width=3.0,
+                   sector_width=8.0, osf=2.0, tag=0):
+    """avx_request for a radial reconstruction: data (T,C,S) sqrt(w)-weighted,
+    traj (T,2,S), dens (T,S) float32, x (T,H,W), b1 (C,H,W)."""
+    if isinstance(method, str):
+        method = METHODS[method.upper()]
+    T, C, S = data.shape
+    _, H, W = x.shape
+    r = Request()
+    r.method, r.op_kind = method, 1
+    r.width, r.height, r.coils, r.frames = W, H, C, T
+    r.params = params if params is not None else default_params(method)
+    r.n_fe, r.spokes_per_frame = n_fe, spokes_per_frame
+    r.d_traj, r.d_dens = _cptr(traj), _cptr(dens)
+    r.kernel_width, r.sector_width, r.osf = kernel_width, sector_width, osf
+    r.d_data, r.d_x, r.d_b1 = _cptr(data), _cptr(x), _cptr(b1)
+    r.tag = int(tag)
+    return r
+
+
+def query_workspace(request):
+    n = ctypes.c_size_t()
+    check(lib.avx_query_workspace(ctypes.byref(request), ctypes.byref(n)))
+    return n.value
+
+
+class BatchEngine:
+    """Worker threads with their own streams and device workspaces; requests
+    start in submission order once their workspace fits the HBM budget."""
+
+    def __init__(self, device=0, hbm_budget=150 << 30, workers=8):
+        self.handle = ctypes.c_void_p()
+        check(lib.avx_batch_create(int(device), int(hbm_budget), int(workers), ctypes.byref(self.handle)))
+
+    def submit(self, request):
+        check(lib.avx_batch_submit(self.handle, ctypes.byref(request)))
+
+    def poll(self, max_items=64, wait_ms=0):
+        out = (Completion * max_items)()
+        n = ctypes.c_int()
+        check(lib.avx_serve_poll(self.handle, out, max_items, ctypes.byref(n), int(wait_ms)))
+        return [out[i] for i in range(n.value)]
+
+    def drain(self):
+        check(lib.avx_batch_drain(self.handle))
+
+    @property
+    def pending(self):
+        return lib.avx_batch_pending(self.handle)
+
+    def close(self):
+        if self.handle:
+            lib.avx_batch_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
 # coil-sensitivity estimation (CoilConstruction)
 # ---------------------------------------------------------------------------
 

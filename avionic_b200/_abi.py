@@ -34,6 +34,25 @@ class CoilParams(C.Structure):
     ]
 
 
+class Request(C.Structure):
+    """avx_request"""
+    _fields_ = [
+        ("method", I), ("op_kind", I), ("width", U), ("height", U), ("coils", U), ("frames", U),
+        ("params", PDParams), ("dft_mode", I), ("d_mask", VP), ("centered", I),
+        ("n_fe", U), ("spokes_per_frame", U), ("d_traj", VP), ("d_dens", VP),
+        ("kernel_width", F), ("sector_width", F), ("osf", F),
+        ("d_data", VP), ("d_x", VP), ("d_b1", VP), ("tag", C.c_ulonglong),
+    ]
+
+
+class Completion(C.Structure):
+    """avx_completion"""
+    _fields_ = [
+        ("tag", C.c_ulonglong), ("status", I), ("dft_mode", I), ("stats", RunStats),
+        ("queue_ms", D), ("run_ms", D), ("workspace_bytes", C.c_size_t),
+    ]
+
+
 EXPORT_CB = C.CFUNCTYPE(None, C.c_char_p, C.c_char_p, VP, C.c_size_t, VP)
 
 # name -> (restype, argtypes)
@@ -88,6 +107,13 @@ SIGNATURES = {
     "avx_reconstruct_host": (I, [I, U, U, U, U, C.POINTER(PDParams), I, VP, VP, VP, VP, VP, C.POINTER(RunStats)]),
     "avx_reconstruct_host_release": (None, []),
     "avx_operator_set_dft_mode": (I, [VP, I]),
+    "avx_query_workspace": (I, [C.POINTER(Request), C.POINTER(C.c_size_t)]),
+    "avx_batch_create": (I, [I, C.c_size_t, I, C.POINTER(VP)]),
+    "avx_batch_submit": (I, [VP, C.POINTER(Request)]),
+    "avx_serve_poll": (I, [VP, C.POINTER(Completion), I, C.POINTER(I), I]),
+    "avx_batch_drain": (I, [VP]),
+    "avx_batch_pending": (I, [VP]),
+    "avx_batch_destroy": (None, [VP]),
     "avx_operator_get_dft_mode": (I, [VP, C.POINTER(I)]),
 }
 

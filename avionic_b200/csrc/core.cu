@@ -16,7 +16,11 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -47,23 +51,67 @@ avx_status fail(avx_status s, const std::string& msg) {
                   std::string(#call) + ": " + cudaGetErrorString(e_));                       \
   } while (0)
 
+// Device memory of a batch worker thread: chunks obtained with cudaMalloc and
+// kept until the worker ends, handed out by a bump pointer that restarts for
+// every request.  (cudaFree synchronises the whole device, which would
+// serialise the reconstructions that other workers run concurrently.)
+struct DevArena {
+  struct Chunk {
+    char* p;
+    size_t size;
+  };
+  std::vector<Chunk> chunks;
+  size_t ci = 0, off = 0;
+  void reset() { ci = off = 0; }
+  void* take(size_t bytes) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    for (; ci < chunks.size(); ++ci, off = 0)
+      if (off + bytes <= chunks[ci].size) {
+        void* r = chunks[ci].p + off;
+        off += bytes;
+        return r;
+      }
+    const size_t sz = std::max(bytes, (size_t)256 << 20);
+    char* p = nullptr;
+    if (cudaMalloc(&p, sz) != cudaSuccess) return nullptr;
+    chunks.push_back({p, sz});
+    ci = chunks.size() - 1;
+    off = bytes;
+    return p;
+  }
+  ~DevArena() {
+    for (const Chunk& c : chunks) cudaFree(c.p);
+  }
+};
+thread_local DevArena* t_arena = nullptr;  // set by a batch worker for its requests
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  bool from_arena = false;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p && !from_arena) cudaFree(p);
     p = nullptr;
     n = 0;
+    from_arena = false;
   }
   cudaError_t alloc(size_t count) {
     if (count <= n && p) return cudaSuccess;
     release();
-    cudaError_t e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    if (t_arena) {
+      p = static_cast<T*>(t_arena->take(bytes));
+      if (!p) return cudaErrorMemoryAllocation;
+      n = count;
+      from_arena = true;
+      return cudaSuccess;
+    }
+    cudaError_t e = cudaMalloc(&p, bytes);
     if (e == cudaSuccess) n = count;
     return e;
   }
@@ -271,7 +319,7 @@ static avx_status build_operator(avx_operator* op, const float* h_mask) {
     AVX_CK(op->d_mask.alloc((size_t)T * H * W));
     AVX_CK(cudaMemcpy(op->d_mask.p, h_mask, (size_t)T * H * W * sizeof(float), cudaMemcpyHostToDevice));
   }
-  // coefficient table of the tensor-core y-transform (at most 64 rows per frame)
+  // coefficient tables of the tensor-core transforms (at most 48 rows per frame)
   int max_rows = 0;
   for (int t = 0; t < T; ++t) max_rows = std::max(max_rows, op->row_off[t + 1] - op->row_off[t]);
   const int np = std::max(16, (2 * max_rows + 15) / 16 * 16);
@@ -1226,7 +1274,7 @@ avx_status avx_operator_set_dft_mode(avx_operator* op, int mode) {
   if (!op) return fail(AVX_E_ARG, "null operator");
   if (mode != AVX_DFT_FP32 && mode != AVX_DFT_SPLIT_BF16X3) return fail(AVX_E_ARG, "unknown DFT mode");
   if (mode == AVX_DFT_SPLIT_BF16X3 && (op->kind != 0 || op->tc_np == 0))
-    return fail(AVX_E_UNSUPPORTED, "split-BF16x3 transform needs a Cartesian operator with <= 64 rows per frame");
+    return fail(AVX_E_UNSUPPORTED, "split-BF16x3 transform needs a Cartesian operator with <= 48 rows per frame");
   op->dft_mode = mode;
   return AVX_OK;
 }
@@ -1901,6 +1949,245 @@ avx_status avx_reconstruct_host(int method, unsigned W, unsigned H, unsigned C, 
 void avx_reconstruct_host_release(void) {
   std::lock_guard<std::mutex> lock(g_plan_mu);
   g_plan.release();
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched and served reconstructions: worker threads with their own streams
+// and device arenas, FIFO admission against an HBM budget.
+// ===========================================================================
+
+namespace {
+
+size_t request_workspace(const avx_request& r, avx_status* st) {
+  *st = AVX_OK;
+  const size_t W = r.width, H = r.height, C = r.coils, T = r.frames, N = W * H * T;
+  const size_t P = (size_t)method_P(r.method), D = (size_t)method_D(r.method);
+  const size_t c8 = sizeof(float2);
+  size_t b = 0;
+  size_t kspace = 0;  // values of z (and of d)
+  if (r.op_kind == 0) {
+    size_t R = H * T, max_rows = H;
+    if (r.d_mask) {
+      std::vector<float> m(N);
+      if (cudaMemcpy(m.data(), r.d_mask, N * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        *st = fail(AVX_E_CUDA, "cannot read the request's mask");
+        return 0;
+      }
+      R = max_rows = 0;
+      for (size_t t = 0; t < T; ++t) {
+        size_t rows = 0;
+        for (size_t y = 0; y < H; ++y) {
+          const float* row = m.data() + (t * H + y) * W;
+          for (size_t x = 0; x < W; ++x)
+            if (row[x] != 0.f) {
+              ++rows;
+              break;
+            }
+        }
+        R += rows;
+        max_rows = std::max(max_rows, rows);
+      }
+    }
+    const size_t Rk = std::max<size_t>(R, 1);
+    kspace = C * Rk * W;
+    b += R * 4 + (T + 1) * 4 + R * W * 4 + (W + H) * c8 + kspace * c8 + N * c8 + (r.d_mask ? N * 4 : 0);
+    const size_t np = std::max<size_t>(16, (2 * max_rows + 15) / 16 * 16);
+    if (max_rows > 0 && np <= TC_MAX_NP) {
+      b += avx::tc_ytab_bytes((int)H, (int)T, (int)np) + avx::tc_ctab_bytes((int)H, (int)T, (int)np);
+      b += avx::b1t_count((int)W, (int)H, (int)C) * c8;
+    }
+  } else {
+    const size_t S = (size_t)r.n_fe * r.spokes_per_frame;
+    const int isw = std::max(2, (int)r.sector_width);
+    const size_t Gx = (size_t)radial_grid_size((int)W, r.osf), Gy = (size_t)radial_grid_size((int)H, r.osf);
+    const size_t sectors = T * ((Gx + isw - 1) / isw) * ((Gy + isw - 1) / isw) + 1;
+    kspace = C * T * S;
+    b += T * S * (2 * 4 + 4 + 4) + (W + H) * 4 + sectors * 4 + (Gx + Gy) * c8 + T * C * Gx * Gy * c8 + N * c8;
+  }
+  // solver: primal, extragradient and step scratch (3P), duals (D), z and d, reductions, history
+  b += (3 * P + D) * N * c8 + 2 * kspace * c8;
+  b += 8 * (size_t)std::max(AVX_RED_BLOCKS, avx::gap_img_blocks((int)W, (int)H, (int)T)) * 8;
+  b += 3 * (std::max(C * T, (T * std::max<size_t>(kspace / std::max<size_t>(C * T, 1), 1) + 255) / 256) + 1) * 8;
+  b += 3 * ((size_t)r.params.maxIt + 3) * 8 + 4096;
+  return b + b / 20 + ((size_t)16 << 20);  // arena alignment and chunk slack
+}
+
+double ms_since(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+avx_completion run_request(const avx_request& r, cudaStream_t stream) {
+  avx_completion c;
+  memset(&c, 0, sizeof(c));
+  c.tag = r.tag;
+  avx_operator* op = nullptr;
+  avx_solver* s = nullptr;
+  avx_status e;
+  if (r.op_kind == 0) {
+    e = avx_cartesian_operator_create(r.width, r.height, r.coils, r.frames, r.d_mask, r.centered, &op);
+    if (e == AVX_OK && avx_operator_set_dft_mode(op, r.dft_mode) != AVX_OK) avx_operator_set_dft_mode(op, AVX_DFT_FP32);
+    if (e == AVX_OK) avx_operator_get_dft_mode(op, &c.dft_mode);
+  } else {
+    e = avx_radial_operator_create(r.width, r.height, r.coils, r.frames, r.spokes_per_frame * r.frames, r.n_fe,
+                                   r.spokes_per_frame, r.d_traj, r.d_dens, r.kernel_width, r.sector_width, r.osf,
+                                   &op);
+  }
+  if (e == AVX_OK) e = avx_solver_create(r.method, r.width, r.height, r.coils, r.frames, &r.params, op, &s);
+  if (e == AVX_OK) e = avx_solver_set_stream(s, stream);
+  if (e == AVX_OK) e = avx_solver_run(s, r.d_data, r.d_x, r.d_b1);
+  if (e == AVX_OK) avx_solver_get_stats(s, &c.stats);
+  c.status = (int)e;
+  if (s) avx_solver_destroy(s);
+  if (op) avx_operator_destroy(op);
+  return c;
+}
+
+}  // namespace
+
+struct avx_batch {
+  int device = 0;
+  size_t budget = 0, used = 0;
+  int running = 0, pending = 0;
+  bool stop = false;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  struct Item {
+    avx_request r;
+    size_t ws;
+    std::chrono::steady_clock::time_point t_submit;
+  };
+  std::deque<Item> queue;
+  std::deque<avx_completion> done;
+  std::vector<std::thread> workers;
+
+  void work() {
+    cudaSetDevice(device);
+    DevArena arena;
+    cudaStream_t stream = nullptr;
+    cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    for (;;) {
+      Item it;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_work.wait(lk, [&] { return stop || (!queue.empty() && used + queue.front().ws <= budget); });
+        if (stop) break;
+        it = queue.front();
+        queue.pop_front();
+        used += it.ws;
+        ++running;
+      }
+      const auto t0 = std::chrono::steady_clock::now();
+      arena.reset();
+      t_arena = &arena;
+      avx_completion c = run_request(it.r, stream);
+      t_arena = nullptr;
+      const auto t1 = std::chrono::steady_clock::now();
+      c.queue_ms = ms_since(it.t_submit, t0);
+      c.run_ms = ms_since(t0, t1);
+      c.workspace_bytes = it.ws;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        used -= it.ws;
+        --running;
+        done.push_back(c);
+      }
+      cv_work.notify_all();
+      cv_done.notify_all();
+    }
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+extern "C" {
+
+avx_status avx_query_workspace(const avx_request* r, size_t* bytes) {
+  if (!r || !bytes) return fail(AVX_E_ARG, "null argument");
+  if (!method_ok(r->method)) return fail(AVX_E_UNSUPPORTED, "method not provided (TV, TGV2, ICTGV2 are)");
+  if (r->op_kind != 0 && r->op_kind != 1) return fail(AVX_E_ARG, "op_kind must be 0 (Cartesian) or 1 (radial)");
+  if (!r->width || !r->height || !r->coils || !r->frames) return fail(AVX_E_ARG, "dimensions must be positive");
+  if (r->op_kind == 1 && (!r->d_traj || !r->d_dens || !r->n_fe || !r->spokes_per_frame))
+    return fail(AVX_E_ARG, "radial request needs trajectory, density and sample counts");
+  avx_status st;
+  *bytes = request_workspace(*r, &st);
+  return st;
+}
+
+avx_status avx_batch_create(int device, size_t hbm_budget, int workers, avx_batch** out) {
+  if (!out || workers < 1 || hbm_budget == 0) return fail(AVX_E_ARG, "invalid batch engine arguments");
+  int n = 0;
+  AVX_CK(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return fail(AVX_E_ARG, "no such CUDA device");
+  AVX_CK(cudaSetDevice(device));
+  avx_status r = configure_once();
+  if (r != AVX_OK) return r;
+  avx_batch* b = new avx_batch();
+  b->device = device;
+  b->budget = hbm_budget;
+  for (int i = 0; i < workers; ++i) b->workers.emplace_back([b] { b->work(); });
+  *out = b;
+  return AVX_OK;
+}
+
+avx_status avx_batch_submit(avx_batch* b, const avx_request* r) {
+  if (!b || !r) return fail(AVX_E_ARG, "null argument");
+  if (!r->d_data || !r->d_x || !r->d_b1) return fail(AVX_E_ARG, "request without data, image or coil maps");
+  size_t ws = 0;
+  AVX_CK(cudaSetDevice(b->device));
+  avx_status st = avx_query_workspace(r, &ws);
+  if (st != AVX_OK) return st;
+  if (ws > b->budget) return fail(AVX_E_NOMEM, "request workspace exceeds the engine's HBM budget");
+  {
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->queue.push_back({*r, ws, std::chrono::steady_clock::now()});
+    ++b->pending;
+  }
+  b->cv_work.notify_all();
+  return AVX_OK;
+}
+
+avx_status avx_serve_poll(avx_batch* b, avx_completion* out, int max, int* n, int wait_ms) {
+  if (!b || !n || (max > 0 && !out)) return fail(AVX_E_ARG, "null argument");
+  std::unique_lock<std::mutex> lk(b->mu);
+  auto ready = [&] { return !b->done.empty() || b->pending == 0; };
+  if (wait_ms < 0)
+    b->cv_done.wait(lk, ready);
+  else if (wait_ms > 0)
+    b->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), ready);
+  int k = 0;
+  while (k < max && !b->done.empty()) {
+    out[k++] = b->done.front();
+    b->done.pop_front();
+    --b->pending;
+  }
+  *n = k;
+  return AVX_OK;
+}
+
+avx_status avx_batch_drain(avx_batch* b) {
+  if (!b) return fail(AVX_E_ARG, "null engine");
+  std::unique_lock<std::mutex> lk(b->mu);
+  b->cv_done.wait(lk, [&] { return b->queue.empty() && b->running == 0; });
+  return AVX_OK;
+}
+
+int avx_batch_pending(const avx_batch* b) {
+  if (!b) return 0;
+  std::lock_guard<std::mutex> lk(const_cast<avx_batch*>(b)->mu);
+  return b->pending;
+}
+
+void avx_batch_destroy(avx_batch* b) {
+  if (!b) return;
+  {
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->stop = true;
+    b->queue.clear();
+  }
+  b->cv_work.notify_all();
+  for (std::thread& t : b->workers) t.join();
+  delete b;
 }
 
 }  // extern "C"

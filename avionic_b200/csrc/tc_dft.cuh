@@ -13,7 +13,8 @@
 #define TC_M 128        // MMA rows (tile of (coil, column) pairs or image rows)
 #define TC_KS 32        // real K per pipeline stage (16 image rows of the y-transform)
 #define TC_THREADS 256  // threads per CTA
-#define TC_MAX_NP 128   // largest MMA N of the y-transform (64 sampled rows per frame)
+#define TC_MAX_NP 96    // largest MMA N of the y-transform / K of the adjoint (48 sampled rows
+                        // per frame): the adjoint's shared memory, 2304 kc bytes, stays within 227 KB
 #define CA_TC_XT 16     // image columns per tile of the tensor-core column adjoint
 
 namespace avx {

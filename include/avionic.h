@@ -115,7 +115,7 @@ avx_status avx_cartesian_operator_create(unsigned width, unsigned height, unsign
  *   AVX_DFT_SPLIT_BF16X3   tcgen05 tensor-core partial DFT with operands split
  *                          into three bf16 pieces (six piece products, fp32
  *                          accumulation; fp32-level accuracy)
- * The split form needs at most 64 sampled rows per frame; otherwise
+ * The split form needs at most 48 sampled rows per frame; otherwise
  * AVX_E_UNSUPPORTED is returned and the mode is unchanged.  New operators
  * use the split form when it applies.  The radial operator ignores this. */
 typedef enum avx_dft_mode { AVX_DFT_FP32 = 0, AVX_DFT_SPLIT_BF16X3 = 1 } avx_dft_mode;
@@ -331,6 +331,67 @@ avx_status avx_coil_time_averaged_radial(unsigned W, unsigned H, unsigned C, uns
 avx_status avx_coil_construction_radial(unsigned W, unsigned H, unsigned C, unsigned T, unsigned S,
                                         const avx_coil_params* p, const float* d_traj, const float* d_dens,
                                         const avx_cf32* d_kdata, avx_cf32* d_u, avx_cf32* d_b1);
+
+/* ------------------------------------------------------------------ */
+/* Batched and served reconstructions                                  */
+/* ------------------------------------------------------------------ */
+
+/* No reference counterpart: the reference runs one reconstruction per
+ * process (main.cpp:789).  An engine owns worker threads, each with its own
+ * CUDA stream and device workspace; submitted requests wait in a FIFO queue
+ * and start, in order, as soon as their workspace fits the engine's HBM
+ * budget, so independent reconstructions of any mix of sizes, methods and
+ * operators run concurrently on one GPU.  Every request is an ordinary
+ * operator + solver run with the given parameters (the result equals
+ * avx_solver_run on the same inputs).  Buffers are the caller's device
+ * buffers and must stay valid until the request's completion is polled. */
+typedef struct avx_request {
+  int method;                /* AVX_METHOD_TV / _TGV2 / _ICTGV2 */
+  int op_kind;               /* 0 Cartesian, 1 radial */
+  unsigned width, height, coils, frames;
+  avx_pd_params params;      /* as for avx_solver_create (lambda adapted when asked) */
+  int dft_mode;              /* Cartesian: preferred AVX_DFT_*; fp32 when the split form does not apply */
+  const float* d_mask;       /* Cartesian: T*H*W mask or NULL */
+  int centered;              /* Cartesian: centred FFT */
+  unsigned n_fe, spokes_per_frame;          /* radial: samples per spoke, spokes per frame */
+  const float* d_traj;                      /* radial: T x 2 x S trajectory in [-0.5, 0.5) */
+  const float* d_dens;                      /* radial: T x S density compensation */
+  float kernel_width, sector_width, osf;    /* radial: gridding parameters */
+  const avx_cf32* d_data;    /* k-space: Cartesian T*C*H*W (masked), radial T*C*S (sqrt(w)-weighted) */
+  avx_cf32* d_x;             /* T*H*W initial image in, reconstruction out */
+  const avx_cf32* d_b1;      /* C*H*W coil maps */
+  unsigned long long tag;    /* returned with the completion */
+} avx_request;
+
+typedef struct avx_completion {
+  unsigned long long tag;
+  int status;                /* avx_status of the run */
+  int dft_mode;              /* form the Cartesian operator used */
+  avx_run_stats stats;
+  double queue_ms;           /* submit -> start (host clock) */
+  double run_ms;             /* start -> finished, operator set-up included (host clock) */
+  size_t workspace_bytes;    /* the admission estimate */
+} avx_completion;
+
+typedef struct avx_batch avx_batch;
+
+/* Device bytes a request needs while it runs (operator, solver, tables). */
+avx_status avx_query_workspace(const avx_request* r, size_t* bytes);
+/* device: CUDA ordinal; hbm_budget: bytes the running requests may hold
+ * together; workers: concurrent reconstructions at most (>= 1). */
+avx_status avx_batch_create(int device, size_t hbm_budget, int workers, avx_batch** out);
+/* Queues a copy of *r.  AVX_E_NOMEM when its workspace exceeds the whole budget. */
+avx_status avx_batch_submit(avx_batch* b, const avx_request* r);
+/* Moves up to max finished requests to out (*n of them), waiting up to
+ * wait_ms for the first (0: do not wait, negative: until one finishes or
+ * nothing is pending). */
+avx_status avx_serve_poll(avx_batch* b, avx_completion* out, int max, int* n, int wait_ms);
+/* Blocks until every submitted request has finished (completions stay queued). */
+avx_status avx_batch_drain(avx_batch* b);
+/* Requests submitted and not yet polled. */
+int avx_batch_pending(const avx_batch* b);
+/* Stops the workers after the running requests; queued requests are dropped. */
+void avx_batch_destroy(avx_batch* b);
 
 /* ------------------------------------------------------------------ */
 /* Host-buffer reconstruction (the CLI path, main.cpp:507-839)         */

@@ -54,3 +54,48 @@ def test_cpu_only_entry_points():
         av.default_params(av.TGV2_3D)
     with pytest.raises(av.AvionicError):
         av.time_space_weights(-1.0)
+
+
+STRUCTS = {
+    # C type: ctypes mirror name in avionic_b200._abi
+    "avx_pd_params": "PDParams",
+    "avx_run_stats": "RunStats",
+    "avx_coil_params": "CoilParams",
+    "avx_request": "Request",
+    "avx_completion": "Completion",
+}
+
+
+@pytest.mark.skipif(not os.path.exists(LIB), reason="library not built")
+def test_struct_layouts_match_the_header(tmp_path):
+    """sizeof and every field offset of the ABI structs, as gcc lays them out
+    from include/avionic.h, equal the ctypes mirrors."""
+    import shutil
+    import subprocess
+    from avionic_b200 import _abi
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("gcc not available")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "avionic.h"', "int main(void) {"]
+    for ctype, pyname in STRUCTS.items():
+        cls = getattr(_abi, pyname)
+        lines.append('printf("%s sizeof %%zu\\n", sizeof(%s));' % (ctype, ctype))
+        for fname, _ in cls._fields_:
+            cf = "lambda" if fname == "lambda_" else fname
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (ctype, fname, ctype, cf))
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([gcc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for ln in out:
+        if ln.strip():
+            c, f, v = ln.split()
+            got[(c, f)] = int(v)
+    for ctype, pyname in STRUCTS.items():
+        cls = getattr(_abi, pyname)
+        assert got[(ctype, "sizeof")] == ctypes.sizeof(cls), ctype
+        for fname, _ in cls._fields_:
+            assert got[(ctype, fname)] == getattr(cls, fname).offset, (ctype, fname)
