@@ -194,6 +194,10 @@ class Solver:
     def set_debug(self, debug, debugstep=1):
         check(lib.avx_solver_set_debug(self.handle, int(debug), int(debugstep)))
 
+    def set_relative_stop(self, rel):
+        """Also stop once the gap falls to rel times the run's first gap."""
+        check(lib.avx_solver_set_relative_stop(self.handle, float(rel)))
+
     def set_verbose(self, verbose):
         check(lib.avx_solver_set_verbose(self.handle, int(verbose)))
 
@@ -369,7 +373,7 @@ Completion = _abi.Completion
 
 
 def cartesian_request(method, data, x, b1, mask=None, params=None, centered=False, dft_mode=DFT_SPLIT_BF16X3,
-                      tag=0):
+                      tag=0, stop_gap_rel=0.0):
     """avx_request for a Cartesian reconstruction.  data (T,C,H,W), x (T,H,W)
     initial image in / result out, b1 (C,H,W), mask (T,H,W) float32 or None:
     CUDA tensors that must stay alive until the completion is polled."""
@@ -385,11 +389,12 @@ def cartesian_request(method, data, x, b1, mask=None, params=None, centered=Fals
     r.centered = int(centered)
     r.d_data, r.d_x, r.d_b1 = _cptr(data), _cptr(x), _cptr(b1)
     r.tag = int(tag)
+    r.stop_gap_rel = float(stop_gap_rel)
     return r
 
 
 def radial_request(method, data, x, b1, traj, dens, spokes_per_frame, n_fe, params=None, kernel_width=3.0,
-                   sector_width=8.0, osf=2.0, tag=0):
+                   sector_width=8.0, osf=2.0, tag=0, stop_gap_rel=0.0):
     """avx_request for a radial reconstruction: data (T,C,S) sqrt(w)-weighted,
     traj (T,2,S), dens (T,S) float32, x (T,H,W), b1 (C,H,W)."""
     if isinstance(method, str):
@@ -405,6 +410,7 @@ def radial_request(method, data, x, b1, traj, dens, spokes_per_frame, n_fe, para
     r.kernel_width, r.sector_width, r.osf = kernel_width, sector_width, osf
     r.d_data, r.d_x, r.d_b1 = _cptr(data), _cptr(x), _cptr(b1)
     r.tag = int(tag)
+    r.stop_gap_rel = float(stop_gap_rel)
     return r
 
 

@@ -41,7 +41,7 @@ class Request(C.Structure):
         ("params", PDParams), ("dft_mode", I), ("d_mask", VP), ("centered", I),
         ("n_fe", U), ("spokes_per_frame", U), ("d_traj", VP), ("d_dens", VP),
         ("kernel_width", F), ("sector_width", F), ("osf", F),
-        ("d_data", VP), ("d_x", VP), ("d_b1", VP), ("tag", C.c_ulonglong),
+        ("d_data", VP), ("d_x", VP), ("d_b1", VP), ("tag", C.c_ulonglong), ("stop_gap_rel", F),
     ]
 
 
@@ -72,6 +72,7 @@ SIGNATURES = {
     "avx_solver_set_params": (I, [VP, C.POINTER(PDParams)]),
     "avx_solver_set_verbose": (I, [VP, I]),
     "avx_solver_set_debug": (I, [VP, I, I]),
+    "avx_solver_set_relative_stop": (I, [VP, D]),
     "avx_solver_set_stream": (I, [VP, VP]),
     "avx_solver_run": (I, [VP, VP, VP, VP]),
     "avx_solver_adapt_step_size": (I, [VP, C.POINTER(VP), VP]),

@@ -58,6 +58,7 @@ struct DevState {
   int iters;              // iterations started (dual_kernel increments it)
   int err;                // non-zero when a device-side check failed
   double d_off;           // energy of the data outside the sampled rows (gap constant)
+  double gap0;            // first normalised gap of the run (relative stop criterion)
 };
 
 // Number of FP64 partial-sum slots a reduction writes per block.

@@ -551,6 +551,7 @@ struct avx_solver {
   avx_operator* op = nullptr;
   bool verbose = false, debug = false;
   int debugstep = 1;
+  double stop_rel = 0.0;  // relative gap stop (avx_solver_set_relative_stop)
   cudaStream_t user_stream = 0;
   cudaStream_t stream = 0;
   // device state
@@ -696,13 +697,15 @@ static avx::GapConst make_gapconst(avx_solver* s) {
   gc.alpha1 = s->p.alpha1;
   gc.ic_a = alpha / m;
   gc.ic_b = (1.0 - alpha) / m;
+  gc.stop_rel = s->stop_rel;
   return gc;
 }
 
 static bool step_due(unsigned k) { return k < 10 || k % 50 == 0; }
+static bool stop_active(const avx_solver* s) { return s->p.stopPDGap > 0 || s->stop_rel > 0; }
 static bool gap_due(const avx_solver* s, unsigned k) {
   return (s->verbose && (k < 10 || k % 50 == 0)) || (s->debug && s->debugstep > 0 && k % (unsigned)s->debugstep == 0) ||
-         (s->p.stopPDGap > 0 && k % 20 == 0);
+         (stop_active(s) && k % 20 == 0);
 }
 
 static unsigned shape_launches(int kind, int shape) {
@@ -904,7 +907,7 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
       cudaGraphDestroy(g);
     }
     AVX_CK(cudaGraphLaunch(s->gexec[shape], s->stream));
-    if (s->p.stopPDGap > 0 && (shape & 2) && (k % 100 == 0)) {
+    if (stop_active(s) && (shape & 2) && (k % 100 == 0)) {
       int stop = 0;
       AVX_CK(cudaMemcpyAsync(&stop, &s->st.p->stop, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
       AVX_CK(cudaStreamSynchronize(s->stream));
@@ -1469,6 +1472,14 @@ avx_status avx_solver_set_verbose(avx_solver* s, int v) {
   s->verbose = v != 0;
   return AVX_OK;
 }
+avx_status avx_solver_set_relative_stop(avx_solver* s, double rel) {
+  if (!s) return fail(AVX_E_ARG, "null solver");
+  if (!(rel >= 0.0) || rel >= 1.0) return fail(AVX_E_ARG, "relative stop must lie in [0, 1)");
+  s->stop_rel = rel;
+  s->drop_graphs();
+  return AVX_OK;
+}
+
 avx_status avx_solver_set_debug(avx_solver* s, int debug, int debugstep) {
   if (!s) return fail(AVX_E_ARG, "null solver");
   s->debug = debug != 0;
@@ -1546,6 +1557,7 @@ avx_status avx_solver_compute_gap(avx_solver* s, const avx_cf32* const* d_x, con
   const KArgs kx = make_kargs(s, reinterpret_cast<const float2*>(d_b1), s->primc(0), nullptr);
   avx::GapConst gc = make_gapconst(s);
   gc.stop_gap = -1.0;
+  gc.stop_rel = 0.0;
   double* h = s->hist.p;
   int nk = s->C * s->T;
   if (s->op->kind == 1) {
@@ -2036,6 +2048,7 @@ avx_completion run_request(const avx_request& r, cudaStream_t stream) {
   }
   if (e == AVX_OK) e = avx_solver_create(r.method, r.width, r.height, r.coils, r.frames, &r.params, op, &s);
   if (e == AVX_OK) e = avx_solver_set_stream(s, stream);
+  if (e == AVX_OK && r.stop_gap_rel > 0.f) e = avx_solver_set_relative_stop(s, r.stop_gap_rel);
   if (e == AVX_OK) e = avx_solver_run(s, r.d_data, r.d_x, r.d_b1);
   if (e == AVX_OK) avx_solver_get_stats(s, &c.stats);
   c.status = (int)e;

@@ -723,7 +723,8 @@ __global__ void gap_finalize_kernel(DevState* st, const double* pk, int nk, cons
     return;
   }
   st->gap = gap;
-  const bool stop = gap < gc.stop_gap;
+  if (st->gap0 == 0.0) st->gap0 = gap;
+  const bool stop = gap < gc.stop_gap || (gc.stop_rel > 0.0 && gap <= gc.stop_rel * st->gap0);
   // TGV2 returns before recording the gap that stops it (tgv2.cpp:325-328)
   const bool record = !(M == AVX_M_TGV2 && stop);
   if (record && st->ngap < cap) {

@@ -27,6 +27,7 @@ struct Ptr8 {
 struct GapConst {
   double lam, N, stop_gap;  // the data-energy constant is DevState::d_off
   double alpha0, alpha1, ic_a, ic_b;
+  double stop_rel;          // > 0: also stop once gap <= stop_rel * first gap
 };
 
 size_t kspace_smem_bytes(int W, int H);  // largest dynamic shared memory of the transform kernels

@@ -178,6 +178,11 @@ avx_status avx_solver_get_params(const avx_solver* s, avx_pd_params* params); /*
 avx_status avx_solver_set_params(avx_solver* s, const avx_pd_params* params);
 avx_status avx_solver_set_verbose(avx_solver* s, int verbose);               /* SetVerbose */
 avx_status avx_solver_set_debug(avx_solver* s, int debug, int debugstep);    /* SetDebug */
+/* No reference counterpart (the reference stops on the absolute gap only,
+ * tv.cpp:189, tgv2.cpp:325, ictgv2.cpp:478): rel > 0 also ends the run at the
+ * first gap evaluation with gap <= rel * (the run's first gap).  Evaluations
+ * then happen every 20 iterations, as with stopPDGap.  rel in [0, 1). */
+avx_status avx_solver_set_relative_stop(avx_solver* s, double rel);
 avx_status avx_solver_set_stream(avx_solver* s, void* cuda_stream);          /* cudaStream_t, 0 = default */
 
 /* IterativeReconstruction(data, x, b1) (pd_recon.h:134-135): d_data dense
@@ -361,6 +366,7 @@ typedef struct avx_request {
   avx_cf32* d_x;             /* T*H*W initial image in, reconstruction out */
   const avx_cf32* d_b1;      /* C*H*W coil maps */
   unsigned long long tag;    /* returned with the completion */
+  float stop_gap_rel;        /* > 0: avx_solver_set_relative_stop(stop_gap_rel) for this run */
 } avx_request;
 
 typedef struct avx_completion {

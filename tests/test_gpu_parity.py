@@ -173,6 +173,37 @@ def test_stop_criterion(av, method, stop):
     assert rel(xg, xo) < REL_IMG
 
 
+@pytest.mark.parametrize("method", ["TV", "TGV2", "ICTGV2"])
+def test_relative_stop(av, method):
+    """avx_solver_set_relative_stop ends the loop at the first gap evaluation
+    (every 20 iterations) whose gap is at most rel times the first gap; rel is
+    placed between two evaluations of the oracle's gap history."""
+    from avionic_b200 import synth
+    prob = synth.small(6)
+    _, tro, _ = _oracle_run(method, prob, 400, debugstep=20)
+    r = np.asarray(tro["PDGap"]) / tro["PDGap"][0]
+    run_min = np.minimum.accumulate(r)
+    js = [j for j in range(3, len(r)) if r[j] < 0.98 * run_min[j - 1]]
+    assert js, "the oracle's gap does not fall"
+    j = js[0]
+    rel_stop = float(np.sqrt(run_min[j - 1] * r[j]))
+    import torch
+    T, C, H, W = prob["kdata"].shape
+    op = av.CartesianOperator(W, H, C, T, mask=av.to_device(prob["mask"]), centered=False)
+    s = av.Solver(method, op)
+    p = s.params
+    p.maxIt = 400
+    s.params = p
+    s.set_relative_stop(rel_stop)
+    x = torch.zeros((T, H, W), dtype=torch.complex64, device="cuda")
+    s.run(av.to_device(prob["kdata"]), x, av.to_device(prob["b1"]))
+    st = s.stats()
+    assert st.stopped_by_gap == 1
+    assert st.iterations == 20 * j + 1
+    xo, _, _ = _oracle_run(method, prob, 20 * j + 1)
+    assert rel(x.cpu().numpy(), xo) < REL_IMG
+
+
 def test_config0_tv_full(av):
     """Benchmark configuration 0 (128x128, 20 frames, 8 coils, 500 iterations)."""
     from avionic_b200 import synth
