@@ -6,6 +6,8 @@
 // symmetrised gradient (xx, yy, xy with 1/2 on the off-diagonal),
 // divergences as their negative adjoints (utils.cpp:156-181, 525-568,
 // 664-684, 817-844, 1078-1117).
+#include <algorithm>
+
 #include "coils.cuh"
 #include "stencil.cuh"
 
@@ -430,6 +432,19 @@ void launch_greedy_inputs(const float2* absb1, const float2* u, const float2* w,
 }
 void launch_abs_sum(const float2* a, const float2* b, int HW, double* partial, int nblocks, cudaStream_t s) {
   abs_sum_kernel<<<nblocks, 256, 0, s>>>(a, b, HW, partial);
+}
+
+// v *= f (agile::scale of the data normalisation, raw_data_preparation.cpp:792, 842)
+__global__ void cscale_kernel(float2* v, long long n, float f) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 a = v[i];
+    v[i] = make_float2(a.x * f, a.y * f);
+  }
+}
+
+void launch_cscale(float2* v, long long n, float f, cudaStream_t s) {
+  const long long nb = std::min<long long>((n + 255) / 256, 148 * 16);
+  if (nb > 0) cscale_kernel<<<(int)nb, 256, 0, s>>>(v, n, f);
 }
 
 }  // namespace avx

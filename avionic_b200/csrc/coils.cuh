@@ -41,6 +41,7 @@ void launch_phase_apply(const float2* absb1, const float2* x1, float2* out, int 
 void launch_weight_update(float2* w, const float2* b, int HW, cudaStream_t s);
 void launch_greedy_inputs(const float2* absb1, const float2* u, const float2* w, const float2* crec, float2* u_in,
                           float2* crec_in, int HW, cudaStream_t s);
+void launch_cscale(float2* v, long long n, float f, cudaStream_t s);
 void launch_abs_sum(const float2* a, const float2* b, int HW, double* partial, int nblocks, cudaStream_t s);
 
 }  // namespace avx

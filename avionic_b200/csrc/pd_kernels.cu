@@ -452,14 +452,14 @@ __global__ void __launch_bounds__(CA_TX* CA_TY) coladj_kernel(KArgs k, float2* i
 // ---------------------------------------------------------------------------
 
 template <int M>
-__global__ void __launch_bounds__(ADJ_TX* ADJ_TY) primal_kernel(PDArgs a) {
+__global__ void __launch_bounds__(PR_TX* PR_TY) primal_kernel(PDArgs a) {
   if (a.st->stop) return;
   const int t = blockIdx.z;
-  const int x0 = blockIdx.x * ADJ_TX, y0 = blockIdx.y * ADJ_TH;
-  float2 kh[ADJ_YP];
+  const int x0 = blockIdx.x * PR_TX, y0 = blockIdx.y * PR_TH;
+  float2 kh[PR_YP];
 #pragma unroll
-  for (int j = 0; j < ADJ_YP; ++j) {
-    const int y = y0 + threadIdx.y * ADJ_YP + j;
+  for (int j = 0; j < PR_YP; ++j) {
+    const int y = y0 + threadIdx.y * PR_YP + j;
     const int x = x0 + threadIdx.x;
     kh[j] = (x < a.W && y < a.H) ? a.khz[((long long)t * a.H + y) * a.W + x] : czero();
   }
@@ -467,8 +467,8 @@ __global__ void __launch_bounds__(ADJ_TX* ADJ_TY) primal_kernel(PDArgs a) {
   if (x >= a.W) return;
   const float tau = (float)a.st->tau;
 #pragma unroll
-  for (int j = 0; j < ADJ_YP; ++j) {
-    const int y = y0 + threadIdx.y * ADJ_YP + j;
+  for (int j = 0; j < PR_YP; ++j) {
+    const int y = y0 + threadIdx.y * PR_YP + j;
     if (y >= a.H) continue;
     const PixCoord p = make_pix(x, y, t, a.W, a.H, a.T);
     // every load of the pixel first (the stores below would otherwise order them)
@@ -805,8 +805,8 @@ void launch_dual(int method, const PDArgs& a, cudaStream_t s) {
 }
 
 void launch_primal(int method, const PDArgs& a, cudaStream_t s) {
-  dim3 gp((a.W + ADJ_TX - 1) / ADJ_TX, (a.H + ADJ_TH - 1) / ADJ_TH, a.T);
-  dim3 bl(ADJ_TX, ADJ_TY);
+  dim3 gp((a.W + PR_TX - 1) / PR_TX, (a.H + PR_TH - 1) / PR_TH, a.T);
+  dim3 bl(PR_TX, PR_TY);
   if (method == AVX_M_TV) primal_kernel<AVX_M_TV><<<gp, bl, 0, s>>>(a);
   else if (method == AVX_M_TGV2) primal_kernel<AVX_M_TGV2><<<gp, bl, 0, s>>>(a);
   else primal_kernel<AVX_M_ICTGV2><<<gp, bl, 0, s>>>(a);

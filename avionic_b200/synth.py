@@ -12,7 +12,18 @@ Shapes and value distributions follow the benchmark configurations:
   (radius factor 1 + 0.15 sin(2 pi t / 30)) over a static textured background
   of smoothed uniform noise; variable-density phase-encode lines (Gaussian
   line density, sigma 0.25 N) at acceleration 12, shifted per frame.
-* ``batched``: sizes drawn from the seed as in the batched configuration.
+* ``batched_specs`` / ``cine_instance_gpu``: 64 instances of uneven size
+  (matrix uniform in {96, 128, 160, 192, 256, 320}, frames 8-48, coils 4-32,
+  acceleration 6-16), each generated as ``config1`` from its own seed, with
+  the k-space formed on the GPU (torch.fft) so that large instances are quick.
+* ``config2_gpu``: radial golden-angle acquisition of the ``config1`` phantom
+  at 128 x 128 (256 readout samples, 21 spokes per frame, 40 frames, 12
+  coils); k-space by an exact float64 non-uniform DFT on the GPU, complex
+  Gaussian noise at 2e-3 of max |k|, sqrt(w)-weighted as the CLI weights it.
+* ``serving_stream``: a Poisson arrival stream mixing TV / TGV2 / ICTGV2 (50 /
+  30 / 20 %) and Cartesian (batched sizes) / radial (128 x 128 image, 256
+  readout samples, 13-34 golden-angle spokes per frame, 20-60 frames, 12
+  coils) requests (70 / 30 %).
 
 k-space is formed with the library's operator convention: the unitary 2D
 transform with the e^{+2 pi i} kernel from image to k-space (numpy ``ifft2``
@@ -151,3 +162,147 @@ def time_average_u0(kdata, mask, b1):
     cnt = np.maximum(mask.sum(axis=0), 1.0)
     img = np.fft.fft2(ksum / cnt[None], norm="ortho")
     return np.sum(np.conj(b1) * img, axis=0).astype(np.complex64)
+
+
+# ---------------------------------------------------------------------------
+# batched and served workloads
+# ---------------------------------------------------------------------------
+
+MATRICES = (96, 128, 160, 192, 256, 320)
+
+
+def batched_specs(seed=3, n=64):
+    """Sizes of the batched configuration, one dict per instance."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        m = int(rng.choice(MATRICES))
+        out.append(dict(W=m, H=m, T=int(rng.integers(8, 49)), C=int(rng.integers(4, 33)),
+                        R=int(rng.integers(6, 17)), seed=int(rng.integers(1 << 31))))
+    return out
+
+
+def cine_instance_gpu(spec, device="cuda", noise_rel=1e-3):
+    """A ``config1``-style instance at spec's sizes: returns CUDA tensors
+    kdata (T,C,H,W) masked, mask (T,H,W), b1 (C,H,W) and x0 (T,H,W), the
+    coil-combined zero-filled time average replicated over the frames."""
+    import torch
+    H, W, T, C = spec["H"], spec["W"], spec["T"], spec["C"]
+    rng = np.random.default_rng(spec["seed"])
+    x = torch.from_numpy(phantom_cine(H, W, T, rng, period=30).astype(np.complex64)).to(device)
+    b1 = torch.from_numpy(coil_maps(H, W, C, rng).astype(np.complex64)).to(device)
+    mask = torch.from_numpy(mask_variable_density(H, W, T, R=spec["R"], rng=rng)).to(device)
+    k = torch.empty((T, C, H, W), dtype=torch.complex64, device=device)
+    for t in range(T):
+        k[t] = torch.fft.ifft2(b1 * x[t], norm="ortho")
+    sd = noise_rel * float(k.abs().max())
+    g = torch.Generator(device=device)
+    g.manual_seed(spec["seed"])
+    k += (sd / np.sqrt(2.0)) * torch.complex(torch.randn(k.shape, generator=g, device=device),
+                                            torch.randn(k.shape, generator=g, device=device))
+    k *= mask[:, None]
+    cnt = torch.clamp(mask.sum(0), min=1.0)
+    img = torch.fft.fft2(k.sum(0) / cnt[None], norm="ortho")
+    u0 = (b1.conj() * img).sum(0)
+    x0 = u0[None].repeat(T, 1, 1).contiguous()
+    return dict(kdata=k, mask=mask, b1=b1, x0=x0)
+
+
+def golden_angle_radial(n_ro, spokes_per_frame, frames, angle_deg=111.246117975):
+    """Golden-angle radial trajectory (T, 2, S) float32 in [-0.5, 0.5) and a
+    ramp density (T, S) normalised to max 1; S = n_ro * spokes_per_frame."""
+    r = (np.arange(n_ro) - n_ro / 2.0) / n_ro
+    th = np.deg2rad(angle_deg) * np.arange(frames * spokes_per_frame).reshape(frames, spokes_per_frame)
+    kx = (np.cos(th)[:, :, None] * r[None, None, :]).reshape(frames, -1)
+    ky = (np.sin(th)[:, :, None] * r[None, None, :]).reshape(frames, -1)
+    traj = np.stack([kx, ky], axis=1).astype(np.float32)
+    dens = np.broadcast_to(np.abs(r) + 0.5 / n_ro, (frames, spokes_per_frame, n_ro)).reshape(frames, -1)
+    dens = (dens / dens.max()).astype(np.float32)
+    return traj, dens
+
+
+def radial_instance_gpu(spec, device="cuda", noise_rel=2e-3, kernel_width=3.0, sector_width=8.0, osf=1.5):
+    """A radial instance: the ``config1`` phantom at spec's image size, coil
+    maps as ``coil_maps``, golden-angle spokes; k-space = the library's radial
+    operator applied to the phantom (sqrt(w)-weighted, as the solver expects)
+    plus complex Gaussian noise.  Returns CUDA tensors kdata (T,C,S), traj,
+    dens, b1, x0 (zeros) and the sample counts."""
+    import torch
+    import avionic_b200 as av
+    H, W, T, C = spec["H"], spec["W"], spec["T"], spec["C"]
+    nfe, spf = spec["n_fe"], spec["spokes"]
+    rng = np.random.default_rng(spec["seed"])
+    x = torch.from_numpy(phantom_cine(H, W, T, rng, period=30).astype(np.complex64)).to(device)
+    b1 = torch.from_numpy(coil_maps(H, W, C, rng).astype(np.complex64)).to(device)
+    traj, dens = golden_angle_radial(nfe, spf, T)
+    traj, dens = torch.from_numpy(traj).to(device), torch.from_numpy(dens).to(device)
+    op = av.RadialOperator(W, H, C, T, traj, dens, spf, kernel_width, sector_width, osf)
+    k = op.backward(x, b1)
+    sd = noise_rel * float(k.abs().max())
+    g = torch.Generator(device=device)
+    g.manual_seed(spec["seed"])
+    k += (sd / np.sqrt(2.0)) * torch.complex(torch.randn(k.shape, generator=g, device=device),
+                                            torch.randn(k.shape, generator=g, device=device))
+    del op
+    return dict(kdata=k, traj=traj, dens=dens, b1=b1, x0=torch.zeros((T, H, W), dtype=torch.complex64,
+                                                                     device=device), n_fe=nfe, spokes=spf,
+                kernel_width=kernel_width, sector_width=sector_width, osf=osf)
+
+
+def serving_stream(seed=4, n=2000, rate=20.0):
+    """Request specs of the serving configuration with Poisson arrival times
+    (seconds from the start) at the given rate."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    out = []
+    for i in range(n):
+        method = ("TV", "TGV2", "ICTGV2")[int(rng.choice(3, p=[0.5, 0.3, 0.2]))]
+        if rng.random() < 0.7:
+            m = int(rng.choice(MATRICES))
+            spec = dict(kind="cartesian", W=m, H=m, T=int(rng.integers(8, 49)), C=int(rng.integers(4, 33)),
+                        R=int(rng.integers(6, 17)))
+        else:
+            spec = dict(kind="radial", W=128, H=128, T=int(rng.integers(20, 61)), C=12,
+                        spokes=int(rng.integers(13, 35)), n_fe=256)
+        spec.update(method=method, arrival=float(t[i]), seed=int(rng.integers(1 << 31)))
+        out.append(spec)
+    return out
+
+
+def nudft_gpu(u, traj_f):
+    """Exact non-uniform DFT in float64 on the GPU:
+    X[..., s] = sum_{y,x} u[..., y, x] exp(-2 pi i (kx_s px + ky_s py)),
+    p = index - floor(extent / 2); u (..., H, W) complex128, traj_f (2, S)."""
+    import torch
+    H, W = u.shape[-2:]
+    dev = u.device
+    kx = traj_f[0].to(dev, torch.float64)
+    ky = traj_f[1].to(dev, torch.float64)
+    px = torch.arange(W, device=dev, dtype=torch.float64) - W // 2
+    py = torch.arange(H, device=dev, dtype=torch.float64) - H // 2
+    ex = torch.exp(-2j * np.pi * torch.outer(px, kx))   # (W, S)
+    ey = torch.exp(-2j * np.pi * torch.outer(py, ky))   # (H, S)
+    return ((u @ ex) * ey).sum(-2)
+
+
+def config2_gpu(seed=2, H=128, W=128, T=40, C=12, n_fe=256, spokes=21, noise_rel=2e-3, device="cuda"):
+    """The radial configuration: returns CUDA tensors kdata (T, C, S)
+    sqrt(w)-weighted, traj (T, 2, S), dens (T, S) and the phantom."""
+    import torch
+    rng = np.random.default_rng(seed)
+    x = torch.from_numpy(phantom_cine(H, W, T, rng, period=30)).to(device)
+    b1 = torch.from_numpy(coil_maps(H, W, C, rng)).to(device)
+    traj, dens = golden_angle_radial(n_fe, spokes, T)
+    traj_d, dens_d = torch.from_numpy(traj).to(device), torch.from_numpy(dens).to(device)
+    S = traj.shape[2]
+    k = torch.empty((T, C, S), dtype=torch.complex128, device=device)
+    for t in range(T):
+        k[t] = nudft_gpu(b1 * x[t], traj_d[t]) / np.sqrt(W * H)
+    sd = noise_rel * float(k.abs().max())
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    k += (sd / np.sqrt(2.0)) * torch.complex(torch.randn(k.shape, generator=g, device=device, dtype=torch.float64),
+                                            torch.randn(k.shape, generator=g, device=device, dtype=torch.float64))
+    k *= torch.sqrt(dens_d.double())[:, None, :]
+    return dict(kdata=k.to(torch.complex64).contiguous(), traj=traj_d, dens=dens_d, truth=x.to(torch.complex64),
+                n_fe=n_fe, spokes=spokes)

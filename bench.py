@@ -182,6 +182,207 @@ def make_problem(seed):
     return prob
 
 
+def _batch_pass(av, torch, items, make_request, workers, dft, arrivals=None):
+    """Runs one request per item through a BatchEngine with the given worker
+    count and DFT form.  arrivals (seconds from the start, sorted) turns the
+    submissions into an open-loop arrival stream; otherwise every request is
+    submitted at once.  Returns the per-request completions, the outputs and
+    the wall time from the first submission to the last completion."""
+    outs = [it["x0"].clone() for it in items]
+    torch.cuda.synchronize()
+    eng = av.BatchEngine(0, hbm_budget=150 << 30, workers=workers)
+    reqs = [make_request(it, out, dft, i) for i, (it, out) in enumerate(zip(items, outs))]
+    done = {}
+    t0 = time.perf_counter()
+    for i, r in enumerate(reqs):
+        if arrivals is not None:
+            while True:
+                lag = arrivals[i] - (time.perf_counter() - t0)
+                if lag <= 0:
+                    break
+                got = eng.poll(wait_ms=max(1, int(lag * 1000)))
+                for c in got:
+                    done[c.tag] = (c, time.perf_counter() - t0)
+                if not got:
+                    time.sleep(min(lag, 0.002))  # nothing pending: poll returns at once
+        eng.submit(r)
+        for c in eng.poll(wait_ms=0):
+            done[c.tag] = (c, time.perf_counter() - t0)
+    while len(done) < len(reqs):
+        for c in eng.poll(wait_ms=-1):
+            done[c.tag] = (c, time.perf_counter() - t0)
+    wall = max(t for _, t in done.values())
+    eng.close()
+    comps = [done[i][0] for i in range(len(reqs))]
+    bad = [c.status for c in comps if c.status != 0]
+    if bad:
+        raise RuntimeError("batched requests failed with status %s" % bad[:4])
+    return comps, outs, wall
+
+
+def _rel_diff(torch, a, b):
+    return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+
+def run_batched(av, torch, workers, n=64, iters=800):
+    """The batched configuration: n TGV2 reconstructions of uneven size
+    (800 iterations each), submitted at once.  The plain form is FP32
+    y-transforms with one reconstruction at a time (workers = 1); the batched
+    form is split-BF16x3 with `workers` concurrent reconstructions."""
+    from avionic_b200 import synth
+    specs = synth.batched_specs(3, n)
+    items = [synth.cine_instance_gpu(sp) for sp in specs]
+    torch.cuda.synchronize()
+
+    def make_request(it, out, dft, tag):
+        p = av.default_params(av.TGV2)
+        p.maxIt = iters
+        return av.cartesian_request(av.TGV2, it["kdata"], out, it["b1"], mask=it["mask"], params=p,
+                                    dft_mode=dft, tag=tag)
+
+    _batch_pass(av, torch, items[:4], make_request, 2, av.DFT_SPLIT_BF16X3)  # warm-up: module loading
+    forms = {}
+    outs = {}
+    for name, w, dft in (("plain_fp32_single", 1, av.DFT_FP32), ("split_single", 1, av.DFT_SPLIT_BF16X3),
+                         ("fp32_batched", workers, av.DFT_FP32), ("split_batched", workers, av.DFT_SPLIT_BF16X3)):
+        comps, o, wall = _batch_pass(av, torch, items, make_request, w, dft)
+        its = sum(c.stats.iterations for c in comps)
+        lat = [c.queue_ms + c.run_ms for c in comps]
+        forms[name] = {"workers": w, "recons_per_s": n / wall, "pd_it_per_s": its / wall, "wall_s": wall,
+                       "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+                       "split_dft_instances": int(sum(c.dft_mode == av.DFT_SPLIT_BF16X3 for c in comps))}
+        outs[name] = o
+    ref = outs["plain_fp32_single"]
+    for name in forms:
+        forms[name]["max_rel_l2_vs_plain_fp32"] = max(_rel_diff(torch, a, b) for a, b in zip(outs[name], ref))
+    del items, outs
+    torch.cuda.empty_cache()
+    return {"workload": "%d TGV2 Cartesian reconstructions of uneven size (matrix 96-320, frames 8-48, coils 4-32, "
+                        "acceleration 6-16), %d iterations each, submitted at once" % (n, iters),
+            "forms": forms,
+            "speedup_split_batched_vs_plain_fp32_single": forms["split_batched"]["recons_per_s"] /
+            forms["plain_fp32_single"]["recons_per_s"],
+            "timing": "host wall clock from the first submission to the last completion (several streams)"}
+
+
+def run_serving(av, torch, workers, n, rates, max_it=1500, rel_gap=1e-4):
+    """The serving configuration on a bounded sample: n requests (50/30/20 %
+    TV/TGV2/ICTGV2, 70/30 % Cartesian/radial) arriving as a Poisson stream at
+    each rate; every request stops at a relative primal-dual gap of rel_gap or
+    at max_it iterations."""
+    from avionic_b200 import synth
+    specs = synth.serving_stream(4, n, 1.0)
+    items = []
+    for sp in specs:
+        it = synth.cine_instance_gpu(sp) if sp["kind"] == "cartesian" else synth.radial_instance_gpu(sp)
+        it["spec"] = sp
+        items.append(it)
+    torch.cuda.synchronize()
+
+    def make_request(it, out, dft, tag):
+        sp = it["spec"]
+        p = av.default_params(av.METHODS[sp["method"]])
+        p.maxIt = max_it
+        if sp["kind"] == "cartesian":
+            return av.cartesian_request(sp["method"], it["kdata"], out, it["b1"], mask=it["mask"], params=p,
+                                        dft_mode=dft, tag=tag, stop_gap_rel=rel_gap)
+        return av.radial_request(sp["method"], it["kdata"], out, it["b1"], it["traj"], it["dens"], it["spokes"],
+                                 it["n_fe"], params=p, kernel_width=it["kernel_width"],
+                                 sector_width=it["sector_width"], osf=it["osf"], tag=tag, stop_gap_rel=rel_gap)
+
+    unit_arrivals = np.array([sp["arrival"] for sp in specs])
+    res = {}
+    outs = {}
+    for name, w, dft in (("plain_fp32_single", 1, av.DFT_FP32), ("split_batched", workers, av.DFT_SPLIT_BF16X3)):
+        per_rate = []
+        for rate in rates:
+            comps, o, wall = _batch_pass(av, torch, items, make_request, w, dft, arrivals=unit_arrivals / rate)
+            lat = [c.queue_ms + c.run_ms for c in comps]
+            per_rate.append({"rate_req_per_s": rate, "recons_per_s": n / wall, "wall_s": wall,
+                             "latency_ms": {q: float(np.percentile(lat, v)) for q, v in
+                                            (("p50", 50), ("p95", 95), ("p99", 99))},
+                             "iterations_mean": float(np.mean([c.stats.iterations for c in comps])),
+                             "stopped_by_gap": int(sum(c.stats.stopped_by_gap for c in comps))})
+            outs[name] = o
+        res[name] = {"workers": w, "per_rate": per_rate}
+    res["max_rel_l2_split_batched_vs_plain_fp32"] = max(
+        _rel_diff(torch, a, b) for a, b in zip(outs["split_batched"], outs["plain_fp32_single"]))
+    del items, outs
+    torch.cuda.empty_cache()
+    return {"workload": "%d requests (sample of the 2000-request stream): 50/30/20%% TV/TGV2/ICTGV2, 70%% Cartesian "
+                        "(matrix 96-320, frames 8-48, coils 4-32) / 30%% radial (128x128, 256 readout samples, 13-34 "
+                        "spokes/frame, 20-60 frames, 12 coils), stop at relative gap %g or %d iterations, HBM budget "
+                        "150 GB" % (n, rel_gap, max_it),
+            "forms": res,
+            "timing": "host wall clock; latency = submission (arrival) to completion"}
+
+
+def run_radial(av, torch, iters=500, steps=3):
+    """The radial configuration: H1 coil-sensitivity estimation from the data,
+    then a TGV2 reconstruction (500 iterations, the reference's default) with
+    the Kaiser-Bessel gridding operator (width 3, grid oversampling 1.5,
+    sector width 8), the CLI's flow for radial data without coil maps."""
+    import ctypes
+    from avionic_b200 import synth
+    prob = synth.config2_gpu(2)
+    k, traj, dens = prob["kdata"], prob["traj"], prob["dens"]
+    T, C, S = k.shape
+    H, W = prob["truth"].shape[1:]
+    q = av.coil_default_params()
+    u = torch.empty((C, H, W), dtype=torch.complex64, device="cuda")
+    b1 = torch.empty_like(u)
+
+    def coils():
+        av.check(av.lib.avx_coil_construction_radial(W, H, C, T, S, ctypes.byref(q), av._cptr(traj), av._cptr(dens),
+                                                     av._cptr(k), av._cptr(u), av._cptr(b1)))
+
+    coils()
+    torch.cuda.synchronize()
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record()
+    coils()
+    c1.record()
+    torch.cuda.synchronize()
+    coil_ms = c0.elapsed_time(c1)
+    x0 = (u[C - 1] / T)[None].repeat(T, 1, 1).contiguous()  # u0 of the radial coil construction (main.cpp:636-640)
+    op = av.RadialOperator(W, H, C, T, traj, dens, prob["spokes"], 3.0, 8.0, 1.5)
+    p = av.default_params(av.TGV2)
+    p.maxIt = iters
+    solver = av.Solver(av.TGV2, op, p)
+    x = torch.empty_like(x0)
+    for _ in range(2):
+        x.copy_(x0)
+        solver.run(k, x, b1)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        x.copy_(x0)
+        solver.run(k, x, b1)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    solver.set_timing(True)
+    x.copy_(x0)
+    solver.run(k, x, b1)
+    torch.cuda.synchronize()
+    t_stage, n_timed = solver.kernel_times()
+    solver.set_timing(False)
+    truth = prob["truth"]
+    err = _rel_diff(torch, x, truth)
+    N = W * H * T
+    peak, _ = load_peaks()
+    stream = {"dual": 8 * N * (4 + 2 * 9), "primal": 8 * N * (1 + 3 * 4 + 9)}
+    names = ["dual", "grid_fft", "interp_prox", "spread_ifft_crop", "primal"]
+    kms = {n: float(t_stage[i]) for i, n in enumerate(names)}
+    return {"workload": "radial golden-angle TGV2, 128x128, 40 frames, 12 coils, 256 readout samples x 21 spokes "
+                        "per frame, KB width 3, osf 1.5, sector 8, %d iterations, H1 coil construction first" % iters,
+            "coil_construction_ms": coil_ms, "recon_ms": ms, "pd_it_per_s": iters / (ms / 1000.0),
+            "kernel_ms": kms,
+            "stream_kernels_frac_of_hbm": {n: stream[n] / (kms[n] / 1000.0) / 1e9 / peak for n in stream},
+            "rel_l2_vs_phantom": err}
+
+
 def run_reference(args, rank, world):
     """The reference arm: the oracle port on the host cores, rank 0 only."""
     if rank != 0:
@@ -221,7 +422,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dft", default="split", choices=["split", "fp32"],
                     help="arithmetic of the y-transforms: split-BF16x3 tensor cores or fp32 CUDA cores")
+    ap.add_argument("--parts", default="headline,radial,batched,serving",
+                    help="comma list: headline (config-1 line), radial, batched, serving (added to the line at N=1)")
+    ap.add_argument("--batch-workers", type=int, default=8, help="concurrent reconstructions of the batched forms")
+    ap.add_argument("--batch-size", type=int, default=64)
+    ap.add_argument("--serve-requests", type=int, default=8,
+                    help="requests per rate (bounded sample of the 2000-request stream)")
+    ap.add_argument("--serve-rates", default="200",
+                    help="comma list of arrival rates in requests/s (the configuration sweeps 20-200)")
     args = ap.parse_args()
+    parts = set(args.parts.split(","))
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -235,6 +445,17 @@ def main():
     import avionic_b200 as av
 
     torch.cuda.set_device(local)
+    extra = {}
+    if world == 1 and "batched" in parts:
+        extra["batched"] = run_batched(av, torch, args.batch_workers, args.batch_size)
+    if world == 1 and "radial" in parts:
+        extra["radial"] = run_radial(av, torch)
+    if world == 1 and "serving" in parts:
+        extra["serving"] = run_serving(av, torch, args.batch_workers, args.serve_requests,
+                                       [float(r) for r in args.serve_rates.split(",")])
+    if "headline" not in parts:
+        print(json.dumps(extra), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime
@@ -419,6 +640,7 @@ def main():
         "clocks": clk,
         "gpu_launches": int(launches * world),
     }
+    line.update(extra)
     print(json.dumps(line), flush=True)
 
 
