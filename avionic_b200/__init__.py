@@ -18,7 +18,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libavionic_core.so")
 
 TV, TVTEMP, TGV2, TGV2_3D, ICTV, ICTGV2 = 0, 1, 2, 3, 4, 5
-METHODS = {"TV": TV, "TGV2": TGV2, "ICTGV2": ICTGV2}
+METHODS = {"TV": TV, "TVTEMP": TVTEMP, "TGV2": TGV2, "ICTV": ICTV, "ICTGV2": ICTGV2}
 P_OF = {TV: 1, TGV2: 4, ICTGV2: 8}
 D_OF = {TV: 3, TGV2: 9, ICTGV2: 18}
 
@@ -341,6 +341,22 @@ def time_space_weights(tsw):
     ds, dt = ctypes.c_float(), ctypes.c_float()
     check(lib.avx_time_space_weights(ctypes.c_float(tsw), ctypes.byref(ds), ctypes.byref(dt)))
     return ds.value, dt.value
+
+
+def normalize_data(kdata, mask=None, traj=None, dens=None, width=None, height=None):
+    """The CLI's -o data normalisation (avx_normalize_data): scales the CUDA
+    k-space tensor kdata in place and returns the factor.  Cartesian: kdata
+    (T, C, H, W) and the mask (T, H, W); radial: kdata (T, C, S), traj
+    (T, 2, S), dens (T, S) and the image size."""
+    f = ctypes.c_float()
+    if traj is None:
+        T, C_, H, W = kdata.shape
+        check(lib.avx_normalize_data(W, H, C_, T, 0, _cptr(mask), None, _cptr(kdata), ctypes.byref(f)))
+    else:
+        T, C_, S = kdata.shape
+        check(lib.avx_normalize_data(width, height, C_, T, S, _cptr(traj), _cptr(dens), _cptr(kdata),
+                                     ctypes.byref(f)))
+    return f.value
 
 
 def reconstruct_host(method, kdata, mask, b1, u0=None, params=None, debugstep=0):

@@ -105,6 +105,7 @@ SIGNATURES = {
     "avx_coil_construction": (I, [U, U, U, U, C.POINTER(CoilParams), VP, VP, VP, VP]),
     "avx_coil_time_averaged_radial": (I, [U, U, U, U, U, VP, VP, VP, VP, VP, I]),
     "avx_coil_construction_radial": (I, [U, U, U, U, U, C.POINTER(CoilParams), VP, VP, VP, VP, VP]),
+    "avx_normalize_data": (I, [U, U, U, U, U, VP, VP, VP, C.POINTER(F)]),
     "avx_reconstruct_host": (I, [I, U, U, U, U, C.POINTER(PDParams), I, VP, VP, VP, VP, VP, C.POINTER(RunStats)]),
     "avx_reconstruct_host_release": (None, []),
     "avx_operator_set_dft_mode": (I, [VP, I]),

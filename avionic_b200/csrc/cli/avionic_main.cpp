@@ -7,7 +7,9 @@
 // (main.cpp:507-519), load b1 (-s) and u0 (-u) or form u0 as the coil-combined
 // time average, replicate u0 over the frames (main.cpp:775-779), run the
 // method, write the image, and with -e write x3_component, PDGap, ICTGVnorm
-// and DATAfidelity next to the output (main.cpp:915-917).
+// and DATAfidelity next to the output (main.cpp:915-917).  With -o the
+// k-space is normalised first (main.cpp:573-579) and the factor is written
+// to datanorm_factor.bin (main.cpp:793-796).
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -95,9 +97,9 @@ int main(int argc, char** argv) {
   const std::string mname = o.conf.count("method") ? o.conf["method"] : "ICTGV2";
   const int method = avcli::method_from_name(mname);
   if (method < 0) return die("invalid method selected");
-  if (method != AVX_METHOD_TV && method != AVX_METHOD_TGV2 && method != AVX_METHOD_ICTGV2)
-    return die("method " + mname + " is not provided by this build (TV, TGV2, ICTGV2 are)");
-  if (o.normalize) return die("data normalisation (-o) is not provided by this build");
+  if (method != AVX_METHOD_TV && method != AVX_METHOD_TVTEMP && method != AVX_METHOD_TGV2 &&
+      method != AVX_METHOD_ICTV && method != AVX_METHOD_ICTGV2)
+    return die("method " + mname + " is not provided by this build (TV, TVTEMP, TGV2, ICTV, ICTGV2 are)");
   avx_pd_params p;
   if (!avcli::params_for_method(o, method, &p, err)) return die(err);
 
@@ -155,6 +157,16 @@ int main(int argc, char** argv) {
   if (o.nonuniform) {
     if (cudaMalloc(&dd.p, S * T * sizeof(float)) != cudaSuccess) return die("device allocation failed");
     cudaMemcpy(dd.p, dens.data(), S * T * sizeof(float), cudaMemcpyHostToDevice);
+  }
+
+  // data normalisation (-o) before the coil maps and u0 (main.cpp:573-579)
+  float datanorm = 1.f;
+  if (o.normalize) {
+    std::cout << "Normalize binary data." << std::endl;
+    if (avx_normalize_data(W, H, C, T, o.nonuniform ? (unsigned)S : 0u, (const float*)dm.p, (const float*)dd.p,
+                           (avx_cf32*)dk.p, &datanorm) != AVX_OK)
+      return die(avx_last_error());
+    std::cout << "datanorm factor (in):" << datanorm << std::endl;
   }
 
   std::vector<cf> b1(HW * C, cf(1, 0)), u0(HW, cf(0, 0));
@@ -248,6 +260,10 @@ int main(int argc, char** argv) {
     return die(avx_last_error());
   avx_run_stats st;
   avx_solver_get_stats(s, &st);
+  if (o.normalize) {  // main.cpp:793-796
+    const std::vector<cd> dn{cd(datanorm, 0.0)};
+    if (!avcli::write_bin(outdir + "/datanorm_factor.bin", dn, true, &err)) return die(err);
+  }
   const auto t_run = std::chrono::steady_clock::now();
   std::cout << "Execution time: " << std::chrono::duration<double>(t_run - t_init).count() << "s (" << st.iterations
             << " iterations, " << st.elapsed_ms << " ms on the device)" << std::endl;

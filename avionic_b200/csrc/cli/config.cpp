@@ -238,21 +238,27 @@ bool params_for_method(const Options& o, int method, avx_pd_params* p, std::stri
     err = avx_last_error();
     return false;
   }
-  const std::string sec = method == AVX_METHOD_TV ? "tv" : method == AVX_METHOD_TGV2 ? "tgv2" : "ictgv2";
+  const std::string sec = method == AVX_METHOD_TV       ? "tv"
+                          : method == AVX_METHOD_TVTEMP ? "tvtemp"
+                          : method == AVX_METHOD_TGV2   ? "tgv2"
+                          : method == AVX_METHOD_ICTV   ? "ictv"
+                                                        : "ictgv2";
   auto f = [&](const char* k, float def) { return conf_f(o, sec + "." + k, def); };
-  p->dx = f("dx", p->dx);
-  p->dy = f("dy", p->dy);
+  // keys a section does not declare (options_parser.cpp:180-324) keep their defaults
+  if (method != AVX_METHOD_TVTEMP) {
+    p->dx = f("dx", p->dx);
+    p->dy = f("dy", p->dy);
+    p->timeSpaceWeight = f("timeSpaceWeight", p->timeSpaceWeight);
+  }
   p->dt = f("dt", p->dt);
   p->sigma = f("sigma", p->sigma);
   p->tau = f("tau", p->tau);
   p->sigmaTauRatio = f("sigmaTauRatio", p->sigmaTauRatio);
-  p->timeSpaceWeight = f("timeSpaceWeight", p->timeSpaceWeight);
   p->lambda = f("lambda", p->lambda);
-  if (method != AVX_METHOD_TV) {
-    p->alpha0 = f("alpha0", p->alpha0);
+  if (method == AVX_METHOD_TGV2 || method == AVX_METHOD_ICTGV2) p->alpha0 = f("alpha0", p->alpha0);
+  if (method == AVX_METHOD_TGV2 || method == AVX_METHOD_ICTV || method == AVX_METHOD_ICTGV2)
     p->alpha1 = f("alpha1", p->alpha1);
-  }
-  if (method == AVX_METHOD_ICTGV2) {
+  if (method == AVX_METHOD_ICTV || method == AVX_METHOD_ICTGV2) {
     p->alpha = f("alpha", p->alpha);
     p->timeSpaceWeight2 = f("timeSpaceWeight2", p->timeSpaceWeight2);
     p->dx2 = f("dx2", p->dx2);
@@ -287,7 +293,7 @@ void print_usage() {
             << "  -s [ --sens ] arg          coil sensitivity data\n"
             << "  -u [ --uzero ] arg         initial image u0\n"
             << "  -b [ --gpudevice ] arg (=-1)  GPU device number\n"
-            << "  -m [ --method ] arg (=ICTGV2) TV, TGV2, ICTGV2\n"
+            << "  -m [ --method ] arg (=ICTGV2) TV, TVTEMP, TGV2, ICTV, ICTGV2\n"
             << "  -i [ --maxIt ] arg (=500)  maximum number of iterations\n"
             << "  -j [ --stopPDGap ] arg (=0) stop at this normalised PD gap\n";
 }

@@ -10,6 +10,10 @@
 #define AVX_HD __host__ __device__ __forceinline__
 #define AVX_D __device__ __forceinline__
 
+// Dynamic shared memory a kernel may request: the 227 KB a CTA can hold on
+// sm_100, less 1 KB for the small static __shared__ arrays some kernels add.
+#define AVX_DYN_SMEM_MAX (227 * 1024 - 1024)
+
 AVX_HD float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 AVX_HD float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 AVX_HD float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
@@ -30,13 +34,21 @@ AVX_HD float2 czero() { return make_float2(0.f, 0.f); }
 
 // Reconstruction methods, numbered as the reference's Method enum
 // (CUDA/include/options_parser.h: TV, TVtemp, TGV2, TGV2_3D, ICTV, ICTGV2, ...).
-enum : int { AVX_M_TV = 0, AVX_M_TGV2 = 2, AVX_M_ICTGV2 = 5 };
+enum : int { AVX_M_TV = 0, AVX_M_TVTEMP = 1, AVX_M_TGV2 = 2, AVX_M_ICTV = 4, AVX_M_ICTGV2 = 5 };
 
 template <int M>
 struct MethodDims;
 template <>
 struct MethodDims<AVX_M_TV> {
   static constexpr int P = 1, D = 3;
+};
+template <>
+struct MethodDims<AVX_M_TVTEMP> {
+  static constexpr int P = 1, D = 1;
+};
+template <>
+struct MethodDims<AVX_M_ICTV> {
+  static constexpr int P = 2, D = 6;
 };
 template <>
 struct MethodDims<AVX_M_TGV2> {

@@ -166,9 +166,19 @@ Wts make_wts(float dx, float dy, float dt) {
   return w;
 }
 
-int method_P(int m) { return m == AVX_METHOD_TV ? 1 : m == AVX_METHOD_TGV2 ? 4 : 8; }
-int method_D(int m) { return m == AVX_METHOD_TV ? 3 : m == AVX_METHOD_TGV2 ? 9 : 18; }
-bool method_ok(int m) { return m == AVX_METHOD_TV || m == AVX_METHOD_TGV2 || m == AVX_METHOD_ICTGV2; }
+// primal and dual component counts: TV 1 / 3, TVtemp 1 / 1, TGV2 4 / 9, ICTV 2 / 6, ICTGV2 8 / 18
+int method_P(int m) {
+  return m == AVX_METHOD_TV || m == AVX_METHOD_TVTEMP ? 1 : m == AVX_METHOD_ICTV ? 2 : m == AVX_METHOD_TGV2 ? 4 : 8;
+}
+int method_D(int m) {
+  return m == AVX_METHOD_TVTEMP ? 1 : m == AVX_METHOD_TV ? 3 : m == AVX_METHOD_ICTV ? 6 : m == AVX_METHOD_TGV2 ? 9 : 18;
+}
+bool method_ok(int m) {
+  return m == AVX_METHOD_TV || m == AVX_METHOD_TVTEMP || m == AVX_METHOD_TGV2 || m == AVX_METHOD_ICTV ||
+         m == AVX_METHOD_ICTGV2;
+}
+// methods with a second TV branch (x3 component, second time-space weight, norm and fidelity histories)
+bool method_ic(int m) { return m == AVX_METHOD_ICTV || m == AVX_METHOD_ICTGV2; }
 
 __global__ void sumsq_kernel(const float2* v, long long n, double* partial) {
   __shared__ double red[32];
@@ -238,6 +248,8 @@ struct avx_operator {
   RadialGeomDev rg{};
   DevBuf<float> r_traj, r_sqrtw, r_ipx, r_ipy;
   DevBuf<int> r_order, r_secstart;
+  DevBuf<int2> r_win0;
+  DevBuf<float> r_winw;
   DevBuf<float2> r_twgx, r_twgy, r_grid;
   DevBuf<float2> r_khz;  // K^H z image (T x H x W), both operator kinds
   bool has_mask = false, binary = true;
@@ -457,7 +469,7 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
     g.radx[i] = i < g.nradx ? rx[i] : 0;
     g.rady[i] = i < g.nrady ? ry[i] : 0;
   }
-  if (avx::radial_fft_smem_bytes(std::max(g.Gx, g.Gy)) > 227 * 1024)
+  if (avx::radial_fft_smem_bytes(std::max(g.Gx, g.Gy)) > AVX_DYN_SMEM_MAX)
     return fail(AVX_E_UNSUPPORTED, "oversampled grid too large for the grid FFT tile");
   std::vector<float2> twx(g.Gx), twy(g.Gy);
   for (int j = 0; j < g.Gx; ++j) twx[j] = make_float2((float)std::cos(2.0 * M_PI * j / g.Gx), (float)std::sin(2.0 * M_PI * j / g.Gx));
@@ -488,6 +500,14 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
   g.sec_start = op->r_secstart.p;
   g.twgx = op->r_twgx.p;
   g.twgy = op->r_twgy.p;
+  // the samples' window starts and weights depend on the trajectory alone
+  AVX_CK(op->r_win0.alloc((size_t)T * S));
+  AVX_CK(op->r_winw.alloc((size_t)T * S * 2 * g.nw));
+  avx::launch_rad_windows(g, op->r_win0.p, op->r_winw.p, 0);
+  AVX_CK(cudaGetLastError());
+  AVX_CK(cudaStreamSynchronize(0));
+  g.win0 = op->r_win0.p;
+  g.winw = op->r_winw.p;
   return AVX_OK;
 }
 
@@ -504,7 +524,7 @@ static RArgs make_rargs(avx_operator* op, const float2* b1, const float2* in, co
 
 static avx_status check_dims(unsigned W, unsigned H, unsigned C, unsigned T) {
   if (!W || !H || !C || !T) return fail(AVX_E_ARG, "dimensions must be positive");
-  if (avx::kspace_smem_bytes((int)W, (int)H) > 227 * 1024)
+  if (avx::kspace_smem_bytes((int)W, (int)H) > AVX_DYN_SMEM_MAX)
     return fail(AVX_E_UNSUPPORTED, "image size exceeds the k-space kernel's shared-memory tile");
   if ((double)W * H * T * C > 4.0e9) return fail(AVX_E_ARG, "problem too large for 32-bit row offsets");
   return AVX_OK;
@@ -629,8 +649,12 @@ static PDArgs make_pdargs(avx_solver* s) {
   solver_weights(s, &a.w1, &a.w2);
   const double alpha = s->p.alpha;
   const double m = std::min(alpha, 1.0 - alpha);
-  if (s->method == AVX_METHOD_TV) {
-    a.r1 = 1.0f;  // ProximalMap3(y, 1.0) (tv.cpp:157)
+  if (s->method == AVX_METHOD_TV || s->method == AVX_METHOD_TVTEMP) {
+    a.r1 = 1.0f;  // ProximalMap3(y, 1.0) (tv.cpp:157), ProximalMap1D(y, 1.0) (tv_temp.cpp:136)
+  } else if (s->method == AVX_METHOD_ICTV) {
+    // ictv.cpp:272-278
+    a.r1 = (float)(1.0 / ((double)s->p.alpha1 * (alpha / m)));
+    a.r3 = (float)(1.0 / ((double)s->p.alpha1 * ((1.0 - alpha) / m)));
   } else if (s->method == AVX_METHOD_TGV2) {
     a.r1 = (float)(1.0 / (double)s->p.alpha1);  // tgv2.cpp:258-259
     a.r2 = (float)(1.0 / (double)s->p.alpha0);
@@ -762,7 +786,7 @@ static void enqueue_shape_radial(avx_solver* s, int shape, const float2* b1, cud
   if (shape & 2) {
     radial_pass(s, 2, b1, s->primc(0), nullptr);
     double* h = s->hist.p;
-    const bool ic = s->method == AVX_METHOD_ICTGV2;
+    const bool ic = method_ic(s->method);
     avx::launch_gap_tail(s->method, a, kdummy, s->pimg.p, s->pk.p, nk, make_gapconst(s), h,
                          ic ? h + (s->cap + 1) : nullptr, ic ? h + 2 * (s->cap + 1) : nullptr, s->cap, 0, s->stream);
   }
@@ -786,7 +810,7 @@ static void enqueue_shape(avx_solver* s, int shape, const float2* b1, cudaEvent_
   if (shape & 2) {
     const KArgs kx = make_kargs(s, b1, s->primc(0), nullptr);
     double* h = s->hist.p;
-    const bool ic = s->method == AVX_METHOD_ICTGV2;
+    const bool ic = method_ic(s->method);
     avx::launch_gap(s->method, a, kx, s->op->r_khz.p, s->pimg.p, s->pk.p, make_gapconst(s), h,
                     ic ? h + (s->cap + 1) : nullptr, ic ? h + 2 * (s->cap + 1) : nullptr, s->cap, 0, s->stream);
   }
@@ -835,10 +859,14 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
   avx_status r = solver_alloc(s);
   if (r != AVX_OK) return r;
   // the reference overwrites dx, dy, dt (and dx2..dt2) from the weights (tv.cpp:103-104)
+  // (TVtemp uses its configured dt as it is, tv_temp.cpp:98-103)
   double ds, dt;
-  if (!time_space_weights(s->p.timeSpaceWeight, &ds, &dt)) return fail(AVX_E_ARG, "ComputeTimeSpaceWeights: invalid ratio");
-  s->p.dx = (float)ds; s->p.dy = (float)ds; s->p.dt = (float)dt;
-  if (s->method == AVX_METHOD_ICTGV2) {
+  if (s->method != AVX_METHOD_TVTEMP) {
+    if (!time_space_weights(s->p.timeSpaceWeight, &ds, &dt))
+      return fail(AVX_E_ARG, "ComputeTimeSpaceWeights: invalid ratio");
+    s->p.dx = (float)ds; s->p.dy = (float)ds; s->p.dt = (float)dt;
+  }
+  if (method_ic(s->method)) {
     if (!time_space_weights(s->p.timeSpaceWeight2, &ds, &dt)) return fail(AVX_E_ARG, "ComputeTimeSpaceWeights: invalid ratio");
     s->p.dx2 = (float)ds; s->p.dy2 = (float)ds; s->p.dt2 = (float)dt;
   }
@@ -968,7 +996,7 @@ struct Fft2dTables {
 avx_status make_fft2d(int W, int H, Fft2dTables& t) {
   const std::vector<int> rx = fft_radices(W), ry = fft_radices(H);
   if (rx.empty() || ry.empty()) return fail(AVX_E_UNSUPPORTED, "image size has no FFT plan (prime factor > 13)");
-  if (avx::fft2d_smem_bytes(std::max(W, H)) > 227 * 1024) return fail(AVX_E_UNSUPPORTED, "image too large for the FFT tile");
+  if (avx::fft2d_smem_bytes(std::max(W, H)) > AVX_DYN_SMEM_MAX) return fail(AVX_E_UNSUPPORTED, "image too large for the FFT tile");
   std::vector<float2> hx(W), hy(H);
   for (int j = 0; j < W; ++j) hx[j] = make_float2((float)std::cos(2.0 * M_PI * j / W), (float)std::sin(2.0 * M_PI * j / W));
   for (int j = 0; j < H; ++j) hy[j] = make_float2((float)std::cos(2.0 * M_PI * j / H), (float)std::sin(2.0 * M_PI * j / H));
@@ -1411,7 +1439,7 @@ void avx_operator_destroy(avx_operator* op) { delete op; }
 
 avx_status avx_default_params(int method, avx_pd_params* p) {
   if (!p) return fail(AVX_E_ARG, "null params");
-  if (!method_ok(method)) return fail(AVX_E_UNSUPPORTED, "method not provided (TV, TGV2, ICTGV2 are)");
+  if (!method_ok(method)) return fail(AVX_E_UNSUPPORTED, "method not provided (TV, TVtemp, TGV2, ICTV, ICTGV2 are)");
   memset(p, 0, sizeof(*p));
   p->maxIt = 500;
   p->stopPDGap = 0.f;
@@ -1429,6 +1457,12 @@ avx_status avx_default_params(int method, avx_pd_params* p) {
     p->alpha = 0.6423f;
     p->adaptK = (float)(0.4 / (5.1191 * 0.35));
     p->adaptD = (float)(10.0 / (5.1191 * 0.35));
+  } else if (method == AVX_METHOD_ICTV) {
+    p->timeSpaceWeight = 4.f;  // ictv.cpp:37-60
+    p->timeSpaceWeight2 = 0.5f;
+    p->alpha = 0.5f;
+    p->adaptK = (float)(0.4 / (5.1191 * 0.35));
+    p->adaptD = (float)(10.0 / (5.1191 * 0.35));
   } else {
     p->timeSpaceWeight = 5.f;  // tv.cpp:48, tgv2.cpp:45
     p->adaptK = (float)(0.4 * 0.2991);
@@ -1441,7 +1475,7 @@ avx_status avx_default_params(int method, avx_pd_params* p) {
 avx_status avx_solver_create(int method, unsigned width, unsigned height, unsigned coils, unsigned frames,
                              const avx_pd_params* params, avx_operator* op, avx_solver** out) {
   if (!out || !op) return fail(AVX_E_ARG, "null argument");
-  if (!method_ok(method)) return fail(AVX_E_UNSUPPORTED, "method not provided (TV, TGV2, ICTGV2 are)");
+  if (!method_ok(method)) return fail(AVX_E_UNSUPPORTED, "method not provided (TV, TVtemp, TGV2, ICTV, ICTGV2 are)");
   if ((int)width != op->W || (int)height != op->H || (int)coils != op->C || (int)frames != op->T)
     return fail(AVX_E_ARG, "solver dimensions differ from the operator's");
   avx_solver* s = new avx_solver();
@@ -1584,8 +1618,10 @@ avx_status avx_solver_compute_gap(avx_solver* s, const avx_cf32* const* d_x, con
   const double lam = s->p.lambda;
   const double g = 0.5 * lam * (v[0] + s->d_off_energy) + v[1] + v[2] / (2.0 * lam) + v[3] + v[4] + v[5] + v[6];
   double reg;
-  if (s->method == AVX_METHOD_TV)
+  if (s->method == AVX_METHOD_TV || s->method == AVX_METHOD_TVTEMP)
     reg = v[7];
+  else if (s->method == AVX_METHOD_ICTV)
+    reg = s->p.alpha1 * gc.ic_a * v[7] + s->p.alpha1 * gc.ic_b * v[9];
   else if (s->method == AVX_METHOD_TGV2)
     reg = s->p.alpha1 * v[7] + s->p.alpha0 * v[8];
   else
@@ -1602,9 +1638,10 @@ avx_status avx_solver_export(avx_solver* s, const char* dir, avx_export_cb cb, v
     for (size_t i = 0; i < v.size(); ++i) c[i] = avx_cf32{(float)v[i], 0.f};
     cb(dir, name, c.data(), c.size(), user);
   };
-  if (s->method == AVX_METHOD_ICTGV2 && s->prim.p) {
+  if (method_ic(s->method) && s->prim.p) {
     std::vector<avx_cf32> x3((size_t)s->N());
-    AVX_CK(cudaMemcpy(x3.data(), s->primc(4), x3.size() * sizeof(avx_cf32), cudaMemcpyDeviceToHost));
+    AVX_CK(cudaMemcpy(x3.data(), s->primc(s->method == AVX_METHOD_ICTV ? 1 : 4), x3.size() * sizeof(avx_cf32),
+                      cudaMemcpyDeviceToHost));
     cb(dir, "x3_component", x3.data(), x3.size(), user);
   }
   if (s->debug && s->hist.p) {
@@ -1616,6 +1653,10 @@ avx_status avx_solver_export(avx_solver* s, const char* dir, avx_export_cb cb, v
       const size_t o = s->cap + 1;
       send("ICTGVnorm", std::vector<double>(h.begin() + o, h.begin() + o + ng + 1));
       send("DATAfidelity", std::vector<double>(h.begin() + 2 * o, h.begin() + 2 * o + ng + 1));
+    } else if (s->method == AVX_METHOD_ICTV) {  // ictv.cpp:375-390, no pre-loop record
+      const size_t o = s->cap + 1;
+      send("ictvnorm", std::vector<double>(h.begin() + o, h.begin() + o + ng));
+      send("DATAfidelity", std::vector<double>(h.begin() + 2 * o, h.begin() + 2 * o + ng));
     }
   }
   return AVX_OK;
@@ -1853,6 +1894,63 @@ avx_status avx_coil_time_averaged_radial(unsigned W, unsigned H, unsigned C, uns
   return coil_time_averaged_radial((int)W, (int)H, (int)C, (int)T, (int)S, d_traj, d_dens,
                                    reinterpret_cast<const float2*>(d_kdata), reinterpret_cast<float2*>(d_u),
                                    reinterpret_cast<float2*>(d_crec), apply_phase, 0);
+}
+
+// FindNormalizationFactor (raw_data_preparation.cpp:661-686): the first
+// largest value, then every later value >= 0.9 of it in scan order (values
+// before the first maximum are not considered), and utils::Median of those
+// (utils.cpp:1442-1462: the mean of the two middle values for an even count).
+static float find_normalization_factor(const std::vector<float>& v) {
+  size_t imax = 0;
+  for (size_t i = 1; i < v.size(); ++i)
+    if (v[i] > v[imax]) imax = i;
+  const double thr = (double)v[imax] * 0.9;
+  std::vector<float> big{v[imax]};
+  for (size_t i = imax + 1; i < v.size(); ++i)
+    if ((double)v[i] >= thr) big.push_back(v[i]);
+  std::sort(big.begin(), big.end());
+  const size_t ind = (size_t)(big.size() * 0.5);
+  if (big.size() % 2 == 0) return (float)(0.5 * (double)(big[ind] + big[ind - 1]));
+  return big[ind];
+}
+
+avx_status avx_normalize_data(unsigned W, unsigned H, unsigned C, unsigned T, unsigned S, const float* d_mask,
+                              const float* d_dens, avx_cf32* d_kdata, float* datanorm) {
+  if (!d_mask || !d_kdata || !datanorm || (S > 0 && !d_dens)) return fail(AVX_E_ARG, "null argument");
+  if (!W || !H || !C || !T) return fail(AVX_E_ARG, "empty dimensions");
+  avx_status r = configure_once();
+  if (r != AVX_OK) return r;
+  const size_t HW = (size_t)W * H;
+  DevBuf<float2> u, crec;
+  AVX_CK(u.alloc(HW));
+  AVX_CK(crec.alloc((size_t)C * HW));
+  float2* kd = reinterpret_cast<float2*>(d_kdata);
+  // |u| = sqrt(sum_c |crec_c|^2) of the time-averaged reconstruction without phase
+  r = S > 0 ? coil_time_averaged_radial((int)W, (int)H, (int)C, (int)T, (int)S, d_mask, d_dens, kd, u.p, crec.p, 0, 0)
+            : coil_time_averaged((int)W, (int)H, (int)C, (int)T, kd, d_mask, u.p, crec.p, 0, 0);
+  if (r != AVX_OK) return r;
+  std::vector<float2> hu(HW);
+  AVX_CK(cudaMemcpy(hu.data(), u.p, HW * sizeof(float2), cudaMemcpyDeviceToHost));
+  // The Cartesian normalisation transforms with the centred FFT
+  // (raw_data_preparation.cpp:372-373), whose image magnitude is the
+  // uncentred one shifted by (W/2, H/2); the scan order below follows it.
+  std::vector<float> mag(HW);
+  for (unsigned y = 0; y < H; ++y)
+    for (unsigned x = 0; x < W; ++x) {
+      const size_t src = S > 0 ? (size_t)y * W + x : (size_t)((y + H - H / 2) % H) * W + (x + W - W / 2) % W;
+      const float2 v = hu[src];
+      mag[(size_t)y * W + x] = std::sqrt(v.x * v.x + v.y * v.y);
+    }
+  const float median = find_normalization_factor(mag);
+  if (!(median > 0.f) || !std::isfinite(median))
+    return fail(AVX_E_NUMERIC, "no valid normalisation factor (the time-averaged image is zero or not finite)");
+  const float f = S > 0 ? 255.f * (float)T / median : 255.f / median;
+  const long long n = S > 0 ? (long long)S * C * T : (long long)HW * C * T;
+  avx::launch_cscale(kd, n, f, 0);
+  AVX_CK(cudaGetLastError());
+  AVX_CK(cudaStreamSynchronize(0));
+  *datanorm = f;
+  return AVX_OK;
 }
 
 avx_status avx_coil_construction_radial(unsigned W, unsigned H, unsigned C, unsigned T, unsigned S,
@@ -2117,7 +2215,7 @@ extern "C" {
 
 avx_status avx_query_workspace(const avx_request* r, size_t* bytes) {
   if (!r || !bytes) return fail(AVX_E_ARG, "null argument");
-  if (!method_ok(r->method)) return fail(AVX_E_UNSUPPORTED, "method not provided (TV, TGV2, ICTGV2 are)");
+  if (!method_ok(r->method)) return fail(AVX_E_UNSUPPORTED, "method not provided (TV, TVtemp, TGV2, ICTV, ICTGV2 are)");
   if (r->op_kind != 0 && r->op_kind != 1) return fail(AVX_E_ARG, "op_kind must be 0 (Cartesian) or 1 (radial)");
   if (!r->width || !r->height || !r->coils || !r->frames) return fail(AVX_E_ARG, "dimensions must be positive");
   if (r->op_kind == 1 && (!r->d_traj || !r->d_dens || !r->n_fe || !r->spokes_per_frame))

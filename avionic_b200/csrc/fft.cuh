@@ -28,7 +28,9 @@ AVX_D void small_dft(const float2* src, float2* dst, const float2* tw, int j, in
     const float2 s0 = src[(j + r * nb) * KCP + kk];
     v[r] = r ? cmul(s0, tw_sign(tw, r * k * tws, sign)) : s0;
   }
-#pragma unroll
+  // outputs one at a time: unrolling them all as well costs registers (and
+  // spills) for the larger radices
+#pragma unroll 1
   for (int q = 0; q < R; ++q) {
     float2 acc = v[0];
 #pragma unroll
@@ -43,7 +45,20 @@ AVX_D void small_dft(const float2* src, float2* dst, const float2* tw, int j, in
 AVX_D unsigned div_magic(unsigned d) { return d == 1u ? 0u : 0xFFFFFFFFu / d + 1u; }
 AVX_D int fast_div(int j, unsigned d, unsigned m) { return d == 1u ? j : (int)__umulhi((unsigned)j, m); }
 
-template <int KC>
+// The radix plans live in the kernels' parameter structs.  Handing row_fft a
+// pointer into one would make every thread copy the struct to local memory;
+// instead thread 0 copies the plan to shared memory with constant indices.  A
+// __syncthreads() must separate this from row_fft.
+AVX_D void stage_plan(const int (&rad)[12], int* splan) {
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < 12; ++i) splan[i] = rad[i];
+  }
+}
+
+// LARGE = false compiles the radix-2/3/4/5 passes only (the plans of sizes
+// whose prime factors are at most 5), which keeps the register count down.
+template <int KC, bool LARGE = true>
 __device__ float2* row_fft(float2* src, float2* dst, const float2* tw, int W, int nrad, const int* rad, int sign) {
   constexpr int KCP = KC + 2;
   int Ns = 1;
@@ -88,7 +103,7 @@ __device__ float2* row_fft(float2* src, float2* dst, const float2* tw, int W, in
         dst[idxD * KCP + kk] = cadd(v0, t1);
         dst[(idxD + Ns) * KCP + kk] = cadd(t2, id);
         dst[(idxD + 2 * Ns) * KCP + kk] = csub(t2, id);
-      } else if (R == 5) {
+      } else if (!LARGE || R == 5) {
         small_dft<5, KCP>(src, dst, tw, j, nb, k, tws, idxD, Ns, kk, W, sign);
       } else if (R == 7) {
         small_dft<7, KCP>(src, dst, tw, j, nb, k, tws, idxD, Ns, kk, W, sign);

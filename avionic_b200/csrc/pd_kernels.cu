@@ -49,55 +49,86 @@ __global__ void __launch_bounds__(256) dual_kernel(PDArgs a) {
     prox_div<3>(y, nrm3(y), a.r1);
 #pragma unroll
     for (int k = 0; k < 3; ++k) a.y[k][p.i] = y[k];
+  } else if (M == AVX_M_TVTEMP) {
+    // y += sigma D_t xbar / dt, y /= max(1, |y|) (tv_temp.cpp:129-136, ProximalMap1D utils.cpp:1307-1311)
+    const float2 g = tgrad(a.xb[0], p, a.w1);
+    const float2 v = a.y[0][p.i];
+    float2 y[1] = {make_float2(v.x + sig * g.x, v.y + sig * g.y)};
+    prox_div<1>(y, sqrtf(cabs2(y[0])), a.r1);
+    a.y[0][p.i] = y[0];
+  } else if (M == AVX_M_ICTV) {
+    // y1 += sigma grad_w1 (xbar1 - xbar3), y3 += sigma grad_w2 xbar3, each
+    // projected onto its ball (ictv.cpp:255-285)
+    float2 g[3], y1[3];
+    grad3_diff(a.xb[0], a.xb[1], p, a.w1, g);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float2 v = a.y[k][p.i];
+      y1[k] = make_float2(v.x + sig * g[k].x, v.y + sig * g[k].y);
+    }
+    prox_div<3>(y1, nrm3(y1), a.r1);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) a.y[k][p.i] = y1[k];
+    grad3(a.xb[1], p, a.w2, g);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float2 v = a.y[3 + k][p.i];
+      y1[k] = make_float2(v.x + sig * g[k].x, v.y + sig * g[k].y);
+    }
+    prox_div<3>(y1, nrm3(y1), a.r3);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) a.y[3 + k][p.i] = y1[k];
   } else {
     // branch 1: y1 += sigma (grad u - v), y2 += sigma E v
     // TGV2: u = xbar1, v = xbar2.  ICTGV2: u = xbar1 - xbar3, v = xbar2.
+    // Every load of a branch is issued before its first store: the dual
+    // pointers may alias as far as the compiler knows, so a store would keep
+    // the loads after it from being moved up.
     {
       float2 g[3], y1[3], e[6], y2[6];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) y1[k] = a.y[k][p.i];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) y2[k] = a.y[3 + k][p.i];
       if (M == AVX_M_TGV2)
         grad3(a.xb[0], p, a.w1, g);
       else
         grad3_diff(a.xb[0], a.xb[4], p, a.w1, g);
+      symgrad(a.xb[1], a.xb[2], a.xb[3], p, a.w1, e);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        float2 v = a.y[k][p.i];
-        float2 q = ldc(a.xb[1 + k], p.i);
-        float2 d = csub(g[k], q);
-        y1[k] = make_float2(v.x + sig * d.x, v.y + sig * d.y);
+        const float2 d = csub(g[k], ldc(a.xb[1 + k], p.i));
+        y1[k] = make_float2(y1[k].x + sig * d.x, y1[k].y + sig * d.y);
       }
       prox_div<3>(y1, nrm3(y1), a.r1);
 #pragma unroll
-      for (int k = 0; k < 3; ++k) a.y[k][p.i] = y1[k];
-      symgrad(a.xb[1], a.xb[2], a.xb[3], p, a.w1, e);
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        float2 v = a.y[3 + k][p.i];
-        y2[k] = make_float2(v.x + sig * e[k].x, v.y + sig * e[k].y);
-      }
+      for (int k = 0; k < 6; ++k) y2[k] = make_float2(y2[k].x + sig * e[k].x, y2[k].y + sig * e[k].y);
       prox_div<6>(y2, nrm6(y2), a.r2);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) a.y[k][p.i] = y1[k];
 #pragma unroll
       for (int k = 0; k < 6; ++k) a.y[3 + k][p.i] = y2[k];
     }
     if (M == AVX_M_ICTGV2) {
       // branch 2: y3 += sigma (grad2 xbar3 - xbar4), y4 += sigma E2 xbar4
       float2 g[3], y3[3], e[6], y4[6];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) y3[k] = a.y[9 + k][p.i];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) y4[k] = a.y[12 + k][p.i];
       grad3(a.xb[4], p, a.w2, g);
+      symgrad(a.xb[5], a.xb[6], a.xb[7], p, a.w2, e);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        float2 v = a.y[9 + k][p.i];
-        float2 d = csub(g[k], ldc(a.xb[5 + k], p.i));
-        y3[k] = make_float2(v.x + sig * d.x, v.y + sig * d.y);
+        const float2 d = csub(g[k], ldc(a.xb[5 + k], p.i));
+        y3[k] = make_float2(y3[k].x + sig * d.x, y3[k].y + sig * d.y);
       }
       prox_div<3>(y3, nrm3(y3), a.r3);
 #pragma unroll
-      for (int k = 0; k < 3; ++k) a.y[9 + k][p.i] = y3[k];
-      symgrad(a.xb[5], a.xb[6], a.xb[7], p, a.w2, e);
-#pragma unroll
-      for (int k = 0; k < 6; ++k) {
-        float2 v = a.y[12 + k][p.i];
-        y4[k] = make_float2(v.x + sig * e[k].x, v.y + sig * e[k].y);
-      }
+      for (int k = 0; k < 6; ++k) y4[k] = make_float2(y4[k].x + sig * e[k].x, y4[k].y + sig * e[k].y);
       prox_div<6>(y4, nrm6(y4), a.r4);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) a.y[9 + k][p.i] = y3[k];
 #pragma unroll
       for (int k = 0; k < 6; ++k) a.y[12 + k][p.i] = y4[k];
     }
@@ -200,7 +231,7 @@ size_t ydft_smem_bytes(int H) { return sizeof(float2) * (size_t)H * (YD_XS + KSP
 // Each CTA reads and rewrites only its own block of k.qp.
 // ---------------------------------------------------------------------------
 
-template <int KC>
+template <int KC, bool LARGE>
 __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
   if (a.st && a.st->stop && mode != 3) return;
   constexpr int KCP = KC + 2;
@@ -219,6 +250,8 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
   double* red = reinterpret_cast<double*>(twx + W);  // [32*3]
 
   const int tid = threadIdx.x, nt = blockDim.x;
+  __shared__ int splan[12];
+  stage_plan(g.rad, splan);
   for (int j = tid; j < W; j += nt) twx[j] = g.twx[j];
   const unsigned mW = div_magic((unsigned)W);  // e < KC W < 2^16
 
@@ -231,19 +264,33 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
     __syncthreads();
     // with the FFT, sequence position n holds x = n + sx (the ifftshift of the
     // centred transform); the dense DFT indexes x directly
-    for (int e = tid; e < KC * W; e += nt) {
-      const int kk = fast_div(e, (unsigned)W, mW), x = e - kk * W;
-      int xs = x;
-      if (g.nrad) {
-        xs = x - g.sx;
-        if (xs < 0) xs += W;
+    // ROWS_RB loads per thread are issued before any is stored, so that their
+    // latencies overlap
+    for (int e0 = tid; e0 < KC * W; e0 += ROWS_RB * nt) {
+      float2 v[ROWS_RB];
+#pragma unroll
+      for (int b = 0; b < ROWS_RB; ++b) {
+        const int e = e0 + b * nt;
+        const int kk = fast_div(e, (unsigned)W, mW), x = e - kk * W;
+        v[b] = (e < KC * W && kk < kc) ? a.qp[zb + (long long)(k0 + kk) * W + x] : czero();
       }
-      P[xs * KCP + kk] = kk < kc ? a.qp[zb + (long long)(k0 + kk) * W + x] : czero();
+#pragma unroll
+      for (int b = 0; b < ROWS_RB; ++b) {
+        const int e = e0 + b * nt;
+        if (e >= KC * W) break;
+        const int kk = fast_div(e, (unsigned)W, mW), x = e - kk * W;
+        int xs = x;
+        if (g.nrad) {
+          xs = x - g.sx;
+          if (xs < 0) xs += W;
+        }
+        P[xs * KCP + kk] = v[b];
+      }
     }
     __syncthreads();
     float2* Xb = X;  // buffer holding the row transform, index (kx - sx) mod W with the FFT
     if (g.nrad) {
-      Xb = row_fft<KC>(P, X, twx, W, g.nrad, g.rad, +1);
+      Xb = row_fft<KC, LARGE>(P, X, twx, W, g.nrad, splan, +1);
     } else {
       // dense DFT along x: thread per kx
       for (int kx = tid; kx < W; kx += nt) {
@@ -271,48 +318,72 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
       }
       __syncthreads();
     }
-    // pointwise stage on the kept samples; Xb[n] holds kx = n + sx (FFT) or kx
-    for (int e = tid; e < kc * W; e += nt) {
-      const int kk = fast_div(e, (unsigned)W, mW), kx = e - kk * W;
-      int n = kx;
-      if (g.nrad) {
-        n = kx - g.sx;
-        if (n < 0) n += W;
+    // pointwise stage on the kept samples; Xb[n] holds kx = n + sx (FFT) or kx.
+    // The mask, z and d values of ROWS_RB samples are loaded first.
+    const bool need_zd = mode == 0 || mode == 2;
+    for (int e0 = tid; e0 < kc * W; e0 += ROWS_RB * nt) {
+      float mb[ROWS_RB];
+      float2 zpre[ROWS_RB], dpre[ROWS_RB];
+#pragma unroll
+      for (int b = 0; b < ROWS_RB; ++b) {
+        const int e = e0 + b * nt;
+        mb[b] = 0.f;
+        zpre[b] = dpre[b] = czero();
+        if (e < kc * W) {
+          const int kk = fast_div(e, (unsigned)W, mW), kx = e - kk * W;
+          const long long gi = zb + (long long)(k0 + kk) * W + kx;
+          mb[b] = g.mrow[(long long)(r0 + k0 + kk) * W + kx];
+          if (need_zd) {
+            zpre[b] = a.z[gi];
+            dpre[b] = a.d[gi];
+          }
+        }
       }
-      const long long gi = zb + (long long)(k0 + kk) * W + kx;
-      const float m = g.mrow[(long long)(r0 + k0 + kk) * W + kx];
-      const float2 Xv = cscale(Xb[n * KCP + kk], g.inv_sqrt_w);
-      const float2 mX = cscale(Xv, m);
-      if (mode == 0) {
-        const float2 zo = a.z[gi], dv = a.d[gi];
-        // z += sigma * (mask X); z = (z - sigma d) * 1/(1 + sigma/lambda); z *= mask
-        float2 zn = make_float2(zo.x + sig * mX.x, zo.y + sig * mX.y);
-        zn = make_float2(zn.x - sig * dv.x, zn.y - sig * dv.y);
-        zn = cscale(zn, zscale);
-        zn = cscale(zn, m);
-        a.z[gi] = zn;
-        Xb[n * KCP + kk] = zn;
-      } else if (mode == 1) {
-        acc_r[0] += (double)cabs2(mX);
-      } else if (mode == 2) {
-        const float2 zo = a.z[gi], dv = a.d[gi];
-        const float2 r = csub(mX, dv);
-        acc_r[0] += (double)cabs2(r);
-        acc_r[1] += (double)dv.x * zo.x + (double)dv.y * zo.y;
-        acc_r[2] += (double)cabs2(zo);
-        const float2 zm = cscale(zo, m);
-        if (!a.binary_mask) a.z[gi] = zm;
-        Xb[n * KCP + kk] = zm;
-      } else {
-        const int ky = g.rows[r0 + k0 + kk];
-        a.dense_out[(((long long)t * C + c) * g.H + ky) * W + kx] = mX;
+#pragma unroll
+      for (int b = 0; b < ROWS_RB; ++b) {
+        const int e = e0 + b * nt;
+        if (e >= kc * W) break;
+        const int kk = fast_div(e, (unsigned)W, mW), kx = e - kk * W;
+        int n = kx;
+        if (g.nrad) {
+          n = kx - g.sx;
+          if (n < 0) n += W;
+        }
+        const long long gi = zb + (long long)(k0 + kk) * W + kx;
+        const float m = mb[b];
+        const float2 Xv = cscale(Xb[n * KCP + kk], g.inv_sqrt_w);
+        const float2 mX = cscale(Xv, m);
+        if (mode == 0) {
+          const float2 zo = zpre[b], dv = dpre[b];
+          // z += sigma * (mask X); z = (z - sigma d) * 1/(1 + sigma/lambda); z *= mask
+          float2 zn = make_float2(zo.x + sig * mX.x, zo.y + sig * mX.y);
+          zn = make_float2(zn.x - sig * dv.x, zn.y - sig * dv.y);
+          zn = cscale(zn, zscale);
+          zn = cscale(zn, m);
+          a.z[gi] = zn;
+          Xb[n * KCP + kk] = zn;
+        } else if (mode == 1) {
+          acc_r[0] += (double)cabs2(mX);
+        } else if (mode == 2) {
+          const float2 zo = zpre[b], dv = dpre[b];
+          const float2 r = csub(mX, dv);
+          acc_r[0] += (double)cabs2(r);
+          acc_r[1] += (double)dv.x * zo.x + (double)dv.y * zo.y;
+          acc_r[2] += (double)cabs2(zo);
+          const float2 zm = cscale(zo, m);
+          if (!a.binary_mask) a.z[gi] = zm;
+          Xb[n * KCP + kk] = zm;
+        } else {
+          const int ky = g.rows[r0 + k0 + kk];
+          a.dense_out[(((long long)t * C + c) * g.H + ky) * W + kx] = mX;
+        }
       }
     }
     if (mode == 1 || mode == 3) continue;
     __syncthreads();
     if (g.nrad) {
       // inverse row FFT; Xb position n holds kx = n + sx, the result position n holds x = n + sx
-      float2* Qb = row_fft<KC>(Xb, Xb == X ? P : X, twx, W, g.nrad, g.rad, -1);
+      float2* Qb = row_fft<KC, LARGE>(Xb, Xb == X ? P : X, twx, W, g.nrad, splan, -1);
       for (int e = tid; e < kc * W; e += nt) {
         const int kk = fast_div(e, (unsigned)W, mW), x = e - kk * W;
         int n = x - g.sx;
@@ -472,10 +543,11 @@ __global__ void __launch_bounds__(PR_TX* PR_TY) primal_kernel(PDArgs a) {
     if (y >= a.H) continue;
     const PixCoord p = make_pix(x, y, t, a.W, a.H, a.T);
     // every load of the pixel first (the stores below would otherwise order them)
-    const float2 dv1 = div3(a.y[0], a.y[1], a.y[2], p, a.w1);
+    const float2 dv1 = M == AVX_M_TVTEMP ? tdiv(a.y[0], p, a.w1) : div3(a.y[0], a.y[1], a.y[2], p, a.w1);
     float2 sd1[3], y1[3], sd2[3], y3[3], xo[8];
     float2 dv3 = czero();
-    if (M != AVX_M_TV) {
+    if (M == AVX_M_ICTV) dv3 = div3(a.y[3], a.y[4], a.y[5], p, a.w2);
+    if (M == AVX_M_TGV2 || M == AVX_M_ICTGV2) {
       symdiv(a.y + 3, p, a.w1, sd1);
 #pragma unroll
       for (int c = 0; c < 3; ++c) y1[c] = ldc(a.y[c], p.i);
@@ -486,13 +558,14 @@ __global__ void __launch_bounds__(PR_TX* PR_TY) primal_kernel(PDArgs a) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) y3[c] = ldc(a.y[9 + c], p.i);
     }
-    constexpr int P = M == AVX_M_TV ? 1 : (M == AVX_M_TGV2 ? 4 : 8);
+    constexpr int P = MethodDims<M>::P;
 #pragma unroll
     for (int c = 0; c < P; ++c) xo[c] = a.x[c][p.i];
     // updates: x' = x + tau r, xbar = 2 x' - x
     float2 r[8];
     r[0] = csub(dv1, kh[j]);                       // x1 <- x1 - tau (K^H z - div y1)
-    if (M != AVX_M_TV)
+    if (M == AVX_M_ICTV) r[1] = csub(dv3, dv1);    // x3 <- x3 - tau (div1 y1 - div2 y3) (ictv.cpp:300-318)
+    if (M == AVX_M_TGV2 || M == AVX_M_ICTGV2)
 #pragma unroll
       for (int c = 0; c < 3; ++c) r[1 + c] = cadd(y1[c], sd1[c]);  // x2 <- x2 + tau (y1 + symdiv y2)
     if (M == AVX_M_ICTGV2) {
@@ -531,6 +604,14 @@ __global__ void __launch_bounds__(256) step_img_kernel(PDArgs a, Ptr8 e, double*
       grad3(e.p[0], p, a.w1, g);
       acc[0] += (double)ss3(g);
       acc[1] += (double)cabs2(ldc(e.p[0], p.i));
+    } else if (M == AVX_M_TVTEMP) {
+      // TVTEMP::AdaptStepSize (tv_temp.cpp:80-95): temporal gradient only
+      acc[0] += (double)cabs2(tgrad(e.p[0], p, a.w1));
+      acc[1] += (double)cabs2(ldc(e.p[0], p.i));
+    } else if (M == AVX_M_ICTV) {
+      // ICTV::AdaptStepSize (ictv.cpp:97-128) forms the gradient sums in a
+      // buffer that the next statement overwrites: |K e1| and |e1|, |e3| remain
+      acc[1] += (double)(cabs2(ldc(e.p[0], p.i)) + cabs2(ldc(e.p[1], p.i)));
     } else {
       float2 g[3], s[6];
       if (M == AVX_M_TGV2)
@@ -637,12 +718,23 @@ __global__ void __launch_bounds__(ADJ_TX* ADJ_TY) gap_img_kernel(PDArgs a, doubl
       const int y = y0 + threadIdx.y * ADJ_YP + j;
       if (y >= a.H) continue;
       const PixCoord p = make_pix(x, y, t, a.W, a.H, a.T);
-      const float2 dv1 = div3(a.y[0], a.y[1], a.y[2], p, a.w1);
+      const float2 dv1 = M == AVX_M_TVTEMP ? tdiv(a.y[0], p, a.w1) : div3(a.y[0], a.y[1], a.y[2], p, a.w1);
       acc[0] += (double)sqrtf(cabs2(csub(kh[j], dv1)));
       float2 g[3];
-      if (M == AVX_M_TV) {
+      if (M == AVX_M_TV || M == AVX_M_TVTEMP) {
+        // TVTEMP::ComputePDGap adds the full TVNorm (tv_temp.cpp:214-222)
         grad3(a.x[0], p, a.w1, g);
         acc[4] += (double)nrm3(g);
+        continue;
+      }
+      if (M == AVX_M_ICTV) {
+        // ICTV::ComputeGStar g5 and ICTVNorm's two TV norms (ictv.cpp:148-190, utils.cpp:1221-1242)
+        const float2 dv3 = div3(a.y[3], a.y[4], a.y[5], p, a.w2);
+        acc[2] += (double)sqrtf(cabs2(csub(dv1, dv3)));
+        grad3_diff(a.x[0], a.x[1], p, a.w1, g);
+        acc[4] += (double)nrm3(g);
+        grad3(a.x[1], p, a.w2, g);
+        acc[6] += (double)nrm3(g);
         continue;
       }
       float2 sd[3], e[6];
@@ -708,8 +800,10 @@ __global__ void gap_finalize_kernel(DevState* st, const double* pk, int nk, cons
   const double g2 = v[1] + v[2] / (2.0 * lam);
   const double g36 = v[3] + v[4] + v[5] + v[6];
   double reg;
-  if (M == AVX_M_TV)
+  if (M == AVX_M_TV || M == AVX_M_TVTEMP)
     reg = v[7];
+  else if (M == AVX_M_ICTV)
+    reg = gc.alpha1 * gc.ic_a * v[7] + gc.alpha1 * gc.ic_b * v[9];
   else if (M == AVX_M_TGV2)
     reg = gc.alpha1 * v[7] + gc.alpha0 * v[8];
   else
@@ -727,10 +821,12 @@ __global__ void gap_finalize_kernel(DevState* st, const double* pk, int nk, cons
   const bool stop = gap < gc.stop_gap || (gc.stop_rel > 0.0 && gap <= gc.stop_rel * st->gap0);
   // TGV2 returns before recording the gap that stops it (tgv2.cpp:325-328)
   const bool record = !(M == AVX_M_TGV2 && stop);
+  // ICTGV2's norm and fidelity histories start with the pre-loop record
+  const int off = M == AVX_M_ICTGV2 ? 1 : 0;
   if (record && st->ngap < cap) {
     hist_gap[st->ngap] = gap;
-    if (hist_norm) hist_norm[st->ngap + 1] = reg;
-    if (hist_fid) hist_fid[st->ngap + 1] = fid;
+    if (hist_norm) hist_norm[st->ngap + off] = reg;
+    if (hist_fid) hist_fid[st->ngap + off] = fid;
     st->ngap += 1;
   }
   if (stop) st->stop = 1;
@@ -800,7 +896,9 @@ static void rec(cudaEvent_t* ev, int i, cudaStream_t s) {
 void launch_dual(int method, const PDArgs& a, cudaStream_t s) {
   dim3 gd((a.W * a.H + 255) / 256, a.T);
   if (method == AVX_M_TV) dual_kernel<AVX_M_TV><<<gd, 256, 0, s>>>(a);
+  else if (method == AVX_M_TVTEMP) dual_kernel<AVX_M_TVTEMP><<<gd, 256, 0, s>>>(a);
   else if (method == AVX_M_TGV2) dual_kernel<AVX_M_TGV2><<<gd, 256, 0, s>>>(a);
+  else if (method == AVX_M_ICTV) dual_kernel<AVX_M_ICTV><<<gd, 256, 0, s>>>(a);
   else dual_kernel<AVX_M_ICTGV2><<<gd, 256, 0, s>>>(a);
 }
 
@@ -808,7 +906,9 @@ void launch_primal(int method, const PDArgs& a, cudaStream_t s) {
   dim3 gp((a.W + PR_TX - 1) / PR_TX, (a.H + PR_TH - 1) / PR_TH, a.T);
   dim3 bl(PR_TX, PR_TY);
   if (method == AVX_M_TV) primal_kernel<AVX_M_TV><<<gp, bl, 0, s>>>(a);
+  else if (method == AVX_M_TVTEMP) primal_kernel<AVX_M_TVTEMP><<<gp, bl, 0, s>>>(a);
   else if (method == AVX_M_TGV2) primal_kernel<AVX_M_TGV2><<<gp, bl, 0, s>>>(a);
+  else if (method == AVX_M_ICTV) primal_kernel<AVX_M_ICTV><<<gp, bl, 0, s>>>(a);
   else primal_kernel<AVX_M_ICTGV2><<<gp, bl, 0, s>>>(a);
 }
 
@@ -822,7 +922,12 @@ void launch_ydft(const KArgs& k, cudaStream_t s) {
 }
 
 void launch_rows(const KArgs& k, int mode, cudaStream_t s) {
-  rows_kernel<KSPACE_KC><<<k.g.C * k.g.T, 256, rows_smem_bytes(k.g.W), s>>>(k, mode);
+  bool large = false;
+  for (int i = 0; i < k.g.nrad; ++i) large = large || k.g.rad[i] > 5;
+  if (large)
+    rows_kernel<KSPACE_KC, true><<<k.g.C * k.g.T, 256, rows_smem_bytes(k.g.W), s>>>(k, mode);
+  else
+    rows_kernel<KSPACE_KC, false><<<k.g.C * k.g.T, 256, rows_smem_bytes(k.g.W), s>>>(k, mode);
 }
 
 void launch_kspace(const KArgs& k, int mode, cudaStream_t s) {
@@ -860,7 +965,9 @@ int gap_img_blocks(int W, int H, int T) {
 void launch_step_img(int method, const PDArgs& a, const Ptr8& e_dev, int P, double* pimg, cudaStream_t s) {
   diff_kernel<<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, P);
   if (method == AVX_M_TV) step_img_kernel<AVX_M_TV><<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, pimg);
+  else if (method == AVX_M_TVTEMP) step_img_kernel<AVX_M_TVTEMP><<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, pimg);
   else if (method == AVX_M_TGV2) step_img_kernel<AVX_M_TGV2><<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, pimg);
+  else if (method == AVX_M_ICTV) step_img_kernel<AVX_M_ICTV><<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, pimg);
   else step_img_kernel<AVX_M_ICTGV2><<<AVX_RED_BLOCKS, 256, 0, s>>>(a, e_dev, pimg);
 }
 
@@ -887,8 +994,12 @@ void launch_gap_tail(int method, const PDArgs& a, const KArgs& k_x, double* pimg
   gap_finalize_kernel<MM><<<1, 256, 0, s>>>(a.st, pk, nk, pimg, nimg, gc, hg, hn, hf, cap, init_only);
   if (method == AVX_M_TV) {
     GAP_IMG(AVX_M_TV)
+  } else if (method == AVX_M_TVTEMP) {
+    GAP_IMG(AVX_M_TVTEMP)
   } else if (method == AVX_M_TGV2) {
     GAP_IMG(AVX_M_TGV2)
+  } else if (method == AVX_M_ICTV) {
+    GAP_IMG(AVX_M_ICTV)
   } else {
     GAP_IMG(AVX_M_ICTGV2)
   }
@@ -914,9 +1025,11 @@ void launch_dense_rowidft(const CartGeomDev& g, float2* dense, float2* qp, const
 
 cudaError_t configure_kernels() {
   // opt in to the full 227 KB of dynamic shared memory per CTA (sm_100)
-  cudaError_t e = cudaFuncSetAttribute(ydft_kernel<KSPACE_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(ydft_kernel<KSPACE_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(rows_kernel<KSPACE_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  e = cudaFuncSetAttribute(rows_kernel<KSPACE_KC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(rows_kernel<KSPACE_KC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
 }
 
 }  // namespace avx

@@ -4,6 +4,9 @@
 #include "pd_args.cuh"
 
 #define KSPACE_KC 16  // compact k-space rows per chunk (y-transform and row kernels)
+#ifndef ROWS_RB
+#define ROWS_RB 4     // global loads a thread of the row kernel issues together
+#endif
 #define YD_XS 16      // image columns per CTA of the y-transform
 #define YD_CG 16      // coil slots per CTA of the y-transform
 #define CA_TX 16      // column-adjoint threads along x (two columns each, 16 apart)

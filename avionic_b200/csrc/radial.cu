@@ -6,6 +6,8 @@
 // The spreading step gathers: one CTA per (frame, sector) owns the sector's
 // grid cells and reads every sample of the 3x3 neighbouring sectors, so each
 // grid value is a fixed-order sum (no floating-point atomics, deterministic).
+#include <algorithm>
+
 #include "fft.cuh"
 #include "radial.cuh"
 
@@ -13,7 +15,6 @@ namespace avx {
 
 #define RAD_FFT_KC 16
 #define RAD_SPREAD_BATCH 64
-#define RAD_SPREAD_CC 8  // coils accumulated per pass of the spreading kernel
 
 // tapered Kaiser-Bessel weight at offset u (grid units); zero for |u| >= J/2
 AVX_D float kbw(float u, const RadialGeomDev& g) {
@@ -66,13 +67,15 @@ __global__ void __launch_bounds__(256) rad_fft_rows_kernel(RArgs a, int sign) {
   const int r0 = blockIdx.x * KC;
   const int rows = min(KC, g.Gy - r0);
   float2* base = a.grid + (long long)slice * g.Gx * g.Gy;
+  __shared__ int splan[12];
+  stage_plan(g.radx, splan);
   for (int j = threadIdx.x; j < G; j += blockDim.x) tw[j] = g.twgx[j];
   for (int e = threadIdx.x; e < KC * G; e += blockDim.x) {
     const int kk = e / G, x = e % G;
     A[x * KCP + kk] = kk < rows ? base[(long long)(r0 + kk) * G + x] : czero();
   }
   __syncthreads();
-  const float2* R = row_fft<KC>(A, B, tw, G, g.nradx, g.radx, sign);
+  const float2* R = row_fft<KC>(A, B, tw, G, g.nradx, splan, sign);
   for (int e = threadIdx.x; e < rows * G; e += blockDim.x) {
     const int kk = e / G, x = e % G;
     base[(long long)(r0 + kk) * G + x] = R[x * KCP + kk];
@@ -92,13 +95,15 @@ __global__ void __launch_bounds__(256) rad_fft_cols_kernel(RArgs a, int sign) {
   const int c0 = blockIdx.x * KC;
   const int cols = min(KC, g.Gx - c0);
   float2* base = a.grid + (long long)slice * g.Gx * g.Gy;
+  __shared__ int splan[12];
+  stage_plan(g.rady, splan);
   for (int j = threadIdx.x; j < G; j += blockDim.x) tw[j] = g.twgy[j];
   for (int e = threadIdx.x; e < KC * G; e += blockDim.x) {
     const int kk = e % KC, y = e / KC;
     A[y * KCP + kk] = kk < cols ? base[(long long)y * g.Gx + c0 + kk] : czero();
   }
   __syncthreads();
-  const float2* R = row_fft<KC>(A, B, tw, G, g.nrady, g.rady, sign);
+  const float2* R = row_fft<KC>(A, B, tw, G, g.nrady, splan, sign);
   for (int e = threadIdx.x; e < KC * G; e += blockDim.x) {
     const int kk = e % KC, y = e / KC;
     if (kk < cols) base[(long long)y * g.Gx + c0 + kk] = R[y * KCP + kk];
@@ -115,6 +120,23 @@ AVX_D int sample_window(float kappa, const RadialGeomDev& g, float (&w)[NW]) {
 }
 
 template <int NW>
+__global__ void rad_window_kernel(RadialGeomDev g, int2* win0, float* winw) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)g.T * g.S;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)(i / g.S), s = (int)(i % g.S);
+    float wx[NW], wy[NW];
+    const int g0x = sample_window<NW>(g.traj[((long long)f * 2 + 0) * g.S + s] * (float)g.Gx, g, wx);
+    const int g0y = sample_window<NW>(g.traj[((long long)f * 2 + 1) * g.S + s] * (float)g.Gy, g, wy);
+    win0[i] = make_int2(g0x, g0y);
+#pragma unroll
+    for (int o = 0; o < NW; ++o) {
+      winw[i * 2 * NW + o] = wx[o];
+      winw[i * 2 * NW + NW + o] = wy[o];
+    }
+  }
+}
+
+template <int NW>
 __global__ void __launch_bounds__(256) rad_interp_kernel(RArgs a, int mode) {
   if (a.st && a.st->stop && mode != 3) return;
   __shared__ double red[32 * 3];
@@ -123,11 +145,14 @@ __global__ void __launch_bounds__(256) rad_interp_kernel(RArgs a, int mode) {
   double acc_r[3] = {0.0, 0.0, 0.0};
   if (i < (long long)g.T * g.S) {
     const int f = (int)(i / g.S), s = (int)(i % g.S);
-    const float kx = g.traj[((long long)f * 2 + 0) * g.S + s];
-    const float ky = g.traj[((long long)f * 2 + 1) * g.S + s];
+    const int2 g0 = g.win0[i];
+    const int g0x = g0.x, g0y = g0.y;
     float wx[NW], wy[NW];
-    const int g0x = sample_window<NW>(kx * (float)g.Gx, g, wx);
-    const int g0y = sample_window<NW>(ky * (float)g.Gy, g, wy);
+#pragma unroll
+    for (int o = 0; o < NW; ++o) {
+      wx[o] = g.winw[i * 2 * NW + o];
+      wy[o] = g.winw[i * 2 * NW + NW + o];
+    }
     int ix[NW], iy[NW];
 #pragma unroll
     for (int o = 0; o < NW; ++o) {
@@ -183,14 +208,15 @@ __global__ void __launch_bounds__(256) rad_interp_kernel(RArgs a, int mode) {
   }
 }
 
-// one CTA per (sector, frame); thread = grid cell of the sector
-template <int NW>
+// one CTA per (sector, frame); thread = grid cell of the sector; CC coils
+// accumulated per pass over the neighbouring sectors' samples
+template <int NW, int CC>
 __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
   if (a.st && a.st->stop) return;
   const RadialGeomDev& g = a.g;
   __shared__ int s_g0x[RAD_SPREAD_BATCH], s_g0y[RAD_SPREAD_BATCH];
   __shared__ float s_wx[RAD_SPREAD_BATCH][NW], s_wy[RAD_SPREAD_BATCH][NW];
-  __shared__ float2 s_v[RAD_SPREAD_BATCH][RAD_SPREAD_CC];
+  __shared__ float2 s_v[RAD_SPREAD_BATCH][CC];
   const int f = blockIdx.y;
   const int sec = blockIdx.x;
   const int sxi = sec % g.nsx, syi = sec / g.nsx;
@@ -202,11 +228,11 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
   const int* start = g.sec_start + (long long)f * (nsec + 1);
   // distinct neighbouring sector offsets (fewer than three sectors along an axis wrap onto themselves)
   const int dxn = g.nsx >= 3 ? 3 : g.nsx, dyn = g.nsy >= 3 ? 3 : g.nsy;
-  for (int c0 = 0; c0 < g.C; c0 += RAD_SPREAD_CC) {
-    const int cc = min(RAD_SPREAD_CC, g.C - c0);
-    float2 acc[RAD_SPREAD_CC];
+  for (int c0 = 0; c0 < g.C; c0 += CC) {
+    const int cc = min(CC, g.C - c0);
+    float2 acc[CC];
 #pragma unroll
-    for (int k = 0; k < RAD_SPREAD_CC; ++k) acc[k] = czero();
+    for (int k = 0; k < CC; ++k) acc[k] = czero();
     for (int dy = 0; dy < dyn; ++dy) {
       for (int dx = 0; dx < dxn; ++dx) {
         const int nsxi = imod(sxi + (dxn == 3 ? dx - 1 : dx), g.nsx);
@@ -218,18 +244,18 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
           __syncthreads();
           for (int e = threadIdx.x; e < nb; e += blockDim.x) {
             const int j = order[b0 + e];
-            const float kx = g.traj[((long long)f * 2 + 0) * g.S + j];
-            const float ky = g.traj[((long long)f * 2 + 1) * g.S + j];
-            float wx[NW], wy[NW];
-            s_g0x[e] = sample_window<NW>(kx * (float)g.Gx, g, wx);
-            s_g0y[e] = sample_window<NW>(ky * (float)g.Gy, g, wy);
+            const long long fj = (long long)f * g.S + j;
+            const int2 g0 = g.win0[fj];
+            s_g0x[e] = g0.x;
+            s_g0y[e] = g0.y;
 #pragma unroll
             for (int o = 0; o < NW; ++o) {
-              s_wx[e][o] = wx[o];
-              s_wy[e][o] = wy[o];
+              s_wx[e][o] = g.winw[fj * 2 * NW + o];
+              s_wy[e][o] = g.winw[fj * 2 * NW + NW + o];
             }
-            const float sc = g.sqrt_w[(long long)f * g.S + j] * g.norm;
-            for (int k = 0; k < RAD_SPREAD_CC; ++k)
+            const float sc = g.sqrt_w[fj] * g.norm;
+#pragma unroll
+            for (int k = 0; k < CC; ++k)
               s_v[e][k] = k < cc ? cscale(samples[((long long)f * g.C + c0 + k) * g.S + j], sc) : czero();
           }
           __syncthreads();
@@ -239,7 +265,7 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
               if (ox < NW && oy < NW) {
                 const float w = s_wx[e][ox] * s_wy[e][oy];
 #pragma unroll
-                for (int k = 0; k < RAD_SPREAD_CC; ++k) {
+                for (int k = 0; k < CC; ++k) {
                   acc[k].x = fmaf(w, s_v[e][k].x, acc[k].x);
                   acc[k].y = fmaf(w, s_v[e][k].y, acc[k].y);
                 }
@@ -249,9 +275,11 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
         }
       }
     }
-    if (active)
-      for (int k = 0; k < cc; ++k)
-        a.grid[(((long long)f * g.C + c0 + k) * g.Gy + gy) * g.Gx + gx] = acc[k];
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < CC; ++k)
+        if (k < cc) a.grid[(((long long)f * g.C + c0 + k) * g.Gy + gy) * g.Gx + gx] = acc[k];
+    }
   }
 }
 
@@ -278,9 +306,9 @@ size_t radial_fft_smem_bytes(int G) { return sizeof(float2) * (2 * (size_t)G * (
 int radial_interp_blocks(const RadialGeomDev& g) { return (int)(((long long)g.T * g.S + 255) / 256); }
 
 cudaError_t configure_radial_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(rad_fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(rad_fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(rad_fft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  return cudaFuncSetAttribute(rad_fft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
 }
 
 void launch_rad_pad(const RArgs& a, cudaStream_t s) {
@@ -313,12 +341,30 @@ void launch_rad_interp(const RArgs& a, int mode, cudaStream_t s) {
 #undef CALL_I
 }
 
+void launch_rad_windows(const RadialGeomDev& g, int2* win0, float* winw, cudaStream_t s) {
+  const int nb = (int)std::min<long long>(((long long)g.T * g.S + 255) / 256, 148 * 16);
+#define CALL_W(N) rad_window_kernel<N><<<nb, 256, 0, s>>>(g, win0, winw)
+  RAD_NW_DISPATCH(g.nw, CALL_W)
+#undef CALL_W
+}
+
 void launch_rad_spread(const RArgs& a, const float2* samples, cudaStream_t s) {
   dim3 grid(a.g.nsx * a.g.nsy, a.g.T);
   const int threads = a.g.sw * a.g.sw;
-#define CALL_S(N) rad_spread_kernel<N><<<grid, threads, 0, s>>>(a, samples)
-  RAD_NW_DISPATCH(a.g.nw, CALL_S)
+  // coils per pass: every pass re-reads the neighbouring sectors' samples
+  if (a.g.C <= 4) {
+#define CALL_S(N) rad_spread_kernel<N, 4><<<grid, threads, 0, s>>>(a, samples)
+    RAD_NW_DISPATCH(a.g.nw, CALL_S)
 #undef CALL_S
+  } else if (a.g.C <= 8) {
+#define CALL_S(N) rad_spread_kernel<N, 8><<<grid, threads, 0, s>>>(a, samples)
+    RAD_NW_DISPATCH(a.g.nw, CALL_S)
+#undef CALL_S
+  } else {
+#define CALL_S(N) rad_spread_kernel<N, 16><<<grid, threads, 0, s>>>(a, samples)
+    RAD_NW_DISPATCH(a.g.nw, CALL_S)
+#undef CALL_S
+  }
 }
 
 void launch_rad_crop(const RArgs& a, float2* img, cudaStream_t s) {

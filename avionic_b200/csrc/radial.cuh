@@ -21,6 +21,8 @@ struct RadialGeomDev {
   const float* inv_psi_y;   // [H]
   const int* order;         // [T][S] sample indices sorted by sector (stable)
   const int* sec_start;     // [T][nsx*nsy + 1] offsets into order
+  const int2* win0;         // [T][S] first grid cell (x, y) of each sample's window, unwrapped
+  const float* winw;        // [T][S][2 nw] the window's weights, x then y
   const float2* twgx;       // [Gx] exp(+2 pi i j / Gx)
   const float2* twgy;       // [Gy]
   int nradx, radx[12];      // FFT plan along x
@@ -47,6 +49,8 @@ size_t radial_fft_smem_bytes(int G);
 int radial_interp_blocks(const RadialGeomDev& g);
 cudaError_t configure_radial_kernels();
 
+// per-sample window starts and weights (g.win0, g.winw), once per operator
+void launch_rad_windows(const RadialGeomDev& g, int2* win0, float* winw, cudaStream_t s);
 // image -> grid: zero-padded, deapodised b1 * (in - in2)
 void launch_rad_pad(const RArgs& a, cudaStream_t s);
 // in-place unnormalised 2D DFT of every grid slice, sign -1 forward, +1 inverse

@@ -86,6 +86,17 @@ AVX_D float2 div3(const float2* y0, const float2* y1, const float2* y2, const Pi
   return make_float2(-a.x, -a.y);
 }
 
+// utils::Gradient_temp (utils.cpp:134-143): the temporal component alone
+AVX_D float2 tgrad(const float2* u, const PixCoord& p, const Wts& w) {
+  return cscale(d_fwd(u, p.i, p.t, p.T, p.sWH), w.it);
+}
+
+// utils::Divergence_temp (utils.cpp:795-805) = -(D+_t)^T y / dt
+AVX_D float2 tdiv(const float2* y, const PixCoord& p, const Wts& w) {
+  const float2 a = cscale(d_fwd_t(y, p.i, p.t, p.T, p.sWH), w.it);
+  return make_float2(-a.x, -a.y);
+}
+
 // utils::SymmetricDivergence, 8-argument form (utils.cpp:961-1012)
 AVX_D void symdiv(float2* const* wv, const PixCoord& p, const Wts& w, float2 (&d)[3]) {
   const float2 *w0 = wv[0], *w1 = wv[1], *w2 = wv[2], *w3 = wv[3], *w4 = wv[4], *w5 = wv[5];

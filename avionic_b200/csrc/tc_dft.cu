@@ -570,11 +570,11 @@ void launch_b1_tile_transpose(const float2* b1, float2* b1t, int W, int H, int C
 }
 
 cudaError_t configure_tc_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(ydft_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(ydft_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(ydft_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  e = cudaFuncSetAttribute(ydft_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(coladj_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  return cudaFuncSetAttribute(coladj_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
 }
 
 void launch_coladj_tc(const KArgs& k, float2* img, cudaStream_t s) {

@@ -8,8 +8,9 @@
  *   operators  <- BaseOperator / CartesianOperator
  *                 (CUDA/include/base_operator.h:24-112,
  *                  CUDA/include/cartesian_operator.h:22-125)
- *   solvers    <- PDRecon / TV / TGV2 / ICTGV2
- *                 (CUDA/include/pd_recon.h:88-185, tv.h, tgv2.h, ictgv2.h)
+ *   solvers    <- PDRecon / TV / TVTEMP / TGV2 / ICTV / ICTGV2
+ *                 (CUDA/include/pd_recon.h:88-185, tv.h, tv_temp.h, tgv2.h,
+ *                  ictv.h, ictgv2.h)
  *   utils      <- namespace utils stencils, norms, proximal maps, Ellipke
  *                 (CUDA/include/utils.h, CUDA/src/utils.cpp)
  *   host path  <- the avionic CLI's load -> reconstruct -> store sequence
@@ -58,8 +59,9 @@ enum {
   AVX_METHOD_ICTGV2 = 5
 };
 
-/* Union of PDParams, TGV2Params and ICTGV2Params
- * (CUDA/include/pd_recon.h:20-74, tgv2.h:9-16, ictgv2.h:9-21) plus the
+/* Union of PDParams, TVtempParams, TGV2Params, ICTVParams and ICTGV2Params
+ * (CUDA/include/pd_recon.h:20-74, tv_temp.h:14-16, tgv2.h:9-16, ictv.h:8-23,
+ * ictgv2.h:9-21) plus the
  * AdaptLambdaParams (pd_recon.h:20-32).  Fields a method does not use are
  * ignored. */
 typedef struct avx_pd_params {
@@ -68,11 +70,12 @@ typedef struct avx_pd_params {
   float sigma, tau, sigmaTauRatio;
   float timeSpaceWeight;
   float lambda;
-  float dx, dy, dt;          /* overwritten from timeSpaceWeight by a run, as in the reference */
-  float alpha0, alpha1;      /* TGV2 / ICTGV2 */
-  float alpha;               /* ICTGV2 trade-off */
-  float timeSpaceWeight2;    /* ICTGV2 second branch */
-  float dx2, dy2, dt2;       /* ICTGV2 second branch (overwritten by a run) */
+  float dx, dy, dt;          /* overwritten from timeSpaceWeight by a run, as in the reference
+                                (TVtemp keeps them: its dt weights the temporal difference) */
+  float alpha0, alpha1;      /* alpha0: TGV2 / ICTGV2; alpha1: TGV2 / ICTV / ICTGV2 */
+  float alpha;               /* ICTV / ICTGV2 trade-off */
+  float timeSpaceWeight2;    /* ICTV / ICTGV2 second branch */
+  float dx2, dy2, dt2;       /* ICTV / ICTGV2 second branch (overwritten by a run) */
   int adaptLambda;           /* 1: lambda = AdaptLambda(adaptK, adaptD) at solver creation */
   float adaptK, adaptD;
 } avx_pd_params;
@@ -161,13 +164,15 @@ void avx_operator_destroy(avx_operator* op);
 /* Primal-dual solvers                                                 */
 /* ------------------------------------------------------------------ */
 
-/* InitParams() defaults of TV / TGV2 / ICTGV2 (tv.cpp:39-57,
- * tgv2.cpp:36-56, ictgv2.cpp:37-63), with adaptLambda = 1 and the method's
- * (k, d). */
+/* InitParams() defaults of TV / TVTEMP / TGV2 / ICTV / ICTGV2 (tv.cpp:39-57,
+ * tv_temp.cpp:39-54, tgv2.cpp:36-56, ictv.cpp:37-60, ictgv2.cpp:37-63), with
+ * adaptLambda = 1 and the method's (k, d).  TVtemp's dx and dy, which its
+ * InitParams leaves unset and only its gap's TV norm reads, are 1. */
 avx_status avx_default_params(int method, avx_pd_params* params);
 
-/* TV/TGV2/ICTGV2(width, height, coils, frames, params, mrOp)
- * (tv.cpp:13-19, tgv2.cpp:10-16, ictgv2.cpp:11-17).  params == NULL uses
+/* TV/TVTEMP/TGV2/ICTV/ICTGV2(width, height, coils, frames, params, mrOp)
+ * (tv.cpp:13-19, tv_temp.cpp:13-19, tgv2.cpp:10-16, ictv.cpp:11-17,
+ * ictgv2.cpp:11-17).  params == NULL uses
  * avx_default_params.  When params->adaptLambda is set, lambda is replaced
  * by AdaptLambda(adaptK, adaptD) here (InitLambda, tv.cpp:25-37).  The
  * solver keeps a pointer to op, which must outlive it. */
@@ -192,22 +197,27 @@ avx_status avx_solver_set_stream(avx_solver* s, void* cuda_stream);          /* 
 avx_status avx_solver_run(avx_solver* s, const avx_cf32* d_data, avx_cf32* d_x, const avx_cf32* d_b1);
 
 /* AdaptStepSize on given extragradient differences (tv.cpp:79-97,
- * tgv2.cpp:89-128, ictgv2.cpp:97-161).  d_diff holds P component pointers
- * (TV 1: e; TGV2 4: e1, e2[3]; ICTGV2 8: e1, e2[3], e3, e4[3]). */
+ * tv_temp.cpp:80-95, tgv2.cpp:89-128, ictv.cpp:97-128, ictgv2.cpp:97-161).
+ * d_diff holds P component pointers (TV, TVtemp 1: e; ICTV 2: e1, e3;
+ * TGV2 4: e1, e2[3]; ICTGV2 8: e1, e2[3], e3, e4[3]).  ICTV's norm of K e
+ * covers the data term alone: the reference's gradient sums land in a buffer
+ * that it then overwrites (ictv.cpp:104-125). */
 avx_status avx_solver_adapt_step_size(avx_solver* s, const avx_cf32* const* d_diff, const avx_cf32* d_b1);
 
-/* ComputeGStar / ComputePDGap (tv.cpp:202-235, tgv2.cpp:130-176,
- * ictgv2.cpp:178-249) on given primal components (P pointers, as above), dual
- * components (D pointers: TV 3, TGV2 9, ICTGV2 18), dense z and data.  The
+/* ComputeGStar / ComputePDGap (tv.cpp:202-235, tv_temp.cpp:184-224,
+ * tgv2.cpp:130-176, ictv.cpp:146-200, ictgv2.cpp:178-249) on given primal
+ * components (P pointers, as above), dual components (D pointers: TV 3,
+ * TVtemp 1, ICTV 6, TGV2 9, ICTGV2 18), dense z and data.  The
  * gap is returned un-normalised, as ComputePDGap returns it.  Uses the
  * solver's current params (dx.. as set, no time-space recomputation). */
 avx_status avx_solver_compute_gap(avx_solver* s, const avx_cf32* const* d_x, const avx_cf32* const* d_y,
                                   const avx_cf32* d_z, const avx_cf32* d_data, const avx_cf32* d_b1,
                                   double* gstar, double* gap);
 
-/* ExportAdditionalResults (tv.cpp:237-248, tgv2.cpp:340-355,
- * ictgv2.cpp:494-516): x3_component (ICTGV2), and with debug on PDGap,
- * ICTGVnorm, DATAfidelity (ICTGV2). */
+/* ExportAdditionalResults (tv.cpp:237-248, tv_temp.cpp:226-236,
+ * tgv2.cpp:340-355, ictv.cpp:372-391, ictgv2.cpp:494-516): x3_component
+ * (ICTV, ICTGV2), and with debug on PDGap, ICTGVnorm and DATAfidelity
+ * (ICTGV2), ictvnorm and DATAfidelity (ICTV). */
 avx_status avx_solver_export(avx_solver* s, const char* output_dir, avx_export_cb cb, void* user);
 avx_status avx_solver_get_stats(const avx_solver* s, avx_run_stats* stats);
 
@@ -337,6 +347,21 @@ avx_status avx_coil_construction_radial(unsigned W, unsigned H, unsigned C, unsi
                                         const avx_coil_params* p, const float* d_traj, const float* d_dens,
                                         const avx_cf32* d_kdata, avx_cf32* d_u, avx_cf32* d_b1);
 
+/* Data normalisation of the CLI's -o switch (main.cpp:573-579 ->
+ * RawDataPreparation::NormalizeData, raw_data_preparation.cpp:340-378).
+ * Cartesian (S == 0; d_mask = W*H*T mask, d_dens unused): the time-averaged
+ * coil combination |u| of the centred transform (NormalizeCartData,
+ * :821-844), factor 255 / m.  Radial (S > 0 samples per frame; d_mask = the
+ * trajectory, d_dens the density): |u| = sqrt(sum_c |crec_c|^2) of the radial
+ * time average (NormalizeNonCartData, :742-786), factor 255 T / m.  m is
+ * FindNormalizationFactor (:661-686): the median of the first maximum of |u|
+ * and every later value >= 0.9 of it.  d_kdata (the CLI's masked or
+ * sqrt(w)-weighted k-space) is scaled in place; *datanorm receives the
+ * factor (written as datanorm_factor.bin by the CLI, main.cpp:793-796).
+ * AVX_E_NUMERIC when |u| is zero everywhere. */
+avx_status avx_normalize_data(unsigned W, unsigned H, unsigned C, unsigned T, unsigned S, const float* d_mask,
+                              const float* d_dens, avx_cf32* d_kdata, float* datanorm);
+
 /* ------------------------------------------------------------------ */
 /* Batched and served reconstructions                                  */
 /* ------------------------------------------------------------------ */
@@ -351,7 +376,7 @@ avx_status avx_coil_construction_radial(unsigned W, unsigned H, unsigned C, unsi
  * avx_solver_run on the same inputs).  Buffers are the caller's device
  * buffers and must stay valid until the request's completion is polled. */
 typedef struct avx_request {
-  int method;                /* AVX_METHOD_TV / _TGV2 / _ICTGV2 */
+  int method;                /* AVX_METHOD_TV / _TVTEMP / _TGV2 / _ICTV / _ICTGV2 */
   int op_kind;               /* 0 Cartesian, 1 radial */
   unsigned width, height, coils, frames;
   avx_pd_params params;      /* as for avx_solver_create (lambda adapted when asked) */

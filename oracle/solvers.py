@@ -1,10 +1,11 @@
-"""TV / TGV2 / ICTGV2 primal-dual loops (float64), following the reference C++.
+"""TV / TVtemp / TGV2 / ICTV / ICTGV2 primal-dual loops (float64), following
+the reference C++.
 
 Test infrastructure (see ``oracle/__init__``).  The loop order, the step-size
 schedule (adapt at k < 10 or k % 50 == 0), the gap cadence and the early-exit
-points follow ``CUDA/src/tv.cpp:99-200``, ``tgv2.cpp:180-338`` and
-``ictgv2.cpp:294-492`` (the drop-in semantics), not the MATLAB variants, which
-adapt every iteration.
+points follow ``CUDA/src/tv.cpp:99-200``, ``tv_temp.cpp:95-182``,
+``tgv2.cpp:180-338``, ``ictv.cpp:202-370`` and ``ictgv2.cpp:294-492`` (the
+drop-in semantics), not the MATLAB variants, which adapt every iteration.
 
 ``norm1`` of a complex vector: the reference calls AGILE ``norm1`` in the
 G* terms (tv.cpp:225, tgv2.cpp:150-160, ictgv2.cpp:205-226).  Which of
@@ -49,6 +50,7 @@ class Params:
         self.alpha0 = np.sqrt(2.0)
         self.alpha1 = 1.0
         self.alpha = 0.6423
+        self.dt = 1.0  # TVtemp only: its temporal step (no time-space weighting)
         self.debug = False
         self.debugstep = 1
         self.verbose = False
@@ -65,9 +67,18 @@ class Params:
 
 def init_params(method):
     """The InitParams() defaults of the reference solvers (tv.cpp:39-57,
-    tgv2.cpp:36-56, ictgv2.cpp:37-63); lambda is left for adapt_lambda."""
+    tv_temp.cpp:39-54, tgv2.cpp:36-56, ictv.cpp:37-60, ictgv2.cpp:37-63);
+    lambda is left for adapt_lambda."""
     p = Params()
-    if method == "TV":
+    if method == "TVTEMP":
+        p.dt = 1.0
+        p.adapt_kd = (0.4 * 0.2991, 10.0 * 0.2991)
+    elif method == "ICTV":
+        p.timeSpaceWeight = 4.0
+        p.timeSpaceWeight2 = 0.5
+        p.alpha = 0.5
+        p.adapt_kd = (0.4 / (5.1191 * 0.35), 10.0 / (5.1191 * 0.35))
+    elif method == "TV":
         p.timeSpaceWeight = 5.0
         p.adapt_kd = (0.4 * 0.2991, 10.0 * 0.2991)
     elif method == "TGV2":
@@ -359,6 +370,138 @@ def ictgv2(data, x1, b1, op, p, trace=None):
     return x1
 
 
+# ---------------------------------------------------------------------------
+# TVtemp
+# ---------------------------------------------------------------------------
+
+def tvtemp_adapt_step(p, op, e, b1):
+    """``TVTEMP::AdaptStepSize`` (tv_temp.cpp:80-95)."""
+    g = st.gradient_temp(e, p.dt)
+    kz = op.backward(e, b1)
+    nKx = np.sqrt(abs(dot_re(g[0], g[0]) + dot_re(kz, kz)))
+    nx = np.linalg.norm(e.ravel())
+    p.sigma, p.tau = st.step_rule(p.sigma, p.tau, nKx, nx, p.sigmaTauRatio)
+    return nKx, nx
+
+
+def tvtemp_gap(p, op, x, y, z, d, b1):
+    """``TVTEMP::ComputeGStar`` / ``ComputePDGap`` (tv_temp.cpp:184-224): the
+    regulariser term is the full TVNorm with dx = dy = 1 and the run's dt."""
+    r = op.backward(x, b1) - d
+    g1 = 0.5 * p.lam * dot_re(r, r)
+    g2 = dot_re(d, z) + dot_re(z, z) / (2.0 * p.lam)
+    g3 = norm1(op.forward(z, b1) - st.divergence_temp(y, p.dt))
+    return abs(g1 + g2 + g3 + st.tv_norm(x, 1.0, 1.0, p.dt))
+
+
+def tvtemp(data, x, b1, op, p, trace=None):
+    """``TVTEMP::IterativeReconstruction`` (tv_temp.cpp:95-182): TV along t
+    only, no time-space weighting."""
+    p = p.copy()
+    N = x.size
+    x = x.astype(np.complex128).copy()
+    ext = x.copy()
+    y = [np.zeros_like(x)]
+    z = np.zeros_like(data, dtype=np.complex128)
+    gaps, steps = [], []
+    k = 0
+    while k < p.maxIt:
+        g = st.gradient_temp(ext, p.dt)
+        y = [y[0] + p.sigma * g[0]]
+        z = z + p.sigma * op.backward(ext, b1)
+        y = st.prox1(y, 1.0)
+        z = (z - p.sigma * data) * (1.0 / (1.0 + p.sigma / p.lam))
+        img = op.forward(z, b1)
+        xn = x - p.tau * (img - st.divergence_temp(y, p.dt))
+        ext = 2.0 * xn - x
+        x = xn
+        if _step_due(k):
+            tvtemp_adapt_step(p, op, ext - x, b1)
+        steps.append((p.sigma, p.tau))
+        if _gap_due(p, k):
+            gap = tvtemp_gap(p, op, x, y, z, data, b1) / N
+            gaps.append(gap)
+            if gap < p.stopPDGap:
+                break
+        k += 1
+    if trace is not None:
+        trace.update(PDGap=gaps, steps=steps, iterations=k, y=y, z=z)
+    return x
+
+
+# ---------------------------------------------------------------------------
+# ICTV
+# ---------------------------------------------------------------------------
+
+def ictv_adapt_step(p, op, e1, e3, b1):
+    """``ICTV::AdaptStepSize`` (ictv.cpp:97-128).  The reference sums the
+    gradient terms into a buffer that it overwrites before use, so only the
+    data term enters nKx."""
+    kz = op.backward(e1, b1)
+    nKx = np.sqrt(abs(float(np.sum(np.abs(kz) ** 2))))
+    nx = np.sqrt(abs(float(np.sum(np.abs(e1) ** 2 + np.abs(e3) ** 2))))
+    p.sigma, p.tau = st.step_rule(p.sigma, p.tau, nKx, nx, p.sigmaTauRatio)
+    return nKx, nx
+
+
+def ictv_gap(p, op, x1, x3, y1, y3, z, d, b1, w1, w2):
+    """``ICTV::ComputeGStar`` / ``ComputePDGap`` (ictv.cpp:146-200)."""
+    r = op.backward(x1, b1) - d
+    g1 = 0.5 * p.lam * dot_re(r, r)
+    g2 = dot_re(d, z) + dot_re(z, z) / (2.0 * p.lam)
+    div1 = st.divergence(y1, *w1)
+    g3 = norm1(op.forward(z, b1) - div1)
+    g5 = norm1(div1 - st.divergence(y3, *w2))
+    return abs(g1 + g2 + g3 + g5 + st.ictv_norm(x1, x3, p.alpha1, p.alpha, w1, w2))
+
+
+def ictv(data, x1, b1, op, p, trace=None):
+    """``ICTV::IterativeReconstruction`` (ictv.cpp:202-370): infimal
+    convolution of two TV functionals with their own time-space weights."""
+    p = p.copy()
+    w1, w2 = ictgv2_weights(p)
+    N = x1.size
+    x1 = x1.astype(np.complex128).copy()
+    ext1 = x1.copy()
+    x3, ext3 = np.zeros_like(x1), np.zeros_like(x1)
+    y1 = [np.zeros_like(x1) for _ in range(3)]
+    y3 = [np.zeros_like(x1) for _ in range(3)]
+    z = np.zeros_like(data, dtype=np.complex128)
+    m = min(p.alpha, 1.0 - p.alpha)
+    gaps, nrm, fid, steps = [], [], [], []
+    k = 0
+    while k < p.maxIt:
+        g = st.gradient(ext1 - ext3, *w1)
+        y1 = [y1[i] + p.sigma * g[i] for i in range(3)]
+        g = st.gradient(ext3, *w2)
+        y3 = [y3[i] + p.sigma * g[i] for i in range(3)]
+        z = z + p.sigma * op.backward(ext1, b1)
+        y1 = st.prox3(y1, 1.0 / (p.alpha1 * (p.alpha / m)))
+        y3 = st.prox3(y3, 1.0 / (p.alpha1 * ((1.0 - p.alpha) / m)))
+        z = (z - p.sigma * data) * (1.0 / (1.0 + p.sigma / p.lam))
+        img = op.forward(z, b1)
+        div1 = st.divergence(y1, *w1)
+        x1n = x1 - p.tau * (img - div1)
+        x3n = x3 - p.tau * (div1 - st.divergence(y3, *w2))
+        ext1 = 2.0 * x1n - x1
+        ext3 = 2.0 * x3n - x3
+        x1, x3 = x1n, x3n
+        if _step_due(k):
+            ictv_adapt_step(p, op, ext1 - x1, ext3 - x3, b1)
+        steps.append((p.sigma, p.tau))
+        if _gap_due(p, k):
+            gap = ictv_gap(p, op, x1, x3, y1, y3, z, data, b1, w1, w2) / N
+            gaps.append(gap)
+            nrm.append(st.ictv_norm(x1, x3, p.alpha1, p.alpha, w1, w2))
+            fid.append(ictgv2_data_fidelity(p, op, x1, data, b1))
+            if gap < p.stopPDGap:
+                break
+        k += 1
+    if trace is not None:
+        trace.update(PDGap=gaps, ictvnorm=nrm, DATAfidelity=fid, steps=steps, iterations=k, x3=x3, w1=w1, w2=w2)
+    return x1
+
+
 def run(method, data, x0, b1, op, p, trace=None):
-    return {"TV": tv, "TGV2": tgv2, "ICTGV2": ictgv2}[method.upper()](
+    return {"TV": tv, "TVTEMP": tvtemp, "TGV2": tgv2, "ICTV": ictv, "ICTGV2": ictgv2}[method.upper()](
         data, x0, b1, op, p, trace)

@@ -85,6 +85,29 @@ def divergence(y, dx=1.0, dy=1.0, dt=1.0):
     return -(diff_t(y[0], 1) / dx + diff_t(y[1], 2) / dy + diff_t(y[2], 3) / dt)
 
 
+def gradient_temp(u, dt=1.0):
+    """``utils::Gradient_temp`` (utils.cpp:134-143): [D+t u / dt]."""
+    return [diff(u, 3) / dt]
+
+
+def divergence_temp(y, dt=1.0):
+    """``utils::Divergence_temp`` (utils.cpp:795-805) = -(D+t)^T y / dt."""
+    return -(diff_t(y[0], 3) / dt)
+
+
+def prox1(y, scale):
+    """``utils::ProximalMap1D`` (utils.cpp:1307-1311): y / max(1, scale*|y|)."""
+    d = np.maximum(1.0, scale * np.abs(y[0]))
+    return [y[0] / d]
+
+
+def ictv_norm(x1, x3, alpha1, alpha, w1, w2):
+    """``utils::ICTVNorm`` (utils.cpp:1221-1242)."""
+    m = min(alpha, 1.0 - alpha)
+    return (alpha1 * (alpha / m) * tv_norm(x1 - x3, *w1)
+            + alpha1 * ((1.0 - alpha) / m) * tv_norm(x3, *w2))
+
+
 def sym_gradient(v, dx=1.0, dy=1.0, dt=1.0):
     """``utils::SymmetricGradient`` 7-argument form used by the PD loops
     (utils.cpp:397-456).  Off-diagonal order (xy, xt, yt).  The yt term

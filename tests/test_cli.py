@@ -79,7 +79,7 @@ def test_bin_format_roundtrip(tmp_path):
 
 @needs_exe
 @pytest.mark.gpu
-@pytest.mark.parametrize("method", ["TV", "TGV2", "ICTGV2"])
+@pytest.mark.parametrize("method", ["TV", "TVTEMP", "TGV2", "ICTV", "ICTGV2"])
 def test_cli_reconstruction_matches_oracle(tmp_path, method):
     from avionic_b200 import synth
     from oracle import solvers as so
@@ -90,9 +90,11 @@ def test_cli_reconstruction_matches_oracle(tmp_path, method):
     out = str(tmp_path / "recon.bin")
     cfg = tmp_path / "run.cfg"
     common = "lambda = 2.5\nsigma = 0.3333\ntau = 0.3333\nsigmaTauRatio = 1.0\n"
-    cfg.write_text("maxIt = 80\n[tv]\n" + common + "timeSpaceWeight = 3.0\n[tgv2]\n" + common +
-                   "timeSpaceWeight = 1.4\nalpha0 = 1.41421356\nalpha1 = 1.0\n[ictgv2]\n" + common +
-                   "timeSpaceWeight = 4.0\ntimeSpaceWeight2 = 0.5\nalpha = 0.5\nalpha0 = 1.41421356\n"
+    cfg.write_text("maxIt = 80\n[tv]\n" + common + "timeSpaceWeight = 3.0\n[tvtemp]\n" + common +
+                   "dt = 1.0\n[tgv2]\n" + common +
+                   "timeSpaceWeight = 1.4\nalpha0 = 1.41421356\nalpha1 = 1.0\n[ictv]\n" + common +
+                   "timeSpaceWeight = 4.0\ntimeSpaceWeight2 = 0.5\nalpha = 0.5\nalpha1 = 1.0\n[ictgv2]\n" +
+                   common + "timeSpaceWeight = 4.0\ntimeSpaceWeight2 = 0.5\nalpha = 0.5\nalpha0 = 1.41421356\n"
                    "alpha1 = 1.0\n")
     r = run(["-m", method, "-p", str(cfg), "-e", "-g", "10", "-d", dims, "-s", paths["b1"], "-u", paths["u0"],
              paths["kdata"], paths["mask"], out])
@@ -102,8 +104,8 @@ def test_cli_reconstruction_matches_oracle(tmp_path, method):
     op = CartesianOperator(W, H, C, T, mask=prob["mask"], centered=False)
     p = so.init_params(method)
     p.maxIt, p.lam, p.sigma, p.tau = 80, 2.5, 0.3333, 0.3333
-    p.timeSpaceWeight = {"TV": 3.0, "TGV2": 1.4, "ICTGV2": 4.0}[method]
-    p.timeSpaceWeight2, p.alpha = 0.5, 0.5
+    p.timeSpaceWeight = {"TV": 3.0, "TVTEMP": 5.0, "TGV2": 1.4, "ICTV": 4.0, "ICTGV2": 4.0}[method]
+    p.timeSpaceWeight2, p.alpha, p.alpha1 = 0.5, 0.5, 1.0
     p.alpha0 = 1.41421356
     p.debug, p.debugstep = True, 10
     tr = {}
@@ -117,6 +119,42 @@ def test_cli_reconstruction_matches_oracle(tmp_path, method):
     if method == "ICTGV2":
         assert binfmt.read_bin(str(tmp_path / "x3_component")).size == T * H * W
         assert binfmt.read_bin(str(tmp_path / "ICTGVnorm")).size == len(tr["ICTGVnorm"])
+    if method == "ICTV":
+        assert binfmt.read_bin(str(tmp_path / "x3_component")).size == T * H * W
+        assert np.allclose(binfmt.read_bin(str(tmp_path / "ictvnorm")).real, tr["ictvnorm"], rtol=1e-3)
+
+
+@needs_exe
+@pytest.mark.gpu
+def test_cli_normalisation(tmp_path):
+    """-o: the data are scaled by 255 / median of the centred time average's
+    top values before the run (main.cpp:573-579); datanorm_factor.bin holds
+    the factor (main.cpp:793-796) and the image is the reconstruction of the
+    scaled data."""
+    from avionic_b200 import synth
+    from oracle import solvers as so
+    from oracle.cartesian import CartesianOperator
+    from oracle.normalize import normalization_factor
+    prob = synth.small(23)
+    T, C, H, W = prob["kdata"].shape
+    paths, dims = write_problem(tmp_path, prob)
+    out = str(tmp_path / "recon.bin")
+    cfg = tmp_path / "run.cfg"
+    cfg.write_text("maxIt = 60\n[tv]\nlambda = 2.5\nsigma = 0.3333\ntau = 0.3333\ntimeSpaceWeight = 3.0\n")
+    r = run(["-m", "TV", "-o", "-p", str(cfg), "-g", "0", "-d", dims, "-s", paths["b1"], "-u", paths["u0"],
+             paths["kdata"], paths["mask"], out])
+    assert r.returncode == 0, r.stderr + r.stdout
+    f = binfmt.read_bin(str(tmp_path / "datanorm_factor.bin"))
+    k64 = prob["kdata"].astype(complex) * prob["mask"][:, None]
+    fo = normalization_factor(k64, prob["mask"])
+    assert f.size == 1 and abs(f[0] - fo) / fo < 1e-5
+    x = binfmt.read_bin(out).reshape(T, H, W)
+    op = CartesianOperator(W, H, C, T, mask=prob["mask"], centered=False)
+    p = so.init_params("TV")
+    p.maxIt, p.lam, p.sigma, p.tau, p.timeSpaceWeight = 60, 2.5, 0.3333, 0.3333, 3.0
+    ks = (prob["kdata"] * np.float32(f[0].real)).astype(complex) * prob["mask"][:, None]
+    xo = so.run("TV", ks, np.zeros((T, H, W), complex), prob["b1"].astype(complex), op, p, {})
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-4
 
 
 @needs_exe
