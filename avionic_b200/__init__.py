@@ -142,7 +142,7 @@ class CartesianOperator:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h and h.value:
+        if h and h.value and lib is not None:  # lib is None once the interpreter is shutting down
             lib.avx_operator_destroy(h)
             self.handle = ctypes.c_void_p()
 
@@ -251,7 +251,7 @@ class Solver:
 
     def __del__(self):
         h = getattr(self, "handle", None)
-        if h and h.value:
+        if h and h.value and lib is not None:  # lib is None once the interpreter is shutting down
             lib.avx_solver_destroy(h)
             self.handle = ctypes.c_void_p()
 
