@@ -469,7 +469,8 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
     g.radx[i] = i < g.nradx ? rx[i] : 0;
     g.rady[i] = i < g.nrady ? ry[i] : 0;
   }
-  if (avx::radial_fft_smem_bytes(std::max(g.Gx, g.Gy)) > AVX_DYN_SMEM_MAX)
+  if (avx::radial_fft_smem_bytes(std::max(g.Gx, g.Gy)) > AVX_DYN_SMEM_MAX ||
+      avx::radial_adj_smem_bytes(g.Gx, W) > AVX_DYN_SMEM_MAX)
     return fail(AVX_E_UNSUPPORTED, "oversampled grid too large for the grid FFT tile");
   std::vector<float2> twx(g.Gx), twy(g.Gy);
   for (int j = 0; j < g.Gx; ++j) twx[j] = make_float2((float)std::cos(2.0 * M_PI * j / g.Gx), (float)std::sin(2.0 * M_PI * j / g.Gx));
@@ -753,15 +754,13 @@ static RArgs solver_rargs(avx_solver* s, const float2* b1, const float2* in, con
 static void radial_pass(avx_solver* s, int mode, const float2* b1, const float2* in, const float2* in2,
                         cudaEvent_t* ev = nullptr) {
   RArgs r = solver_rargs(s, b1, in, in2);
-  avx::launch_rad_pad(r, s->stream);
-  avx::launch_rad_fft(r, -1, s->stream);
+  avx::launch_rad_forward_grid(r, s->stream);
   if (ev) cudaEventRecord(ev[0], s->stream);
   avx::launch_rad_interp(r, mode, s->stream);
   if (ev) cudaEventRecord(ev[1], s->stream);
   if (mode == 1) return;
   avx::launch_rad_spread(r, s->z.p, s->stream);
-  avx::launch_rad_fft(r, +1, s->stream);
-  avx::launch_rad_crop(r, s->op->r_khz.p, s->stream);
+  avx::launch_rad_adjoint_image(r, s->op->r_khz.p, s->stream);
   if (ev) cudaEventRecord(ev[2], s->stream);
 }
 
@@ -1172,8 +1171,7 @@ avx_status coil_time_averaged_radial(int W, int H, int C, int T, int S, const fl
       AVX_CK(cudaMemcpyAsync(samp.p + (size_t)f * S, kdata + ((size_t)f * C + c) * S, S * sizeof(float2),
                              cudaMemcpyDeviceToDevice, s));
     avx::launch_rad_spread(ra, samp.p, s);
-    avx::launch_rad_fft(ra, +1, s);
-    avx::launch_rad_crop(ra, crec + (size_t)c * W * H, s);
+    avx::launch_rad_adjoint_image(ra, crec + (size_t)c * W * H, s);
   }
   avx::launch_ta_combine(crec, u, W * H, C, 1.f, apply_phase, s);
   AVX_CK(cudaGetLastError());
@@ -1366,8 +1364,7 @@ avx_status avx_operator_backward(avx_operator* op, const avx_cf32* d_x, avx_cf32
   if (op->kind == 1) {
     RArgs ra = make_rargs(op, reinterpret_cast<const float2*>(d_b1), reinterpret_cast<const float2*>(d_x), nullptr);
     ra.out = reinterpret_cast<float2*>(d_k);
-    avx::launch_rad_pad(ra, 0);
-    avx::launch_rad_fft(ra, -1, 0);
+    avx::launch_rad_forward_grid(ra, 0);
     avx::launch_rad_interp(ra, 3, 0);
     AVX_CK(cudaGetLastError());
     AVX_CK(cudaDeviceSynchronize());
@@ -1394,8 +1391,7 @@ avx_status avx_operator_forward(avx_operator* op, avx_cf32* d_k, avx_cf32* d_x, 
   if (op->kind == 1) {
     RArgs ra = make_rargs(op, reinterpret_cast<const float2*>(d_b1), nullptr, nullptr);
     avx::launch_rad_spread(ra, reinterpret_cast<const float2*>(d_k), 0);
-    avx::launch_rad_fft(ra, +1, 0);
-    avx::launch_rad_crop(ra, reinterpret_cast<float2*>(d_x), 0);
+    avx::launch_rad_adjoint_image(ra, reinterpret_cast<float2*>(d_x), 0);
     AVX_CK(cudaGetLastError());
     AVX_CK(cudaDeviceSynchronize());
     return AVX_OK;

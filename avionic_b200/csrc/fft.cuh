@@ -122,3 +122,129 @@ __device__ float2* row_fft(float2* src, float2* dst, const float2* tw, int W, in
   return src;
 }
 
+
+// ---------------------------------------------------------------------------
+// Compile-time plans.  The same Stockham passes as row_fft with the radix
+// sequence, the sequence length, the direction and the block size (NT
+// threads) fixed at compile time, so that the index arithmetic folds to
+// shifts and constants.  Plans exist for the lengths fft_plan_id() lists;
+// row_fft_planned falls back to row_fft for the others.
+// ---------------------------------------------------------------------------
+
+template <int R, int SIGN>
+AVX_D void butterfly_fixed(float2 (&v)[R], const float2* tw, int nb) {
+  if constexpr (R == 2) {
+    const float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if constexpr (R == 4) {
+    const float2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    const float2 b0 = cadd(v[1], v[3]), b1 = csub(v[1], v[3]);
+    const float2 ib1 = SIGN > 0 ? make_float2(-b1.y, b1.x) : make_float2(b1.y, -b1.x);  // i*sign*b1
+    v[0] = cadd(a0, b0);
+    v[1] = cadd(a1, ib1);
+    v[2] = csub(a0, b0);
+    v[3] = csub(a1, ib1);
+  } else if constexpr (R == 3) {
+    const float2 t1 = cadd(v[1], v[2]);
+    const float2 t2 = make_float2(v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y);
+    const float2 d = csub(v[1], v[2]);
+    const float h = 0.86602540378443864676f * (float)SIGN;
+    const float2 id = make_float2(-h * d.y, h * d.x);  // i*sign*(sqrt(3)/2)*(v1 - v2)
+    v[0] = cadd(v[0], t1);
+    v[1] = cadd(t2, id);
+    v[2] = csub(t2, id);
+  } else {
+    // direct R-point DFT with the table's R-th roots of unity (index (m q mod R) nb)
+    float2 o[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      float2 acc = v[0];
+#pragma unroll
+      for (int m = 1; m < R; ++m) {
+        const float2 w = tw[((m * q) % R) * nb];
+        cfma(acc, v[m], make_float2(w.x, SIGN > 0 ? w.y : -w.y));
+      }
+      o[q] = acc;
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = o[q];
+  }
+}
+
+template <int KC, int NT, int W, int SIGN, int NS, int R>
+AVX_D void fft_pass_fixed(const float2* src, float2* dst, const float2* tw) {
+  constexpr int KCP = KC + 2, NB = W / R, TWS = W / (NS * R), TOTAL = NB * KC;
+#pragma unroll
+  for (int e0 = 0; e0 < TOTAL; e0 += NT) {
+    const int e = e0 + (int)threadIdx.x;
+    if (TOTAL % NT != 0 && e >= TOTAL) break;
+    const int kk = e % KC, j = e / KC;
+    const int q = j / NS, k = j - q * NS;
+    const int idxD = q * NS * R + k;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const float2 s0 = src[(j + r * NB) * KCP + kk];
+      if (r == 0) {
+        v[r] = s0;
+      } else {
+        const float2 w = tw[r * k * TWS];
+        v[r] = cmul(s0, make_float2(w.x, SIGN > 0 ? w.y : -w.y));
+      }
+    }
+    butterfly_fixed<R, SIGN>(v, tw, NB);
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[(idxD + r * NS) * KCP + kk] = v[r];
+  }
+}
+
+template <int KC, int NT, int W, int SIGN, int NS>
+AVX_D float2* fft_fixed_rec(float2* src, float2*, const float2*) {
+  return src;
+}
+
+template <int KC, int NT, int W, int SIGN, int NS, int R, int... Rest>
+AVX_D float2* fft_fixed_rec(float2* src, float2* dst, const float2* tw) {
+  fft_pass_fixed<KC, NT, W, SIGN, NS, R>(src, dst, tw);
+  __syncthreads();
+  return fft_fixed_rec<KC, NT, W, SIGN, NS * R, Rest...>(dst, src, tw);
+}
+
+// Plan identifiers: a length with a compile-time plan is its own identifier;
+// 1 = a run-time plan whose radices are at most 5, 0 = any run-time plan.
+// The compile-time radix orders are those of the host's run-time plans.
+inline int fft_plan_id(int n, int nrad, const int* rad) {
+  switch (n) {
+    case 96: case 128: case 160: case 192: case 256: case 320: return n;
+    default: break;
+  }
+  for (int i = 0; i < nrad; ++i)
+    if (rad[i] > 5) return 0;
+  return 1;
+}
+
+// row_fft with a plan chosen at compile time; blockDim.x must be 256
+template <int KC, int PLAN, int SIGN>
+AVX_D float2* row_fft_planned(float2* src, float2* dst, const float2* tw, int W, int nrad, const int* rad) {
+  if constexpr (PLAN == 96) return fft_fixed_rec<KC, 256, 96, SIGN, 1, 4, 4, 2, 3>(src, dst, tw);
+  else if constexpr (PLAN == 128) return fft_fixed_rec<KC, 256, 128, SIGN, 1, 4, 4, 4, 2>(src, dst, tw);
+  else if constexpr (PLAN == 160) return fft_fixed_rec<KC, 256, 160, SIGN, 1, 4, 4, 2, 5>(src, dst, tw);
+  else if constexpr (PLAN == 192) return fft_fixed_rec<KC, 256, 192, SIGN, 1, 4, 4, 4, 3>(src, dst, tw);
+  else if constexpr (PLAN == 256) return fft_fixed_rec<KC, 256, 256, SIGN, 1, 4, 4, 4, 4>(src, dst, tw);
+  else if constexpr (PLAN == 320) return fft_fixed_rec<KC, 256, 320, SIGN, 1, 4, 4, 4, 5>(src, dst, tw);
+  else return row_fft<KC, PLAN == 0>(src, dst, tw, W, nrad, rad, SIGN);
+}
+
+// calls CALL(id) with the compile-time plan identifier id
+#define AVX_FFT_PLAN_DISPATCH(ID, CALL) \
+  switch (ID) {                         \
+    case 96: CALL(96); break;           \
+    case 128: CALL(128); break;         \
+    case 160: CALL(160); break;         \
+    case 192: CALL(192); break;         \
+    case 256: CALL(256); break;         \
+    case 320: CALL(320); break;         \
+    case 1: CALL(1); break;             \
+    default: CALL(0); break;            \
+  }

@@ -231,7 +231,7 @@ size_t ydft_smem_bytes(int H) { return sizeof(float2) * (size_t)H * (YD_XS + KSP
 // Each CTA reads and rewrites only its own block of k.qp.
 // ---------------------------------------------------------------------------
 
-template <int KC, bool LARGE>
+template <int KC, int PLAN>
 __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
   if (a.st && a.st->stop && mode != 3) return;
   constexpr int KCP = KC + 2;
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
     __syncthreads();
     float2* Xb = X;  // buffer holding the row transform, index (kx - sx) mod W with the FFT
     if (g.nrad) {
-      Xb = row_fft<KC, LARGE>(P, X, twx, W, g.nrad, splan, +1);
+      Xb = row_fft_planned<KC, PLAN, +1>(P, X, twx, W, g.nrad, splan);
     } else {
       // dense DFT along x: thread per kx
       for (int kx = tid; kx < W; kx += nt) {
@@ -383,7 +383,7 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
     __syncthreads();
     if (g.nrad) {
       // inverse row FFT; Xb position n holds kx = n + sx, the result position n holds x = n + sx
-      float2* Qb = row_fft<KC, LARGE>(Xb, Xb == X ? P : X, twx, W, g.nrad, splan, -1);
+      float2* Qb = row_fft_planned<KC, PLAN, -1>(Xb, Xb == X ? P : X, twx, W, g.nrad, splan);
       for (int e = tid; e < kc * W; e += nt) {
         const int kk = fast_div(e, (unsigned)W, mW), x = e - kk * W;
         int n = x - g.sx;
@@ -922,12 +922,10 @@ void launch_ydft(const KArgs& k, cudaStream_t s) {
 }
 
 void launch_rows(const KArgs& k, int mode, cudaStream_t s) {
-  bool large = false;
-  for (int i = 0; i < k.g.nrad; ++i) large = large || k.g.rad[i] > 5;
-  if (large)
-    rows_kernel<KSPACE_KC, true><<<k.g.C * k.g.T, 256, rows_smem_bytes(k.g.W), s>>>(k, mode);
-  else
-    rows_kernel<KSPACE_KC, false><<<k.g.C * k.g.T, 256, rows_smem_bytes(k.g.W), s>>>(k, mode);
+  // 256 threads, as the compile-time FFT plans assume
+#define CALL_R(ID) rows_kernel<KSPACE_KC, ID><<<k.g.C * k.g.T, 256, rows_smem_bytes(k.g.W), s>>>(k, mode)
+  AVX_FFT_PLAN_DISPATCH(fft_plan_id(k.g.W, k.g.nrad, k.g.rad), CALL_R)
+#undef CALL_R
 }
 
 void launch_kspace(const KArgs& k, int mode, cudaStream_t s) {
@@ -1027,9 +1025,14 @@ cudaError_t configure_kernels() {
   // opt in to the full 227 KB of dynamic shared memory per CTA (sm_100)
   cudaError_t e = cudaFuncSetAttribute(ydft_kernel<KSPACE_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(rows_kernel<KSPACE_KC, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(rows_kernel<KSPACE_KC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
+  for (int id : {96, 128, 160, 192, 256, 320, 1, 0}) {
+#define SET_R(ID) \
+  e = cudaFuncSetAttribute(rows_kernel<KSPACE_KC, ID>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX)
+    AVX_FFT_PLAN_DISPATCH(id, SET_R)
+#undef SET_R
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 }  // namespace avx

@@ -1,8 +1,9 @@
 // Radial gridding operator kernels (see radial.cuh and oracle/radial.py).
 //
-// Forward  (image -> samples): pad+deapodise -> 2D DFT (sign -1) -> interpolate
-// Adjoint  (samples -> image): spread (sector gather) -> 2D DFT (sign +1) ->
-//                              crop+deapodise+coil-combine
+// Forward  (image -> samples): row DFT fused with pad+deapodise (sign -1) ->
+//                              column DFT -> interpolate
+// Adjoint  (samples -> image): spread (sector gather) -> column DFT (sign +1) ->
+//                              row DFT fused with crop+deapodise+coil-combine
 // The spreading step gathers: one CTA per (frame, sector) owns the sector's
 // grid cells and reads every sample of the 3x3 neighbouring sectors, so each
 // grid value is a fixed-order sum (no floating-point atomics, deterministic).
@@ -14,6 +15,7 @@
 namespace avx {
 
 #define RAD_FFT_KC 16
+#define RAD_ADJ_KC 8  // image rows per CTA of the adjoint's fused row pass
 #define RAD_SPREAD_BATCH 64
 
 // tapered Kaiser-Bessel weight at offset u (grid units); zero for |u| >= J/2
@@ -28,6 +30,9 @@ AVX_D int imod(int a, int n) {
   return r < 0 ? r + n : r;
 }
 
+// a mod n for -n <= a < 2n
+AVX_D int wrap1(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
+
 // grid index -> image index along one axis, or -1 outside the image
 AVX_D int grid_to_img(int m, int d, int G) {
   const int h = d / 2;
@@ -36,54 +41,100 @@ AVX_D int grid_to_img(int m, int d, int G) {
   return -1;
 }
 
-__global__ void rad_pad_kernel(RArgs a) {
-  const RadialGeomDev& g = a.g;
-  const int slice = blockIdx.y;  // f * C + c
-  const int c = slice % g.C, f = slice / g.C;
-  const int cell = blockIdx.x * blockDim.x + threadIdx.x;
-  if (cell >= g.Gx * g.Gy) return;
-  const int gy = cell / g.Gx, gx = cell % g.Gx;
-  const int ny = grid_to_img(gy, g.H, g.Gy), nx = grid_to_img(gx, g.W, g.Gx);
-  float2 v = czero();
-  if (ny >= 0 && nx >= 0) {
-    const long long pi = ((long long)f * g.H + ny) * g.W + nx;
-    float2 u = a.in[pi];
-    if (a.in2) u = csub(u, a.in2[pi]);
-    v = cscale(cmul(a.b1[((long long)c * g.H + ny) * g.W + nx], u), g.inv_psi_y[ny] * g.inv_psi_x[nx]);
-  }
-  a.grid[(long long)slice * g.Gx * g.Gy + cell] = v;
-}
-
-// rows (along x) of 16 grid lines per CTA
-__global__ void __launch_bounds__(256) rad_fft_rows_kernel(RArgs a, int sign) {
+// Forward, first pass: 16 grid rows of slice (f, c) per CTA, each formed from
+// the zero-padded, deapodised b1 (in - in2) and transformed along x with
+// sign -1.  Chunks without image rows store zeros.
+template <int PLAN>
+__global__ void __launch_bounds__(256) rad_rows_fwd_kernel(RArgs a) {
   constexpr int KC = RAD_FFT_KC, KCP = KC + 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RadialGeomDev& g = a.g;
   const int G = g.Gx;
-  float2* A = reinterpret_cast<float2*>(smem_raw);
-  float2* B = A + (size_t)G * KCP;
-  float2* tw = B + (size_t)G * KCP;
   const int slice = blockIdx.y;
+  const int c = slice % g.C, f = slice / g.C;
   const int r0 = blockIdx.x * KC;
   const int rows = min(KC, g.Gy - r0);
   float2* base = a.grid + (long long)slice * g.Gx * g.Gy;
+  bool any = false;  // the same for every thread of the CTA
+  for (int kk = 0; kk < rows; ++kk) any = any || grid_to_img(r0 + kk, g.H, g.Gy) >= 0;
+  if (!any) {
+    for (int e = threadIdx.x; e < rows * G; e += blockDim.x) base[(long long)r0 * G + e] = czero();
+    return;
+  }
+  float2* A = reinterpret_cast<float2*>(smem_raw);
+  float2* B = A + (size_t)G * KCP;
+  float2* tw = B + (size_t)G * KCP;
   __shared__ int splan[12];
   stage_plan(g.radx, splan);
   for (int j = threadIdx.x; j < G; j += blockDim.x) tw[j] = g.twgx[j];
   for (int e = threadIdx.x; e < KC * G; e += blockDim.x) {
-    const int kk = e / G, x = e % G;
-    A[x * KCP + kk] = kk < rows ? base[(long long)(r0 + kk) * G + x] : czero();
+    const int kk = e / G, mx = e % G;
+    const int ny = kk < rows ? grid_to_img(r0 + kk, g.H, g.Gy) : -1, nx = grid_to_img(mx, g.W, g.Gx);
+    float2 v = czero();
+    if (ny >= 0 && nx >= 0) {
+      const long long pi = ((long long)f * g.H + ny) * g.W + nx;
+      float2 u = a.in[pi];
+      if (a.in2) u = csub(u, a.in2[pi]);
+      v = cscale(cmul(a.b1[((long long)c * g.H + ny) * g.W + nx], u), g.inv_psi_y[ny] * g.inv_psi_x[nx]);
+    }
+    A[mx * KCP + kk] = v;
   }
   __syncthreads();
-  const float2* R = row_fft<KC>(A, B, tw, G, g.nradx, splan, sign);
+  const float2* R = row_fft_planned<KC, PLAN, -1>(A, B, tw, G, g.nradx, splan);
   for (int e = threadIdx.x; e < rows * G; e += blockDim.x) {
     const int kk = e / G, x = e % G;
     base[(long long)(r0 + kk) * G + x] = R[x * KCP + kk];
   }
 }
 
-// columns (along y) of 16 grid columns per CTA
-__global__ void __launch_bounds__(256) rad_fft_cols_kernel(RArgs a, int sign) {
+// Adjoint, last pass: RAD_ADJ_KC image rows of frame f per CTA.  For every
+// coil the matching grid rows are transformed along x with sign +1, cropped,
+// multiplied by conj(b1) and summed; the sum is deapodised into img.
+template <int PLAN>
+__global__ void __launch_bounds__(256) rad_rows_adj_kernel(RArgs a, float2* img) {
+  if (a.st && a.st->stop) return;
+  constexpr int KC = RAD_ADJ_KC, KCP = KC + 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const RadialGeomDev& g = a.g;
+  const int G = g.Gx, W = g.W;
+  const int f = blockIdx.y;
+  const int y0 = blockIdx.x * KC;
+  const int rows = min(KC, g.H - y0);
+  float2* A = reinterpret_cast<float2*>(smem_raw);
+  float2* B = A + (size_t)G * KCP;
+  float2* tw = B + (size_t)G * KCP;
+  float2* acc = tw + G;  // [KC][W]
+  __shared__ int splan[12];
+  stage_plan(g.radx, splan);
+  for (int j = threadIdx.x; j < G; j += blockDim.x) tw[j] = g.twgx[j];
+  for (int e = threadIdx.x; e < KC * W; e += blockDim.x) acc[e] = czero();
+  for (int c = 0; c < g.C; ++c) {
+    const float2* base = a.grid + ((long long)f * g.C + c) * g.Gx * g.Gy;
+    __syncthreads();
+    for (int e = threadIdx.x; e < KC * G; e += blockDim.x) {
+      const int kk = e / G, mx = e % G;
+      const int my = imod(y0 + kk - g.H / 2, g.Gy);
+      A[mx * KCP + kk] = kk < rows ? base[(long long)my * G + mx] : czero();
+    }
+    __syncthreads();
+    const float2* R = row_fft_planned<KC, PLAN, +1>(A, B, tw, G, g.nradx, splan);
+    // each thread owns the same entries of acc in every coil pass
+    for (int e = threadIdx.x; e < rows * W; e += blockDim.x) {
+      const int kk = e / W, x = e % W;
+      const int mx = imod(x - W / 2, G);
+      const float2 bv = a.b1[((long long)c * g.H + y0 + kk) * W + x];
+      acc[e] = cadd(acc[e], cmulc(bv, R[mx * KCP + kk]));
+    }
+  }
+  for (int e = threadIdx.x; e < rows * W; e += blockDim.x) {
+    const int kk = e / W, x = e % W, y = y0 + kk;
+    img[((long long)f * g.H + y) * W + x] = cscale(acc[e], g.inv_psi_y[y] * g.inv_psi_x[x]);
+  }
+}
+
+// columns (along y) of 16 grid columns per CTA, in place
+template <int PLAN, int SIGN>
+__global__ void __launch_bounds__(256) rad_fft_cols_kernel(RArgs a) {
   constexpr int KC = RAD_FFT_KC, KCP = KC + 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RadialGeomDev& g = a.g;
@@ -103,7 +154,7 @@ __global__ void __launch_bounds__(256) rad_fft_cols_kernel(RArgs a, int sign) {
     A[y * KCP + kk] = kk < cols ? base[(long long)y * g.Gx + c0 + kk] : czero();
   }
   __syncthreads();
-  const float2* R = row_fft<KC>(A, B, tw, G, g.nrady, splan, sign);
+  const float2* R = row_fft_planned<KC, PLAN, SIGN>(A, B, tw, G, g.nrady, splan);
   for (int e = threadIdx.x; e < KC * G; e += blockDim.x) {
     const int kk = e % KC, y = e / KC;
     if (kk < cols) base[(long long)y * g.Gx + c0 + kk] = R[y * KCP + kk];
@@ -156,8 +207,8 @@ __global__ void __launch_bounds__(256) rad_interp_kernel(RArgs a, int mode) {
     int ix[NW], iy[NW];
 #pragma unroll
     for (int o = 0; o < NW; ++o) {
-      ix[o] = imod(g0x + o, g.Gx);
-      iy[o] = imod(g0y + o, g.Gy);
+      ix[o] = wrap1(g0x + o, g.Gx);
+      iy[o] = wrap1(g0y + o, g.Gy);
     }
     const float sc = g.sqrt_w[(long long)f * g.S + s] * g.norm;
     const float sig = a.st ? (float)a.st->sigma : 0.f;
@@ -226,50 +277,73 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
   const int nsec = g.nsx * g.nsy;
   const int* order = g.order + (long long)f * g.S;
   const int* start = g.sec_start + (long long)f * (nsec + 1);
-  // distinct neighbouring sector offsets (fewer than three sectors along an axis wrap onto themselves)
-  const int dxn = g.nsx >= 3 ? 3 : g.nsx, dyn = g.nsy >= 3 ? 3 : g.nsy;
-  for (int c0 = 0; c0 < g.C; c0 += CC) {
-    const int cc = min(CC, g.C - c0);
-    float2 acc[CC];
-#pragma unroll
-    for (int k = 0; k < CC; ++k) acc[k] = czero();
-    for (int dy = 0; dy < dyn; ++dy) {
+  // The neighbourhood's samples, sector by sector in (dy, dx) order, as at
+  // most nine ranges of the sorted order; neighbouring sectors of one row
+  // are adjacent there and merge into one range.  The batches run over the
+  // ranges' concatenation, so a sparse neighbourhood takes a single batch.
+  __shared__ int s_rb[9], s_rl[9], s_nr, s_tot;
+  if (threadIdx.x == 0) {
+    // distinct neighbouring sector offsets (fewer than three sectors along an axis wrap onto themselves)
+    const int dxn = g.nsx >= 3 ? 3 : g.nsx, dyn = g.nsy >= 3 ? 3 : g.nsy;
+    int nr = 0, tot = 0;
+    for (int dy = 0; dy < dyn; ++dy)
       for (int dx = 0; dx < dxn; ++dx) {
         const int nsxi = imod(sxi + (dxn == 3 ? dx - 1 : dx), g.nsx);
         const int nsyi = imod(syi + (dyn == 3 ? dy - 1 : dy), g.nsy);
         const int ns = nsyi * g.nsx + nsxi;
         const int p0 = start[ns], p1 = start[ns + 1];
-        for (int b0 = p0; b0 < p1; b0 += RAD_SPREAD_BATCH) {
-          const int nb = min(RAD_SPREAD_BATCH, p1 - b0);
-          __syncthreads();
-          for (int e = threadIdx.x; e < nb; e += blockDim.x) {
-            const int j = order[b0 + e];
-            const long long fj = (long long)f * g.S + j;
-            const int2 g0 = g.win0[fj];
-            s_g0x[e] = g0.x;
-            s_g0y[e] = g0.y;
+        if (p1 <= p0) continue;
+        if (nr > 0 && s_rb[nr - 1] + s_rl[nr - 1] == p0) {
+          s_rl[nr - 1] += p1 - p0;
+        } else {
+          s_rb[nr] = p0;
+          s_rl[nr] = p1 - p0;
+          ++nr;
+        }
+        tot += p1 - p0;
+      }
+    s_nr = nr;
+    s_tot = tot;
+  }
+  __syncthreads();
+  const int nr = s_nr, tot = s_tot;
+  for (int c0 = 0; c0 < g.C; c0 += CC) {
+    const int cc = min(CC, g.C - c0);
+    float2 acc[CC];
 #pragma unroll
-            for (int o = 0; o < NW; ++o) {
-              s_wx[e][o] = g.winw[fj * 2 * NW + o];
-              s_wy[e][o] = g.winw[fj * 2 * NW + NW + o];
-            }
-            const float sc = g.sqrt_w[fj] * g.norm;
+    for (int k = 0; k < CC; ++k) acc[k] = czero();
+    for (int b0 = 0; b0 < tot; b0 += RAD_SPREAD_BATCH) {
+      const int nb = min(RAD_SPREAD_BATCH, tot - b0);
+      __syncthreads();
+      for (int e = threadIdx.x; e < nb; e += blockDim.x) {
+        int q = b0 + e, k = 0;
+        while (k < nr - 1 && q >= s_rl[k]) q -= s_rl[k++];
+        const int j = order[s_rb[k] + q];
+        const long long fj = (long long)f * g.S + j;
+        const int2 g0 = g.win0[fj];
+        s_g0x[e] = g0.x;
+        s_g0y[e] = g0.y;
 #pragma unroll
-            for (int k = 0; k < CC; ++k)
-              s_v[e][k] = k < cc ? cscale(samples[((long long)f * g.C + c0 + k) * g.S + j], sc) : czero();
-          }
-          __syncthreads();
-          if (active) {
-            for (int e = 0; e < nb; ++e) {
-              const int ox = imod(gx - s_g0x[e], g.Gx), oy = imod(gy - s_g0y[e], g.Gy);
-              if (ox < NW && oy < NW) {
-                const float w = s_wx[e][ox] * s_wy[e][oy];
+        for (int o = 0; o < NW; ++o) {
+          s_wx[e][o] = g.winw[fj * 2 * NW + o];
+          s_wy[e][o] = g.winw[fj * 2 * NW + NW + o];
+        }
+        const float sc = g.sqrt_w[fj] * g.norm;
 #pragma unroll
-                for (int k = 0; k < CC; ++k) {
-                  acc[k].x = fmaf(w, s_v[e][k].x, acc[k].x);
-                  acc[k].y = fmaf(w, s_v[e][k].y, acc[k].y);
-                }
-              }
+        for (int k = 0; k < CC; ++k)
+          s_v[e][k] = k < cc ? cscale(samples[((long long)f * g.C + c0 + k) * g.S + j], sc) : czero();
+      }
+      __syncthreads();
+      if (active) {
+        for (int e = 0; e < nb; ++e) {
+          // window starts lie within J of the grid, so one wrap suffices
+          const int ox = wrap1(gx - s_g0x[e], g.Gx), oy = wrap1(gy - s_g0y[e], g.Gy);
+          if (ox < NW && oy < NW) {
+            const float w = s_wx[e][ox] * s_wy[e][oy];
+#pragma unroll
+            for (int k = 0; k < CC; ++k) {
+              acc[k].x = fmaf(w, s_v[e][k].x, acc[k].x);
+              acc[k].y = fmaf(w, s_v[e][k].y, acc[k].y);
             }
           }
         }
@@ -283,44 +357,54 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
   }
 }
 
-__global__ void rad_crop_kernel(RArgs a, float2* img) {
-  if (a.st && a.st->stop) return;
-  const RadialGeomDev& g = a.g;
-  const int f = blockIdx.y;
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= g.W * g.H) return;
-  const int y = p / g.W, x = p % g.W;
-  const int my = imod(y - g.H / 2, g.Gy), mx = imod(x - g.W / 2, g.Gx);
-  float2 s = czero();
-  for (int c = 0; c < g.C; ++c) {
-    const float2 v = a.grid[(((long long)f * g.C + c) * g.Gy + my) * g.Gx + mx];
-    s = cadd(s, cmulc(a.b1[((long long)c * g.H + y) * g.W + x], v));
-  }
-  img[((long long)f * g.H + y) * g.W + x] = cscale(s, g.inv_psi_y[y] * g.inv_psi_x[x]);
-}
-
 // ---------------------------------------------------------------------------
 
 size_t radial_fft_smem_bytes(int G) { return sizeof(float2) * (2 * (size_t)G * (RAD_FFT_KC + 2) + G); }
+size_t radial_adj_smem_bytes(int G, int W) {
+  return sizeof(float2) * (2 * (size_t)G * (RAD_ADJ_KC + 2) + G + (size_t)RAD_ADJ_KC * W);
+}
 
 int radial_interp_blocks(const RadialGeomDev& g) { return (int)(((long long)g.T * g.S + 255) / 256); }
 
 cudaError_t configure_radial_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(rad_fft_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(rad_fft_cols_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
+  cudaError_t e = cudaSuccess;
+  for (int id : {96, 128, 160, 192, 256, 320, 1, 0}) {
+#define SET_K(ID)                                                                                                   \
+  e = cudaFuncSetAttribute(rad_fft_cols_kernel<ID, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX); \
+  if (e == cudaSuccess)                                                                                             \
+    e = cudaFuncSetAttribute(rad_fft_cols_kernel<ID, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);  \
+  if (e == cudaSuccess)                                                                                             \
+    e = cudaFuncSetAttribute(rad_rows_fwd_kernel<ID>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);     \
+  if (e == cudaSuccess)                                                                                             \
+    e = cudaFuncSetAttribute(rad_rows_adj_kernel<ID>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX)
+    AVX_FFT_PLAN_DISPATCH(id, SET_K)
+#undef SET_K
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
-void launch_rad_pad(const RArgs& a, cudaStream_t s) {
-  dim3 grid((a.g.Gx * a.g.Gy + 255) / 256, a.g.C * a.g.T);
-  rad_pad_kernel<<<grid, 256, 0, s>>>(a);
-}
-
-void launch_rad_fft(const RArgs& a, int sign, cudaStream_t s) {
+// every FFT kernel runs 256 threads, as the compile-time plans assume
+void launch_rad_forward_grid(const RArgs& a, cudaStream_t s) {
   dim3 gr((a.g.Gy + RAD_FFT_KC - 1) / RAD_FFT_KC, a.g.C * a.g.T);
-  rad_fft_rows_kernel<<<gr, 256, radial_fft_smem_bytes(a.g.Gx), s>>>(a, sign);
+#define CALL_F(ID) rad_rows_fwd_kernel<ID><<<gr, 256, radial_fft_smem_bytes(a.g.Gx), s>>>(a)
+  AVX_FFT_PLAN_DISPATCH(fft_plan_id(a.g.Gx, a.g.nradx, a.g.radx), CALL_F)
+#undef CALL_F
   dim3 gc((a.g.Gx + RAD_FFT_KC - 1) / RAD_FFT_KC, a.g.C * a.g.T);
-  rad_fft_cols_kernel<<<gc, 256, radial_fft_smem_bytes(a.g.Gy), s>>>(a, sign);
+#define CALL_C(ID) rad_fft_cols_kernel<ID, -1><<<gc, 256, radial_fft_smem_bytes(a.g.Gy), s>>>(a)
+  AVX_FFT_PLAN_DISPATCH(fft_plan_id(a.g.Gy, a.g.nrady, a.g.rady), CALL_C)
+#undef CALL_C
+}
+
+void launch_rad_adjoint_image(const RArgs& a, float2* img, cudaStream_t s) {
+  dim3 gc((a.g.Gx + RAD_FFT_KC - 1) / RAD_FFT_KC, a.g.C * a.g.T);
+#define CALL_C(ID) rad_fft_cols_kernel<ID, 1><<<gc, 256, radial_fft_smem_bytes(a.g.Gy), s>>>(a)
+  AVX_FFT_PLAN_DISPATCH(fft_plan_id(a.g.Gy, a.g.nrady, a.g.rady), CALL_C)
+#undef CALL_C
+  dim3 gr((a.g.H + RAD_ADJ_KC - 1) / RAD_ADJ_KC, a.g.T);
+#define CALL_A(ID) rad_rows_adj_kernel<ID><<<gr, 256, radial_adj_smem_bytes(a.g.Gx, a.g.W), s>>>(a, img)
+  AVX_FFT_PLAN_DISPATCH(fft_plan_id(a.g.Gx, a.g.nradx, a.g.radx), CALL_A)
+#undef CALL_A
 }
 
 #define RAD_NW_DISPATCH(NWV, CALL) \
@@ -367,9 +451,5 @@ void launch_rad_spread(const RArgs& a, const float2* samples, cudaStream_t s) {
   }
 }
 
-void launch_rad_crop(const RArgs& a, float2* img, cudaStream_t s) {
-  dim3 grid((a.g.W * a.g.H + 255) / 256, a.g.T);
-  rad_crop_kernel<<<grid, 256, 0, s>>>(a, img);
-}
 
 }  // namespace avx

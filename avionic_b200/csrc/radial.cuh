@@ -46,20 +46,21 @@ struct RArgs {
 namespace avx {
 
 size_t radial_fft_smem_bytes(int G);
+size_t radial_adj_smem_bytes(int G, int W);
 int radial_interp_blocks(const RadialGeomDev& g);
 cudaError_t configure_radial_kernels();
 
 // per-sample window starts and weights (g.win0, g.winw), once per operator
 void launch_rad_windows(const RadialGeomDev& g, int2* win0, float* winw, cudaStream_t s);
-// image -> grid: zero-padded, deapodised b1 * (in - in2)
-void launch_rad_pad(const RArgs& a, cudaStream_t s);
-// in-place unnormalised 2D DFT of every grid slice, sign -1 forward, +1 inverse
-void launch_rad_fft(const RArgs& a, int sign, cudaStream_t s);
 // grid -> samples; mode 0 z prox, 1 sum |K u|^2, 2 gap sums, 3 write samples to a.out
 void launch_rad_interp(const RArgs& a, int mode, cudaStream_t s);
+// forward image -> grid: the zero-padded, deapodised b1 (in - in2) and its
+// unnormalised 2D DFT (sign -1) in two passes, the padding fused into the row pass
+void launch_rad_forward_grid(const RArgs& a, cudaStream_t s);
+// adjoint grid -> image: column DFT (sign +1), then the row DFT fused with
+// the crop, deapodisation and coil combination with conj(b1) into img
+void launch_rad_adjoint_image(const RArgs& a, float2* img, cudaStream_t s);
 // samples (a.z, or a.in as samples when from_in) -> grid, by sector gather
 void launch_rad_spread(const RArgs& a, const float2* samples, cudaStream_t s);
-// grid -> image: crop, deapodise, coil-combine with conj(b1) into a.out
-void launch_rad_crop(const RArgs& a, float2* img, cudaStream_t s);
 
 }  // namespace avx
