@@ -264,15 +264,18 @@ __global__ void __launch_bounds__(256) rad_interp_kernel(RArgs a, int mode) {
 template <int NW, int CC>
 __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
   if (a.st && a.st->stop) return;
+  constexpr int NB = RAD_SPREAD_BATCH, NBP = NB + 1;  // NBP: padded rows, conflict-free column reads
   const RadialGeomDev& g = a.g;
-  __shared__ int s_g0x[RAD_SPREAD_BATCH], s_g0y[RAD_SPREAD_BATCH];
-  __shared__ float s_wx[RAD_SPREAD_BATCH][NW], s_wy[RAD_SPREAD_BATCH][NW];
-  __shared__ float2 s_v[RAD_SPREAD_BATCH][CC];
+  __shared__ int s_g0x[NB], s_g0y[NB];
+  __shared__ float s_wx[NW][NBP], s_wy[NW][NBP];
+  __shared__ float2 s_v[CC][NB];
+  __shared__ unsigned long long s_mask[2];  // staged samples whose window reaches this sector
   const int f = blockIdx.y;
   const int sec = blockIdx.x;
   const int sxi = sec % g.nsx, syi = sec / g.nsx;
+  const int X0 = sxi * g.sw, Y0 = syi * g.sw;
   const int lx = threadIdx.x % g.sw, ly = threadIdx.x / g.sw;
-  const int gx = sxi * g.sw + lx, gy = syi * g.sw + ly;
+  const int gx = X0 + lx, gy = Y0 + ly;
   const bool active = gx < g.Gx && gy < g.Gy;
   const int nsec = g.nsx * g.nsy;
   const int* order = g.order + (long long)f * g.S;
@@ -304,16 +307,22 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
       }
     s_nr = nr;
     s_tot = tot;
+    s_mask[0] = s_mask[1] = 0ull;
   }
   __syncthreads();
   const int nr = s_nr, tot = s_tot;
+  // the sector's cells, per axis: window offsets (cell - g0) mod G run over
+  // [d0, d0 + sw); the window reaches them when one of those is below NW
+  const int swx = min(g.sw, g.Gx - X0), swy = min(g.sw, g.Gy - Y0);
+  int bi = 0;  // batch counter over all coil passes (selects s_mask)
   for (int c0 = 0; c0 < g.C; c0 += CC) {
     const int cc = min(CC, g.C - c0);
     float2 acc[CC];
 #pragma unroll
     for (int k = 0; k < CC; ++k) acc[k] = czero();
-    for (int b0 = 0; b0 < tot; b0 += RAD_SPREAD_BATCH) {
-      const int nb = min(RAD_SPREAD_BATCH, tot - b0);
+    for (int b0 = 0; b0 < tot; b0 += NB, ++bi) {
+      const int nb = min(NB, tot - b0);
+      unsigned long long* mask = &s_mask[bi & 1];
       __syncthreads();
       for (int e = threadIdx.x; e < nb; e += blockDim.x) {
         int q = b0 + e, k = 0;
@@ -321,30 +330,38 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
         const int j = order[s_rb[k] + q];
         const long long fj = (long long)f * g.S + j;
         const int2 g0 = g.win0[fj];
+        const int dx0 = imod(X0 - g0.x, g.Gx), dy0 = imod(Y0 - g0.y, g.Gy);
+        const bool hit = (dx0 < NW || dx0 + swx > g.Gx) && (dy0 < NW || dy0 + swy > g.Gy);
+        if (!hit) continue;
+        atomicOr(mask, 1ull << e);  // bitwise OR: the result does not depend on the order
         s_g0x[e] = g0.x;
         s_g0y[e] = g0.y;
 #pragma unroll
         for (int o = 0; o < NW; ++o) {
-          s_wx[e][o] = g.winw[fj * 2 * NW + o];
-          s_wy[e][o] = g.winw[fj * 2 * NW + NW + o];
+          s_wx[o][e] = g.winw[fj * 2 * NW + o];
+          s_wy[o][e] = g.winw[fj * 2 * NW + NW + o];
         }
         const float sc = g.sqrt_w[fj] * g.norm;
 #pragma unroll
-        for (int k = 0; k < CC; ++k)
-          s_v[e][k] = k < cc ? cscale(samples[((long long)f * g.C + c0 + k) * g.S + j], sc) : czero();
+        for (int kc = 0; kc < CC; ++kc)
+          s_v[kc][e] = kc < cc ? cscale(samples[((long long)f * g.C + c0 + kc) * g.S + j], sc) : czero();
       }
       __syncthreads();
-      if (active) {
-        for (int e = 0; e < nb; ++e) {
-          // window starts lie within J of the grid, so one wrap suffices
-          const int ox = wrap1(gx - s_g0x[e], g.Gx), oy = wrap1(gy - s_g0y[e], g.Gy);
-          if (ox < NW && oy < NW) {
-            const float w = s_wx[e][ox] * s_wy[e][oy];
+      unsigned long long m = *mask;
+      // the other mask is free again (every thread read it before this batch's first barrier)
+      if (threadIdx.x == 0) s_mask[(bi + 1) & 1] = 0ull;
+      if (!active) continue;
+      while (m) {  // staged samples in order
+        const int e = __ffsll((long long)m) - 1;
+        m &= m - 1;
+        // window starts lie within J of the grid, so one wrap suffices
+        const int ox = wrap1(gx - s_g0x[e], g.Gx), oy = wrap1(gy - s_g0y[e], g.Gy);
+        if (ox < NW && oy < NW) {
+          const float w = s_wx[ox][e] * s_wy[oy][e];
 #pragma unroll
-            for (int k = 0; k < CC; ++k) {
-              acc[k].x = fmaf(w, s_v[e][k].x, acc[k].x);
-              acc[k].y = fmaf(w, s_v[e][k].y, acc[k].y);
-            }
+          for (int k = 0; k < CC; ++k) {
+            acc[k].x = fmaf(w, s_v[k][e].x, acc[k].x);
+            acc[k].y = fmaf(w, s_v[k][e].y, acc[k].y);
           }
         }
       }
@@ -442,6 +459,10 @@ void launch_rad_spread(const RArgs& a, const float2* samples, cudaStream_t s) {
 #undef CALL_S
   } else if (a.g.C <= 8) {
 #define CALL_S(N) rad_spread_kernel<N, 8><<<grid, threads, 0, s>>>(a, samples)
+    RAD_NW_DISPATCH(a.g.nw, CALL_S)
+#undef CALL_S
+  } else if (a.g.C == 12) {
+#define CALL_S(N) rad_spread_kernel<N, 12><<<grid, threads, 0, s>>>(a, samples)
     RAD_NW_DISPATCH(a.g.nw, CALL_S)
 #undef CALL_S
   } else {
