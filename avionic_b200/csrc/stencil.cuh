@@ -127,10 +127,15 @@ AVX_D float ss6(const float2 (&g)[6]) {
   return cabs2(g[0]) + cabs2(g[1]) + cabs2(g[2]) + 2.f * (cabs2(g[3]) + cabs2(g[4]) + cabs2(g[5]));
 }
 
-// y / max(1, scale * |y|): utils::ProximalMap3/6 (utils.cpp:1297-1351)
+// y / max(1, scale * |y|): utils::ProximalMap3/6 (utils.cpp:1297-1351).
+// Inside the ball y is left as it is; outside it is multiplied by one
+// reciprocal (one division per pixel instead of one per component).
 template <int K>
 AVX_D void prox_div(float2 (&y)[K], float n, float scale) {
-  float den = fmaxf(1.f, scale * n);
+  const float den = scale * n;
+  if (den > 1.f) {
+    const float inv = 1.f / den;
 #pragma unroll
-  for (int k = 0; k < K; ++k) y[k] = make_float2(y[k].x / den, y[k].y / den);
+    for (int k = 0; k < K; ++k) y[k] = make_float2(y[k].x * inv, y[k].y * inv);
+  }
 }
