@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
   constexpr int KCP = KC + 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const CartGeomDev& g = a.g;
-  const int W = g.W, C = g.C;
+  const int W = PLAN > 1 ? PLAN : g.W, C = g.C;  // W compile-time with a fixed plan
   const int c = blockIdx.x % C;
   const int t = blockIdx.x / C;
   const int r0 = g.row_off[t], r1 = g.row_off[t + 1];

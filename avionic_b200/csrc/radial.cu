@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(256) rad_rows_fwd_kernel(RArgs a) {
   constexpr int KC = RAD_FFT_KC, KCP = KC + 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RadialGeomDev& g = a.g;
-  const int G = g.Gx;
+  const int G = PLAN > 1 ? PLAN : g.Gx;  // compile-time with a fixed plan
   const int slice = blockIdx.y;
   const int c = slice % g.C, f = slice / g.C;
   const int r0 = blockIdx.x * KC;
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(256) rad_rows_adj_kernel(RArgs a, float2* img)
   constexpr int KC = RAD_ADJ_KC, KCP = KC + 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RadialGeomDev& g = a.g;
-  const int G = g.Gx, W = g.W;
+  const int G = PLAN > 1 ? PLAN : g.Gx, W = g.W;  // G compile-time with a fixed plan
   const int f = blockIdx.y;
   const int y0 = blockIdx.x * KC;
   const int rows = min(KC, g.H - y0);
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(256) rad_fft_cols_kernel(RArgs a) {
   constexpr int KC = RAD_FFT_KC, KCP = KC + 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RadialGeomDev& g = a.g;
-  const int G = g.Gy;
+  const int G = PLAN > 1 ? PLAN : g.Gy;  // compile-time with a fixed plan
   float2* A = reinterpret_cast<float2*>(smem_raw);
   float2* B = A + (size_t)G * KCP;
   float2* tw = B + (size_t)G * KCP;
