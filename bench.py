@@ -426,9 +426,9 @@ def main():
                     help="comma list: headline (config-1 line), radial, batched, serving (added to the line at N=1)")
     ap.add_argument("--batch-workers", type=int, default=8, help="concurrent reconstructions of the batched forms")
     ap.add_argument("--batch-size", type=int, default=64)
-    ap.add_argument("--serve-requests", type=int, default=8,
+    ap.add_argument("--serve-requests", type=int, default=24,
                     help="requests per rate (bounded sample of the 2000-request stream)")
-    ap.add_argument("--serve-rates", default="200",
+    ap.add_argument("--serve-rates", default="20,200",
                     help="comma list of arrival rates in requests/s (the configuration sweeps 20-200)")
     args = ap.parse_args()
     parts = set(args.parts.split(","))
