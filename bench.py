@@ -14,7 +14,9 @@ reference's step-rule schedule.
          (avx_reconstruct_host): host -> device copy of k-space, mask, coil
          maps and u0 and device -> host copy of the image inside the timed region
 Multi-GPU: one independent reconstruction per rank (instances shard with no
-collective); barrier + max-over-ranks device time.
+collective); barrier + max-over-ranks device time.  The batched
+configuration's 64 instances are partitioned across ranks by device
+footprint; its wall time is the slowest rank's.
 
 --impl reference times the reference algorithm's CPU restatement (the
 float64 oracle; the reference's own C++/CUDA and MATLAB code cannot run
@@ -224,14 +226,18 @@ def _rel_diff(torch, a, b):
     return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
 
 
-def run_batched(av, torch, workers, n=64, iters=800):
+def run_batched(av, torch, workers, n=64, iters=800, rank=0, world=1, dist=None):
     """The batched configuration: n TGV2 reconstructions of uneven size
     (800 iterations each), submitted at once.  The plain form is FP32
     y-transforms with one reconstruction at a time (workers = 1); the batched
-    form is split-BF16x3 with `workers` concurrent reconstructions."""
+    form is split-BF16x3 with `workers` concurrent reconstructions.  With
+    several ranks the instances are partitioned by device footprint (complex
+    values: the TGV2 fields and the k-space) and every rank runs its share;
+    the wall time is the slowest rank's."""
     from avionic_b200 import synth
     specs = synth.batched_specs(3, n)
-    items = [synth.cine_instance_gpu(sp) for sp in specs]
+    owner = shard_by_footprint([sp["W"] * sp["H"] * sp["T"] * (21 + sp["C"]) for sp in specs], world)
+    items = [synth.cine_instance_gpu(sp) for sp, o in zip(specs, owner) if o == rank]
     torch.cuda.synchronize()
 
     def make_request(it, out, dft, tag):
@@ -246,15 +252,17 @@ def run_batched(av, torch, workers, n=64, iters=800):
     for name, w, dft in (("plain_fp32_single", 1, av.DFT_FP32), ("split_single", 1, av.DFT_SPLIT_BF16X3),
                          ("fp32_batched", workers, av.DFT_FP32), ("split_batched", workers, av.DFT_SPLIT_BF16X3)):
         comps, o, wall = _batch_pass(av, torch, items, make_request, w, dft)
-        its = sum(c.stats.iterations for c in comps)
-        lat = [c.queue_ms + c.run_ms for c in comps]
+        wall = max_over_ranks(dist, wall, "cuda")
+        its = sum_over_ranks(dist, sum(c.stats.iterations for c in comps), "cuda")
+        lat = [c.queue_ms + c.run_ms for c in comps]  # this rank's requests
         forms[name] = {"workers": w, "recons_per_s": n / wall, "pd_it_per_s": its / wall, "wall_s": wall,
                        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
                        "split_dft_instances": int(sum(c.dft_mode == av.DFT_SPLIT_BF16X3 for c in comps))}
         outs[name] = o
     ref = outs["plain_fp32_single"]
     for name in forms:
-        forms[name]["max_rel_l2_vs_plain_fp32"] = max(_rel_diff(torch, a, b) for a, b in zip(outs[name], ref))
+        forms[name]["max_rel_l2_vs_plain_fp32"] = max_over_ranks(
+            dist, max(_rel_diff(torch, a, b) for a, b in zip(outs[name], ref)), "cuda")
     del items, outs
     torch.cuda.empty_cache()
     return {"workload": "%d TGV2 Cartesian reconstructions of uneven size (matrix 96-320, frames 8-48, coils 4-32, "
@@ -262,7 +270,8 @@ def run_batched(av, torch, workers, n=64, iters=800):
             "forms": forms,
             "speedup_split_batched_vs_plain_fp32_single": forms["split_batched"]["recons_per_s"] /
             forms["plain_fp32_single"]["recons_per_s"],
-            "timing": "host wall clock from the first submission to the last completion (several streams)"}
+            "timing": "host wall clock from the first submission to the last completion (several streams)"
+                      + ("; slowest of %d ranks, latencies of rank 0's share" % world if world > 1 else "")}
 
 
 def run_serving(av, torch, workers, n, rates, max_it=1500, rel_gap=1e-4):
@@ -383,6 +392,52 @@ def run_radial(av, torch, iters=500, steps=3):
             "rel_l2_vs_phantom": err}
 
 
+def max_over_ranks(dist, value, device):
+    """The job's time is its slowest rank's: the largest value over all ranks
+    (the value itself without a process group)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, value, device):
+    """The sum of value over all ranks (the value itself without a process group)."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def shard_by_footprint(footprints, world):
+    """Rank of every instance: the largest first, each to the rank with the
+    least footprint so far (the lowest rank on ties).  Every rank computes the
+    same assignment from the same list, so no exchange is needed."""
+    load = [0.0] * world
+    owner = [0] * len(footprints)
+    for i in sorted(range(len(footprints)), key=lambda k: (-footprints[k], k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[i] = r
+        load[r] += footprints[i]
+    return owner
+
+
+def job_rate(world, steps, ms):
+    """PD iterations per second of the whole job: each of `world` ranks runs
+    `steps` reconstructions of ITERS iterations; `ms` is the slowest rank's time."""
+    return world * steps * ITERS / (ms / 1000.0)
+
+
+def instance_seed(rank):
+    """Each rank reconstructs its own instance (weak scaling, no collective on
+    the data path)."""
+    return 1 + rank
+
+
 def run_reference(args, rank, world):
     """The reference arm: the oracle port on the host cores, rank 0 only."""
     if rank != 0:
@@ -445,28 +500,32 @@ def main():
     import avionic_b200 as av
 
     torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     extra = {}
-    if world == 1 and "batched" in parts:
-        extra["batched"] = run_batched(av, torch, args.batch_workers, args.batch_size)
+    if "batched" in parts:
+        extra["batched"] = run_batched(av, torch, args.batch_workers, args.batch_size, rank=rank, world=world,
+                                       dist=dist)
     if world == 1 and "radial" in parts:
         extra["radial"] = run_radial(av, torch)
     if world == 1 and "serving" in parts:
         extra["serving"] = run_serving(av, torch, args.batch_workers, args.serve_requests,
                                        [float(r) for r in args.serve_rates.split(",")])
     if "headline" not in parts:
-        print(json.dumps(extra), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(extra), flush=True)
         return
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    prob = make_problem(1 + rank)
+    prob = make_problem(instance_seed(rank))
     T, C, H, W = prob["kdata"].shape
     kd = av.to_device(prob["kdata"])
     md = av.to_device(prob["mask"])
@@ -507,13 +566,9 @@ def main():
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(dist, e0.elapsed_time(e1), "cuda")
     step_ms = [a.elapsed_time(b) for a, b in lat]
-    if dist is not None:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-    value = world * args.steps * ITERS / (ms / 1000.0)
+    value = job_rate(world, args.steps, ms)
 
     # the other arithmetic of the y-transforms, same problem and schedule (reported beside the headline)
     other = None
@@ -531,7 +586,7 @@ def main():
         g1.record()
         torch.cuda.synchronize()
         x_fp32 = x.clone()
-        other = {"dft": "fp32 CUDA cores", "value": world * args.steps * ITERS / (g0.elapsed_time(g1) / 1000.0),
+        other = {"dft": "fp32 CUDA cores", "value": job_rate(world, args.steps, max_over_ranks(dist, g0.elapsed_time(g1), "cuda")),
                  "unit": UNIT}
         op.dft_mode = av.DFT_SPLIT_BF16X3
         x.copy_(x0)
@@ -596,12 +651,8 @@ def main():
     f1.record()
     torch.cuda.synchronize()
     barrier()
-    ems = f0.elapsed_time(f1)
-    if dist is not None:
-        tt = torch.tensor([ems], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ems = float(tt.item())
-    e2e_value = world * args.steps * ITERS / (ems / 1000.0)
+    ems = max_over_ranks(dist, f0.elapsed_time(f1), "cuda")
+    e2e_value = job_rate(world, args.steps, ems)
     av.lib.avx_reconstruct_host_release()
     h2d = pk.numel() * 8 + pm.numel() * 4 + pb.numel() * 8 + pu.numel() * 8
     d2h = px.numel() * 8
