@@ -201,6 +201,18 @@ class Solver:
     def set_verbose(self, verbose):
         check(lib.avx_solver_set_verbose(self.handle, int(verbose)))
 
+    def set_tuning(self, autotune=True, primal_tile=0, dual_block=0):
+        """Launch shapes of the dual and primal kernels (avx_solver_set_tuning)."""
+        check(lib.avx_solver_set_tuning(self.handle, int(autotune), primal_tile, dual_block))
+
+    def tuning(self):
+        """(primal tile index, dual block index, primal tile name, dual threads) in use."""
+        p, d, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        name = ctypes.c_char_p()
+        check(lib.avx_solver_get_tuning(self.handle, ctypes.byref(p), ctypes.byref(d), ctypes.byref(name),
+                                        ctypes.byref(t)))
+        return p.value, d.value, name.value.decode(), t.value
+
     def set_stream(self, stream):
         check(lib.avx_solver_set_stream(self.handle, ctypes.c_void_p(stream)))
 

@@ -19,8 +19,10 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <thread>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -573,6 +575,9 @@ struct avx_solver {
   bool verbose = false, debug = false;
   int debugstep = 1;
   double stop_rel = 0.0;  // relative gap stop (avx_solver_set_relative_stop)
+  // launch shapes of the dual and primal kernels (avx_solver_set_tuning)
+  bool autotune = true, tuned = false;
+  int primal_tile = 0, dual_block = 0;
   cudaStream_t user_stream = 0;
   cudaStream_t stream = 0;
   // device state
@@ -673,7 +678,83 @@ static PDArgs make_pdargs(avx_solver* s) {
   a.ic_b = (float)((1.0 - alpha) / m);
   a.khz = s->op->r_khz.p;
   a.st = s->st.p;
+  a.primal_tile = s->primal_tile;
+  a.dual_block = s->dual_block;
   return a;
+}
+
+// Autotuner of the two field-streaming kernels' launch shapes.  The first run
+// of a (device, method, W, H, T) times every candidate shape on the solver's
+// own fields (3 warm-up and 5 timed launches each, CUDA events on its stream)
+// and keeps the fastest; later runs and solvers of that shape reuse it.  The
+// trial launches overwrite the fields, so the caller prepares them again.
+struct TuneKey {
+  int dev, method, W, H, T;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(dev, method, W, H, T) < std::tie(o.dev, o.method, o.W, o.H, o.T);
+  }
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, std::pair<int, int>> g_tune;
+
+static avx_status time_launches(avx_solver* s, void (*launch)(int, const PDArgs&, cudaStream_t), const PDArgs& a,
+                                float* ms) {
+  cudaEvent_t e0, e1;
+  AVX_CK(cudaEventCreate(&e0));
+  AVX_CK(cudaEventCreate(&e1));
+  for (int i = 0; i < 3; ++i) launch(s->method, a, s->stream);
+  AVX_CK(cudaEventRecord(e0, s->stream));
+  for (int i = 0; i < 5; ++i) launch(s->method, a, s->stream);
+  AVX_CK(cudaEventRecord(e1, s->stream));
+  AVX_CK(cudaEventSynchronize(e1));
+  AVX_CK(cudaEventElapsedTime(ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  AVX_CK(cudaGetLastError());
+  return AVX_OK;
+}
+
+static avx_status autotune(avx_solver* s) {
+  int dev = 0;
+  AVX_CK(cudaGetDevice(&dev));
+  const TuneKey key{dev, s->method, s->W, s->H, s->T};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      s->primal_tile = it->second.first;
+      s->dual_block = it->second.second;
+      s->tuned = true;
+      return AVX_OK;
+    }
+  }
+  PDArgs a = make_pdargs(s);
+  float best = 0.f;
+  for (int i = 0; i < AVX_PRIMAL_TILES; ++i) {
+    a.primal_tile = i;
+    float ms;
+    avx_status r = time_launches(s, avx::launch_primal, a, &ms);
+    if (r != AVX_OK) return r;
+    if (i == 0 || ms < best) {
+      best = ms;
+      s->primal_tile = i;
+    }
+  }
+  a.primal_tile = s->primal_tile;
+  for (int i = 0; i < AVX_DUAL_BLOCKS; ++i) {
+    a.dual_block = i;
+    float ms;
+    avx_status r = time_launches(s, avx::launch_dual, a, &ms);
+    if (r != AVX_OK) return r;
+    if (i == 0 || ms < best) {
+      best = ms;
+      s->dual_block = i;
+    }
+  }
+  s->tuned = true;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = {s->primal_tile, s->dual_block};
+  return AVX_OK;
 }
 
 static void set_tc(KArgs* k, const avx_operator* op) {
@@ -878,6 +959,12 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
   AVX_CK(cudaStreamWaitEvent(s->stream, evin, 0));
   r = prepare_run(s, data, x);
   if (r != AVX_OK) return r;
+  if (s->autotune && !s->tuned) {
+    r = autotune(s);
+    if (r != AVX_OK) return r;
+    r = prepare_run(s, data, x);  // the trial launches overwrote the fields
+    if (r != AVX_OK) return r;
+  }
   r = prepare_b1t(s, b1);
   if (r != AVX_OK) return r;
   if (s->method == AVX_METHOD_ICTGV2 && s->debug) {
@@ -900,7 +987,8 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
   avx_pd_params pk = s->p;
   pk.sigma = pk.tau = 0.f;
   const size_t key = (size_t)b1 ^ ((size_t)s->prim.p << 1) ^ ((size_t)s->op << 2) ^
-                     ((size_t)s->op->dft_mode << 7) ^ std::hash<std::string>()(std::string((const char*)&pk, sizeof(pk)));
+                     ((size_t)s->op->dft_mode << 7) ^ ((size_t)(s->primal_tile * 8 + s->dual_block) << 9) ^
+                     std::hash<std::string>()(std::string((const char*)&pk, sizeof(pk)));
   if (key != s->graph_key) {
     s->drop_graphs();
     s->graph_key = key;
@@ -1507,6 +1595,28 @@ avx_status avx_solver_set_relative_stop(avx_solver* s, double rel) {
   if (!(rel >= 0.0) || rel >= 1.0) return fail(AVX_E_ARG, "relative stop must lie in [0, 1)");
   s->stop_rel = rel;
   s->drop_graphs();
+  return AVX_OK;
+}
+
+avx_status avx_solver_set_tuning(avx_solver* s, int autotune, int primal_tile, int dual_block) {
+  if (!s) return fail(AVX_E_ARG, "null solver");
+  if (primal_tile < 0 || primal_tile >= AVX_PRIMAL_TILES || dual_block < 0 || dual_block >= AVX_DUAL_BLOCKS)
+    return fail(AVX_E_ARG, "tuning index out of range");
+  s->autotune = autotune != 0;
+  s->tuned = false;
+  s->primal_tile = primal_tile;
+  s->dual_block = dual_block;
+  s->drop_graphs();
+  return AVX_OK;
+}
+
+avx_status avx_solver_get_tuning(const avx_solver* s, int* primal_tile, int* dual_block, const char** primal_name,
+                                 int* dual_threads) {
+  if (!s) return fail(AVX_E_ARG, "null solver");
+  if (primal_tile) *primal_tile = s->primal_tile;
+  if (dual_block) *dual_block = s->dual_block;
+  if (primal_name) *primal_name = avx::primal_tile_name(s->primal_tile);
+  if (dual_threads) *dual_threads = avx::dual_block_threads(s->dual_block);
   return AVX_OK;
 }
 

@@ -45,6 +45,7 @@ struct PDArgs {
   float ic_a, ic_b;             // ICTGV2 branch factors alpha/m, (1-alpha)/m
   const float2* khz;            // K^H z image when the operator supplies it (radial)
   DevState* st;
+  int primal_tile, dual_block;  // launch shapes (indices into the tuning tables of pd_kernels.cu)
 };
 
 struct KArgs {

@@ -17,13 +17,11 @@
 #define ADJ_TY 4      // thread rows per tile
 #define ADJ_YP 4      // pixels per thread along y
 #define ADJ_TH (ADJ_TY * ADJ_YP)
-// primal kernel tile: PR_TX x PR_TY threads, PR_YP pixels per thread along y.
-// 32 x 8 x 1 measured fastest on B200 at 192 x 192 x 30 (ICTGV2): 68 us
-// against 90 us for 32 x 4 x 4 (more independent loads in flight per SM).
-#define PR_TX 32
-#define PR_TY 8
-#define PR_YP 1
-#define PR_TH (PR_TY * PR_YP)
+// Launch shapes the autotuner chooses from (PDArgs::primal_tile, dual_block):
+// primal tiles (threads along x, threads along y, pixels per thread along y)
+// and dual-kernel block sizes; index 0 of each is the untuned default.
+#define AVX_PRIMAL_TILES 5
+#define AVX_DUAL_BLOCKS 3
 
 // timed stages of one iteration (avx_solver_kernel_times)
 #define AVX_NSTAGE 5
@@ -50,6 +48,9 @@ void launch_iteration(int method, const PDArgs& a, const KArgs& k, float2* khz, 
                       cudaEvent_t* ev = nullptr);
 void launch_dual(int method, const PDArgs& a, cudaStream_t s);
 void launch_primal(int method, const PDArgs& a, cudaStream_t s);
+// the shape behind a tuning index: primal tile "TXxTYxYP", dual block "N threads"
+const char* primal_tile_name(int i);
+int dual_block_threads(int i);
 void launch_ydft(const KArgs& k, cudaStream_t s);
 void launch_rows(const KArgs& k, int mode, cudaStream_t s);
 void launch_step_img(int method, const PDArgs& a, const Ptr8& e_dev, int P, double* pimg, cudaStream_t s);

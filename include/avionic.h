@@ -190,6 +190,22 @@ avx_status avx_solver_set_debug(avx_solver* s, int debug, int debugstep);    /* 
 avx_status avx_solver_set_relative_stop(avx_solver* s, double rel);
 avx_status avx_solver_set_stream(avx_solver* s, void* cuda_stream);          /* cudaStream_t, 0 = default */
 
+/* No reference counterpart (the reference's AGILE kernels have fixed launch
+ * shapes).  Launch shapes of the dual and primal kernels: with autotune set
+ * (the default) the first run of a (device, method, W, H, T) times each
+ * candidate on the solver's own fields, keeps the fastest and reuses it for
+ * later runs and solvers of that shape in the process; with autotune clear
+ * the given indices are used.  primal_tile in [0, 5): 32x8x1, 32x4x2, 64x4x1,
+ * 32x4x4, 32x16x1 (threads along x, threads along y, pixels per thread along
+ * y); dual_block in [0, 3): 256, 128, 512 threads.  Index 0 is the default
+ * shape.  The shapes change the schedule only: every pixel's arithmetic is
+ * the same in all of them (results agree to rounding; the compiler may fuse
+ * multiply-adds differently in each). */
+avx_status avx_solver_set_tuning(avx_solver* s, int autotune, int primal_tile, int dual_block);
+/* The shapes in use (chosen by the autotuner after the first run); any output may be NULL. */
+avx_status avx_solver_get_tuning(const avx_solver* s, int* primal_tile, int* dual_block, const char** primal_name,
+                                 int* dual_threads);
+
 /* IterativeReconstruction(data, x, b1) (pd_recon.h:134-135): d_data dense
  * k-space (W*H*C*T), d_x initial image in / result out (W*H*T), d_b1 coil maps
  * (W*H*C).  Runs asynchronously on the solver's stream until the final

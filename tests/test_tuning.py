@@ -1,0 +1,68 @@
+"""Launch-shape autotuning of the dual and primal kernels (avx_solver_set_tuning).
+
+Every shape runs the same per-pixel arithmetic; the compiler may still fuse
+multiply-adds differently in each instantiation, so the images are compared
+to 1e-5 relative L2 (rounding level after 40 iterations, far below the 1e-4
+held against the oracle)."""
+
+import numpy as np
+import pytest
+
+REL = 1e-5
+
+
+def rel(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def _run(av, prob, method, autotune, primal_tile=0, dual_block=0, iters=40):
+    import torch
+    T, C, H, W = prob["kdata"].shape
+    op = av.CartesianOperator(W, H, C, T, mask=av.to_device(prob["mask"]), centered=False)
+    s = av.Solver(method, op)
+    p = s.params
+    p.maxIt = iters
+    s.params = p
+    s.set_tuning(autotune, primal_tile, dual_block)
+    x = torch.zeros((T, H, W), dtype=torch.complex64, device="cuda")
+    s.run(av.to_device(prob["kdata"]), x, av.to_device(prob["b1"]))
+    return x.cpu().numpy(), s.tuning()
+
+
+def test_rejects_bad_arguments_without_a_device():
+    import avionic_b200 as av
+    assert av.lib.avx_solver_set_tuning(None, 1, 0, 0) == 1  # AVX_E_ARG
+    assert av.lib.avx_solver_get_tuning(None, None, None, None, None) == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["TV", "ICTGV2"])
+def test_every_shape_gives_the_same_image(method):
+    import avionic_b200 as av
+    from avionic_b200 import synth
+    prob = synth.small(41, H=30, W=36, T=5, C=3)
+    ref, t0 = _run(av, prob, method, False)
+    assert t0[:2] == (0, 0)
+    for i in range(1, 5):
+        x, t = _run(av, prob, method, False, primal_tile=i)
+        assert t[0] == i
+        assert rel(x, ref) < REL, (i, t, rel(x, ref))
+    for j in range(1, 3):
+        x, t = _run(av, prob, method, False, dual_block=j)
+        assert t[1] == j
+        assert rel(x, ref) < REL, (j, t, rel(x, ref))
+
+
+@pytest.mark.gpu
+def test_autotuned_run_matches_and_is_reused():
+    import avionic_b200 as av
+    from avionic_b200 import synth
+    prob = synth.small(43, H=40, W=48, T=6, C=4)
+    ref, _ = _run(av, prob, "TGV2", False)
+    x, t = _run(av, prob, "TGV2", True)
+    assert 0 <= t[0] < 5 and 0 <= t[1] < 3
+    assert t[2] in ("32x8x1", "32x4x2", "64x4x1", "32x4x4", "32x16x1") and t[3] in (128, 256, 512)
+    assert rel(x, ref) < REL
+    # a second solver of the same shape takes the kept choice
+    _, t2 = _run(av, prob, "TGV2", True)
+    assert t2 == t
