@@ -2225,7 +2225,7 @@ size_t request_workspace(const avx_request& r, avx_status* st) {
   // solver: primal, extragradient and step scratch (3P), duals (D), z and d, reductions, history
   b += (3 * P + D) * N * c8 + 2 * kspace * c8;
   b += 8 * (size_t)std::max(AVX_RED_BLOCKS, avx::gap_img_blocks((int)W, (int)H, (int)T)) * 8;
-  b += 3 * (std::max(C * T, (T * std::max<size_t>(kspace / std::max<size_t>(C * T, 1), 1) + 255) / 256) + 1) * 8;
+  b += 3 * (std::max(C * T, (kspace + 255) / 256) + 1) * 8;
   b += 3 * ((size_t)r.params.maxIt + 3) * 8 + 4096;
   return b + b / 20 + ((size_t)16 << 20);  // arena alignment and chunk slack
 }

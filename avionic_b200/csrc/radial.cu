@@ -192,17 +192,21 @@ __global__ void __launch_bounds__(256) rad_interp_kernel(RArgs a, int mode) {
   if (a.st && a.st->stop && mode != 3) return;
   __shared__ double red[32 * 3];
   const RadialGeomDev& g = a.g;
+  // one thread per (frame, coil, sample), in the layout of z and d
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   double acc_r[3] = {0.0, 0.0, 0.0};
-  if (i < (long long)g.T * g.S) {
-    const int f = (int)(i / g.S), s = (int)(i % g.S);
-    const int2 g0 = g.win0[i];
+  if (i < (long long)g.T * g.C * g.S) {
+    const int s = (int)(i % g.S);
+    const long long fc = i / g.S;  // f * C + c
+    const int f = (int)(fc / g.C);
+    const long long fs = (long long)f * g.S + s;
+    const int2 g0 = g.win0[fs];
     const int g0x = g0.x, g0y = g0.y;
     float wx[NW], wy[NW];
 #pragma unroll
     for (int o = 0; o < NW; ++o) {
-      wx[o] = g.winw[i * 2 * NW + o];
-      wy[o] = g.winw[i * 2 * NW + NW + o];
+      wx[o] = g.winw[fs * 2 * NW + o];
+      wy[o] = g.winw[fs * 2 * NW + NW + o];
     }
     int ix[NW], iy[NW];
 #pragma unroll
@@ -210,11 +214,11 @@ __global__ void __launch_bounds__(256) rad_interp_kernel(RArgs a, int mode) {
       ix[o] = wrap1(g0x + o, g.Gx);
       iy[o] = wrap1(g0y + o, g.Gy);
     }
-    const float sc = g.sqrt_w[(long long)f * g.S + s] * g.norm;
+    const float sc = g.sqrt_w[fs] * g.norm;
     const float sig = a.st ? (float)a.st->sigma : 0.f;
     const float zscale = (mode == 0) ? (float)(1.0 / (1.0 + a.st->sigma / (double)a.lam)) : 1.f;
-    for (int c = 0; c < g.C; ++c) {
-      const float2* gr = a.grid + ((long long)f * g.C + c) * g.Gx * g.Gy;
+    {
+      const float2* gr = a.grid + fc * g.Gx * g.Gy;
       float2 v = czero();
 #pragma unroll
       for (int oy = 0; oy < NW; ++oy) {
@@ -229,7 +233,7 @@ __global__ void __launch_bounds__(256) rad_interp_kernel(RArgs a, int mode) {
         v.y = fmaf(wy[oy], row.y, v.y);
       }
       const float2 k = cscale(v, sc);
-      const long long zi = ((long long)f * g.C + c) * g.S + s;
+      const long long zi = i;
       if (mode == 0) {
         // z += sigma K x; z = (z - sigma d) / (1 + sigma / lambda)   (tgv2.cpp:254-264)
         const float2 zo = a.z[zi], dv = a.d[zi];
@@ -381,7 +385,7 @@ size_t radial_adj_smem_bytes(int G, int W) {
   return sizeof(float2) * (2 * (size_t)G * (RAD_ADJ_KC + 2) + G + (size_t)RAD_ADJ_KC * W);
 }
 
-int radial_interp_blocks(const RadialGeomDev& g) { return (int)(((long long)g.T * g.S + 255) / 256); }
+int radial_interp_blocks(const RadialGeomDev& g) { return (int)(((long long)g.T * g.C * g.S + 255) / 256); }
 
 cudaError_t configure_radial_kernels() {
   cudaError_t e = cudaSuccess;
