@@ -145,6 +145,24 @@ AVX_D void butterfly_fixed(float2 (&v)[R], const float2* tw, int nb) {
     v[1] = cadd(a1, ib1);
     v[2] = csub(a0, b0);
     v[3] = csub(a1, ib1);
+  } else if constexpr (R == 8) {
+    // two 4-point DFTs of the even and odd inputs, joined by the 8th roots of unity
+    float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+    butterfly_fixed<4, SIGN>(e, tw, nb);
+    butterfly_fixed<4, SIGN>(o, tw, nb);
+    constexpr float h = 0.70710678118654752440f;
+    const float s = (float)SIGN;
+    const float2 t1 = make_float2(h * (o[1].x - s * o[1].y), h * (o[1].y + s * o[1].x));    // o1 (1 + i s) / sqrt 2
+    const float2 t2 = make_float2(-s * o[2].y, s * o[2].x);                                 // o2 i s
+    const float2 t3 = make_float2(-h * (o[3].x + s * o[3].y), h * (s * o[3].x - o[3].y));  // o3 (-1 + i s) / sqrt 2
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], t1);
+    v[5] = csub(e[1], t1);
+    v[2] = cadd(e[2], t2);
+    v[6] = csub(e[2], t2);
+    v[3] = cadd(e[3], t3);
+    v[7] = csub(e[3], t3);
   } else if constexpr (R == 3) {
     const float2 t1 = cadd(v[1], v[2]);
     const float2 t2 = make_float2(v[0].x - 0.5f * t1.x, v[0].y - 0.5f * t1.y);
@@ -213,7 +231,8 @@ AVX_D float2* fft_fixed_rec(float2* src, float2* dst, const float2* tw) {
 
 // Plan identifiers: a length with a compile-time plan is its own identifier;
 // 1 = a run-time plan whose radices are at most 5, 0 = any run-time plan.
-// The compile-time radix orders are those of the host's run-time plans.
+// The compile-time plans lead with radix-8 passes (one shared-memory round
+// trip fewer than the run-time plans' radix-4 passes).
 inline int fft_plan_id(int n, int nrad, const int* rad) {
   switch (n) {
     case 96: case 128: case 160: case 192: case 256: case 320: return n;
@@ -227,12 +246,12 @@ inline int fft_plan_id(int n, int nrad, const int* rad) {
 // row_fft with a plan chosen at compile time; blockDim.x must be 256
 template <int KC, int PLAN, int SIGN>
 AVX_D float2* row_fft_planned(float2* src, float2* dst, const float2* tw, int W, int nrad, const int* rad) {
-  if constexpr (PLAN == 96) return fft_fixed_rec<KC, 256, 96, SIGN, 1, 4, 4, 2, 3>(src, dst, tw);
-  else if constexpr (PLAN == 128) return fft_fixed_rec<KC, 256, 128, SIGN, 1, 4, 4, 4, 2>(src, dst, tw);
-  else if constexpr (PLAN == 160) return fft_fixed_rec<KC, 256, 160, SIGN, 1, 4, 4, 2, 5>(src, dst, tw);
-  else if constexpr (PLAN == 192) return fft_fixed_rec<KC, 256, 192, SIGN, 1, 4, 4, 4, 3>(src, dst, tw);
-  else if constexpr (PLAN == 256) return fft_fixed_rec<KC, 256, 256, SIGN, 1, 4, 4, 4, 4>(src, dst, tw);
-  else if constexpr (PLAN == 320) return fft_fixed_rec<KC, 256, 320, SIGN, 1, 4, 4, 4, 5>(src, dst, tw);
+  if constexpr (PLAN == 96) return fft_fixed_rec<KC, 256, 96, SIGN, 1, 8, 4, 3>(src, dst, tw);
+  else if constexpr (PLAN == 128) return fft_fixed_rec<KC, 256, 128, SIGN, 1, 8, 8, 2>(src, dst, tw);
+  else if constexpr (PLAN == 160) return fft_fixed_rec<KC, 256, 160, SIGN, 1, 8, 4, 5>(src, dst, tw);
+  else if constexpr (PLAN == 192) return fft_fixed_rec<KC, 256, 192, SIGN, 1, 8, 8, 3>(src, dst, tw);
+  else if constexpr (PLAN == 256) return fft_fixed_rec<KC, 256, 256, SIGN, 1, 8, 8, 4>(src, dst, tw);
+  else if constexpr (PLAN == 320) return fft_fixed_rec<KC, 256, 320, SIGN, 1, 8, 8, 5>(src, dst, tw);
   else return row_fft<KC, PLAN == 0>(src, dst, tw, W, nrad, rad, SIGN);
 }
 
