@@ -65,6 +65,23 @@ def test_usage_and_errors(tmp_path):
     assert r.returncode == 255 and "truncated" in r.stderr
 
 
+@needs_exe
+def test_method_sections_declare_their_own_keys(tmp_path):
+    """[tvtemp] declares dt, sigma, tau, sigmaTauRatio and lambda only; [ictv]
+    has no alpha0 (options_parser.cpp:204-257)."""
+    rng = np.random.default_rng(1)
+    prob = {"kdata": (rng.standard_normal((2, 2, 4, 5)) + 0j).astype(np.complex64),
+            "mask": np.ones((2, 4, 5), np.float32), "b1": np.ones((2, 4, 5), np.complex64)}
+    paths, dims = write_problem(tmp_path, prob)
+    out = str(tmp_path / "x.bin")
+    for method, section, key in (("TVTEMP", "tvtemp", "dx"), ("TVTEMP", "tvtemp", "timeSpaceWeight"),
+                                 ("ICTV", "ictv", "alpha0")):
+        cfg = tmp_path / ("%s.cfg" % key)
+        cfg.write_text("[%s]\n%s = 1.0\n" % (section, key))
+        r = run(["-p", str(cfg), "-m", method, "-d", dims, "-s", paths["b1"], paths["kdata"], paths["mask"], out])
+        assert r.returncode == 255 and "unrecognised option '%s.%s'" % (section, key) in r.stderr
+
+
 def test_bin_format_roundtrip(tmp_path):
     """The .bin layout of matlab/writebin_vector.m:35-44."""
     v = np.arange(5) + 1j * np.arange(5, 10)
