@@ -414,6 +414,12 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
   const int lastx = g.Gx - (g.nsx - 1) * isw, lasty = g.Gy - (g.nsy - 1) * isw;
   if (J / 2.f > (float)std::min(lastx, lasty) || J / 2.f > (float)isw)
     return fail(AVX_E_ARG, "kernelWidth too wide for the sector layout");
+  // the kernels wrap window offsets with one add or subtract, which needs the
+  // trajectory in [-1/2, 1/2] and a grid wider than the window plus two cells
+  if ((float)std::min(g.Gx, g.Gy) <= J + 2.f)
+    return fail(AVX_E_ARG, "oversampled grid too small for the kernel width");
+  for (size_t i = 0; i < (size_t)T * 2 * S; ++i)
+    if (!(std::fabs(h_traj[i]) <= 0.5f)) return fail(AVX_E_ARG, "trajectory values must lie in [-0.5, 0.5]");
   g.nw = (int)std::ceil(J) + 1;
   g.J = J;
   const double beta = M_PI * std::sqrt((J / osf) * (J / osf) * (osf - 0.5) * (osf - 0.5) - 0.8);

@@ -30,7 +30,9 @@ AVX_D int imod(int a, int n) {
   return r < 0 ? r + n : r;
 }
 
-// a mod n for -n <= a < 2n
+// a mod n for -n <= a < 2n.  Window offsets on the grid lie in that range:
+// window starts g0 = floor(k G - J/2) with k in [-1/2, 1/2) lie in
+// [-G/2 - J/2 - 1, G/2), and the operator requires G > J + 2.
 AVX_D int wrap1(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
 
 // grid index -> image index along one axis, or -1 outside the image
@@ -334,7 +336,7 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
         const int j = order[s_rb[k] + q];
         const long long fj = (long long)f * g.S + j;
         const int2 g0 = g.win0[fj];
-        const int dx0 = imod(X0 - g0.x, g.Gx), dy0 = imod(Y0 - g0.y, g.Gy);
+        const int dx0 = wrap1(X0 - g0.x, g.Gx), dy0 = wrap1(Y0 - g0.y, g.Gy);
         const bool hit = (dx0 < NW || dx0 + swx > g.Gx) && (dy0 < NW || dy0 + swy > g.Gy);
         if (!hit) continue;
         atomicOr(mask, 1ull << e);  // bitwise OR: the result does not depend on the order

@@ -128,7 +128,8 @@ avx_status avx_operator_get_dft_mode(const avx_operator* op, int* mode);
 /* NoncartesianOperator(width, height, coils, frames, nSpokes, nFE,
  * spokesPerFrame, kTraj, dens, kernelWidth, sectorWidth, osf)
  * (CUDA/src/noncartesian_operator.cpp:3-86): the radial gridding operator.
- * d_traj holds per frame [kx(S) | ky(S)] in cycles/pixel, [-0.5, 0.5)
+ * d_traj holds per frame [kx(S) | ky(S)] in cycles/pixel, within [-0.5, 0.5]
+ * (AVX_E_ARG otherwise)
  * (S = nFE * spokesPerFrame); d_dens the density compensation w per frame
  * and sample.  K x = sqrt(w) NUFFT(b1 x) / sqrt(W H) with a tapered
  * Kaiser-Bessel gridding of width kernelWidth on a grid oversampled by osf,

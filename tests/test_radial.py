@@ -145,3 +145,16 @@ def test_radial_adapt_lambda(av):
     p = _problem(6)
     g, o = _ops(av, p)
     assert abs(g.adapt_lambda(0.34, 4.57) - o.adapt_lambda(0.34, 4.57, p["spf"])) < 1e-5
+
+
+@pytest.mark.gpu
+def test_trajectory_outside_the_grid_is_rejected():
+    """Window offsets are wrapped once; a trajectory beyond +-1/2 cycle/pixel is refused."""
+    import torch
+    import avionic_b200 as av
+    p = _problem(3)
+    tr = torch.from_numpy(p["traj"].astype(np.float32)).cuda()
+    de = torch.from_numpy(p["dens"].astype(np.float32)).cuda()
+    tr[0, 0, 5] = 0.6
+    with pytest.raises(av.AvionicError, match="trajectory"):
+        av.RadialOperator(p["W"], p["H"], p["C"], p["T"], tr, de, p["spf"], 3.0, 8.0, 1.5)
