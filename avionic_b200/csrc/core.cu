@@ -724,15 +724,15 @@ static avx_status autotune(avx_solver* s) {
   int dev = 0;
   AVX_CK(cudaGetDevice(&dev));
   const TuneKey key{dev, s->method, s->W, s->H, s->T};
-  {
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tune.find(key);
-    if (it != g_tune.end()) {
-      s->primal_tile = it->second.first;
-      s->dual_block = it->second.second;
-      s->tuned = true;
-      return AVX_OK;
-    }
+  // held while tuning, so that solvers of one shape on several threads (the
+  // batch engine's workers) all take the one choice
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(key);
+  if (it != g_tune.end()) {
+    s->primal_tile = it->second.first;
+    s->dual_block = it->second.second;
+    s->tuned = true;
+    return AVX_OK;
   }
   PDArgs a = make_pdargs(s);
   float best = 0.f;
@@ -758,7 +758,6 @@ static avx_status autotune(avx_solver* s) {
     }
   }
   s->tuned = true;
-  std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[key] = {s->primal_tile, s->dual_block};
   return AVX_OK;
 }
