@@ -1,8 +1,8 @@
 // Radial (non-Cartesian) operator: geometry and launchers (radial.cu).
 //
 // K_f x = sqrt(w_f) NUFFT_f(b1_c x_f) / sqrt(HW) with a tapered Kaiser-Bessel
-// gridding NUFFT on an oversampled grid (definition in oracle/radial.py and
-// DESIGN.md); K^H its exact adjoint.  Grid layout [frame][coil][Gy][Gx];
+// gridding NUFFT on an oversampled grid (definition in oracle/radial.py);
+// K^H its exact adjoint.  Grid layout [frame][coil][Gy][Gx];
 // samples [frame][coil][S].
 #pragma once
 

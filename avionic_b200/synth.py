@@ -1,22 +1,22 @@
 """Seeded synthetic Cartesian 2D+t problems (stand-ins for the reference's
 public cine / perfusion data, which are not available here).
 
-Shapes and value distributions follow the benchmark configurations:
+Shapes and value distributions follow the benchmark problems:
 
-* ``config0``: 128x128, 20 frames, 8 coils; three ellipses whose radii
+* ``tv_ellipses_128``: 128x128, 20 frames, 8 coils; three ellipses whose radii
   oscillate with period 20 frames, smooth random phase; Gaussian-decay coil
   maps from 8 centres on a circle of radius 0.8 FOV (sigma 0.4 FOV) times a
   linear phase; per-frame mask of the 8 central phase-encode lines plus random
   lines to acceleration 8; complex Gaussian noise at 1e-3 of max |k|.
-* ``config1``: 192x192, 30 frames, 16 coils; beating ring and blood-pool disc
+* ``cine_192``: 192x192, 30 frames, 16 coils; beating ring and blood-pool disc
   (radius factor 1 + 0.15 sin(2 pi t / 30)) over a static textured background
   of smoothed uniform noise; variable-density phase-encode lines (Gaussian
   line density, sigma 0.25 N) at acceleration 12, shifted per frame.
 * ``batched_specs`` / ``cine_instance_gpu``: 64 instances of uneven size
   (matrix uniform in {96, 128, 160, 192, 256, 320}, frames 8-48, coils 4-32,
-  acceleration 6-16), each generated as ``config1`` from its own seed, with
+  acceleration 6-16), each generated as ``cine_192`` from its own seed, with
   the k-space formed on the GPU (torch.fft) so that large instances are quick.
-* ``config2_gpu``: radial golden-angle acquisition of the ``config1`` phantom
+* ``radial_128_gpu``: radial golden-angle acquisition of the ``cine_192`` phantom
   at 128 x 128 (256 readout samples, 21 spokes per frame, 40 frames, 12
   coils); k-space by an exact float64 non-uniform DFT on the GPU, complex
   Gaussian noise at 2e-3 of max |k|, sqrt(w)-weighted as the CLI weights it.
@@ -126,7 +126,7 @@ def simulate(x, b1, mask, rng, noise_rel):
     return k * mask[:, None, :, :]
 
 
-def config0(seed=0, H=128, W=128, T=20, C=8):
+def tv_ellipses_128(seed=0, H=128, W=128, T=20, C=8):
     rng = np.random.default_rng(seed)
     x = phantom_ellipses(H, W, T, rng, period=20)
     b1 = coil_maps(H, W, C, rng)
@@ -135,7 +135,7 @@ def config0(seed=0, H=128, W=128, T=20, C=8):
     return dict(kdata=k.astype(np.complex64), mask=mask, b1=b1.astype(np.complex64), truth=x.astype(np.complex64))
 
 
-def config1(seed=1, H=192, W=192, T=30, C=16):
+def cine_192(seed=1, H=192, W=192, T=30, C=16):
     rng = np.random.default_rng(seed)
     x = phantom_cine(H, W, T, rng, period=30)
     b1 = coil_maps(H, W, C, rng)
@@ -183,7 +183,7 @@ def batched_specs(seed=3, n=64):
 
 
 def cine_instance_gpu(spec, device="cuda", noise_rel=1e-3):
-    """A ``config1``-style instance at spec's sizes: returns CUDA tensors
+    """A ``cine_192``-style instance at spec's sizes: returns CUDA tensors
     kdata (T,C,H,W) masked, mask (T,H,W), b1 (C,H,W) and x0 (T,H,W), the
     coil-combined zero-filled time average replicated over the frames."""
     import torch
@@ -222,7 +222,7 @@ def golden_angle_radial(n_ro, spokes_per_frame, frames, angle_deg=111.246117975)
 
 
 def radial_instance_gpu(spec, device="cuda", noise_rel=2e-3, kernel_width=3.0, sector_width=8.0, osf=1.5):
-    """A radial instance: the ``config1`` phantom at spec's image size, coil
+    """A radial instance: the ``cine_192`` phantom at spec's image size, coil
     maps as ``coil_maps``, golden-angle spokes; k-space = the library's radial
     operator applied to the phantom (sqrt(w)-weighted, as the solver expects)
     plus complex Gaussian noise.  Returns CUDA tensors kdata (T,C,S), traj,
@@ -285,7 +285,7 @@ def nudft_gpu(u, traj_f):
     return ((u @ ex) * ey).sum(-2)
 
 
-def config2_gpu(seed=2, H=128, W=128, T=40, C=12, n_fe=256, spokes=21, noise_rel=2e-3, device="cuda"):
+def radial_128_gpu(seed=2, H=128, W=128, T=40, C=12, n_fe=256, spokes=21, noise_rel=2e-3, device="cuda"):
     """The radial configuration: returns CUDA tensors kdata (T, C, S)
     sqrt(w)-weighted, traj (T, 2, S), dens (T, S) and the phantom."""
     import torch

@@ -39,7 +39,7 @@ sys.path.insert(0, ROOT)
 METRIC = "PD iters/s, recons/s & p99 latency vs plain FP32 at <=1e-4 rel L2 err"
 UNIT = "PD it/s"
 ITERS = 1000
-WORKLOAD = "config1 Cartesian ICTGV2 cine-like 192x192x30 frames x16 coils, R=12 line mask, 1000 PD iterations/recon"
+WORKLOAD = "Cartesian ICTGV2 cine-like 192x192, 30 frames, 16 coils, R=12 line mask, 1000 PD iterations/recon"
 
 
 def cfg_params(av):
@@ -179,7 +179,7 @@ def cpu_oracle_rate(prob, n_iter, workers):
 
 def make_problem(seed):
     from avionic_b200 import synth
-    prob = synth.config1(seed)
+    prob = synth.cine_192(seed)
     prob["u0"] = synth.time_average_u0(prob["kdata"], prob["mask"], prob["b1"])
     return prob
 
@@ -333,7 +333,7 @@ def run_radial(av, torch, iters=500, steps=3):
     sector width 8), the CLI's flow for radial data without coil maps."""
     import ctypes
     from avionic_b200 import synth
-    prob = synth.config2_gpu(2)
+    prob = synth.radial_128_gpu(2)
     k, traj, dens = prob["kdata"], prob["traj"], prob["dens"]
     T, C, S = k.shape
     H, W = prob["truth"].shape[1:]
@@ -478,7 +478,7 @@ def main():
     ap.add_argument("--dft", default="split", choices=["split", "fp32"],
                     help="arithmetic of the y-transforms: split-BF16x3 tensor cores or fp32 CUDA cores")
     ap.add_argument("--parts", default="headline,radial,batched,serving",
-                    help="comma list: headline (config-1 line), radial, batched, serving (added to the line at N=1)")
+                    help="comma list: headline (the 192x192x30 cine ICTGV2 line), radial, batched, serving (added to the line at N=1)")
     ap.add_argument("--batch-workers", type=int, default=8, help="concurrent reconstructions of the batched forms")
     ap.add_argument("--batch-size", type=int, default=64)
     ap.add_argument("--serve-requests", type=int, default=24,

@@ -216,10 +216,10 @@ def test_relative_stop(av, method):
     assert rel(x.cpu().numpy(), xo) < REL_IMG
 
 
-def test_config0_tv_full(av):
-    """Benchmark configuration 0 (128x128, 20 frames, 8 coils, 500 iterations)."""
+def test_tv_ellipses_128_full(av):
+    """The TV benchmark problem (128x128, 20 frames, 8 coils, 500 iterations)."""
     from avionic_b200 import synth
-    prob = synth.config0(0)
+    prob = synth.tv_ellipses_128(0)
     u0 = synth.time_average_u0(prob["kdata"], prob["mask"], prob["b1"])
     xo, _, _ = _oracle_run("TV", prob, 500, u0=u0)
     xg, _ = _gpu_run(av, "TV", prob, 500, u0=u0)
@@ -266,12 +266,12 @@ def test_reconstruct_host_reuses_state_correctly(av):
     av.lib.avx_reconstruct_host_release()
 
 
-def test_split_dft_matches_fp32_config1_shape(av):
+def test_split_dft_matches_fp32_cine_192_shape(av):
     """The split-BF16x3 tensor-core y-transform agrees with the fp32 CUDA-core
     one at the benchmark shape (192 x 192, 16 coils, 16 rows per frame)."""
     import torch
     from avionic_b200 import synth
-    prob = synth.config1(2, T=4)
+    prob = synth.cine_192(2, T=4)
     T, C, H, W = prob["kdata"].shape
     rng = np.random.default_rng(3)
     x = av.to_device(cplx(rng, (T, H, W)))
