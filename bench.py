@@ -73,7 +73,8 @@ def algorithmic_bytes(W, H, T, C, R):
         "coladj": 8 * S + 8 * C * W * H + 8 * N,
         # read K^H z, x (P), y (D); write x, xbar (2P)
         "primal": 8 * N * (1 + 3 * P + D),
-        # the whole iteration, the formula of the scope table: 8 [4PN + 2DN + 3CS] + 8 C W H + 4 S
+        # the whole iteration: fields read and written once, z and d at the
+        # sampled values, b1 once, the kept rows' mask: 8 [4PN + 2DN + 3CS] + 8 C W H + 4 R W
         "iteration": 8 * (4 * P * N + 2 * D * N + 3 * S) + 8 * C * W * H + 4 * R * W,
     }
 
