@@ -16,7 +16,9 @@
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (the host-side name of a __device__ variable is
 //    only a stand-in and must not be passed to a kernel); make that first
-//    call before any stream capture;
+//    call before any stream capture.  The address is kept for the life of
+//    the process: do not call this entry point after cudaDeviceReset on that
+//    device (the reset unloads the module that holds the array);
 //  * all calls share the array and it keeps the last call's contents; each
 //    call overwrites every slot it later reads, so nothing needs clearing,
 //    but calls that overlap on the GPU (different streams or threads) race.
@@ -71,6 +73,13 @@ double* g_noalloc_addr[64] = {nullptr};  // per device
 // sets the message avx_last_error() returns (core.cu)
 void avx_internal_set_error(const char* msg);
 
+static avx_status cuda_fail(const char* what, cudaError_t e) {
+  char msg[200];
+  std::snprintf(msg, sizeof(msg), "avx_tv_norm_noalloc: %s failed: %s", what, cudaGetErrorString(e));
+  avx_internal_set_error(msg);
+  return AVX_E_CUDA;
+}
+
 extern "C" avx_status avx_tv_norm_noalloc(const avx_cf32* d_u, unsigned W, unsigned H, unsigned T, float dx,
                                           float dy, float dt, double* out) {
   if (!d_u || !out || !W || !H || !T) {
@@ -86,14 +95,21 @@ extern "C" avx_status avx_tv_norm_noalloc(const avx_cf32* d_u, unsigned W, unsig
     return AVX_E_ARG;
   }
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return AVX_E_CUDA;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail("cudaGetDevice", e);
+  if (dev < 0 || dev >= 64) {
+    avx_internal_set_error("avx_tv_norm_noalloc: device ordinal beyond 63");
+    return AVX_E_ARG;
+  }
   double* scratch;
   {
     // set-up once per device, with that device current
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_addr[dev]) {
       void* p = nullptr;
-      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return AVX_E_CUDA;
+      e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess) return cuda_fail("cudaGetSymbolAddress", e);
+      if (!p) return cuda_fail("cudaGetSymbolAddress", cudaErrorInvalidSymbol);
       g_noalloc_addr[dev] = static_cast<double*>(p);
     }
     scratch = g_noalloc_addr[dev];
@@ -106,11 +122,14 @@ extern "C" avx_status avx_tv_norm_noalloc(const avx_cf32* d_u, unsigned W, unsig
   w.hy = (float)(1.0 / (2.0 * (double)dy));
   w.ht = (float)(1.0 / (2.0 * (double)dt));
   const int nblocks = (int)((n + AVX_NOALLOC_THREADS - 1) / AVX_NOALLOC_THREADS);
+  // an error left pending by an earlier, unrelated call is not this call's failure
+  (void)cudaGetLastError();
   tv_norm_partial_kernel<<<nblocks, AVX_NOALLOC_THREADS>>>(reinterpret_cast<const float2*>(d_u), (int)W, (int)H,
                                                           (int)T, w, scratch);
   tv_norm_final_kernel<<<1, AVX_NOALLOC_THREADS>>>(scratch, nblocks);
-  if (cudaGetLastError() != cudaSuccess) return AVX_E_CUDA;
-  if (cudaMemcpy(out, scratch + AVX_NOALLOC_MAX_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
-    return AVX_E_CUDA;
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail("kernel launch", e);
+  e = cudaMemcpy(out, scratch + AVX_NOALLOC_MAX_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail("cudaMemcpy of the result", e);
   return AVX_OK;
 }

@@ -306,3 +306,91 @@ def radial_128_gpu(seed=2, H=128, W=128, T=40, C=12, n_fe=256, spokes=21, noise_
     k *= torch.sqrt(dens_d.double())[:, None, :]
     return dict(kdata=k.to(torch.complex64).contiguous(), traj=traj_d, dens=dens_d, truth=x.to(torch.complex64),
                 n_fe=n_fe, spokes=spokes)
+
+
+# ---------------------------------------------------------------------------
+# problems with float64-oracle fixtures (numpy only, reproducible bit for bit)
+# ---------------------------------------------------------------------------
+
+# The cine benchmark's solver parameters: the reference's default configuration
+# file's [ictgv2] section, 1000 iterations, no gap evaluation.
+CINE_192_PARAMS = dict(maxIt=1000, stopPDGap=0.0, sigma=0.3333, tau=0.3333, sigmaTauRatio=1.0,
+                       timeSpaceWeight=4.0, timeSpaceWeight2=0.5, alpha=0.5, alpha0=1.41421356, alpha1=1.0,
+                       **{"lambda": 6.0})
+BATCHED_ITERS = 800
+TV_ELLIPSES_ITERS = 500
+RADIAL_ITERS = 500
+
+
+def tv_ellipses_128_problem(seed=0):
+    """``tv_ellipses_128`` with its initial image (the coil-combined
+    zero-filled time average)."""
+    prob = tv_ellipses_128(seed)
+    prob["u0"] = time_average_u0(prob["kdata"], prob["mask"], prob["b1"])
+    return prob
+
+
+def cine_192_problem(seed=1):
+    """``cine_192`` with the initial image the benchmark starts from (the
+    coil-combined zero-filled time average, replicated over the frames)."""
+    prob = cine_192(seed)
+    prob["u0"] = time_average_u0(prob["kdata"], prob["mask"], prob["b1"])
+    return prob
+
+
+def cine_instance(spec, noise_rel=1e-3):
+    """A batched instance generated on the host (numpy arrays: kdata
+    (T,C,H,W) masked, mask, b1, u0 (H,W)): the problems the float64 oracle
+    fixtures hold.  Same construction as ``cine_instance_gpu``; the noise
+    comes from the spec's numpy generator."""
+    H, W, T, C = spec["H"], spec["W"], spec["T"], spec["C"]
+    rng = np.random.default_rng(spec["seed"])
+    x = phantom_cine(H, W, T, rng, period=30)
+    b1 = coil_maps(H, W, C, rng)
+    mask = mask_variable_density(H, W, T, R=spec["R"], rng=rng)
+    k = simulate(x, b1, mask, rng, noise_rel).astype(np.complex64)
+    b1 = b1.astype(np.complex64)
+    return dict(kdata=k, mask=mask, b1=b1, u0=time_average_u0(k, mask, b1), truth=x.astype(np.complex64))
+
+
+def oracle_batched_indices(seed=3, n=64):
+    """Instances of the batched set with oracle fixtures: size ranks 0, 16,
+    32 and 48 of 64 (by W H T C, ties by index), one per quartile below the
+    largest."""
+    specs = batched_specs(seed, n)
+    order = sorted(range(n), key=lambda i: (specs[i]["W"] * specs[i]["H"] * specs[i]["T"] * specs[i]["C"], i))
+    return [order[r] for r in (0, n // 4, n // 2, 3 * n // 4)]
+
+
+def nudft(u, traj_f):
+    """Exact non-uniform DFT in float64 (numpy):
+    X[..., s] = sum_{y,x} u[..., y, x] exp(-2 pi i (kx_s px + ky_s py)),
+    p = index - floor(extent / 2); u (..., H, W), traj_f (2, S)."""
+    H, W = u.shape[-2:]
+    kx = traj_f[0].astype(np.float64)
+    ky = traj_f[1].astype(np.float64)
+    px = np.arange(W, dtype=np.float64) - W // 2
+    py = np.arange(H, dtype=np.float64) - H // 2
+    ex = np.exp(-2j * np.pi * np.outer(px, kx))   # (W, S)
+    ey = np.exp(-2j * np.pi * np.outer(py, ky))   # (H, S)
+    return ((u @ ex) * ey).sum(-2)
+
+
+def radial_128(seed=2, H=128, W=128, T=40, C=12, n_fe=256, spokes=21, noise_rel=2e-3):
+    """The radial configuration generated on the host (numpy): kdata (T, C, S)
+    complex64, sqrt(w)-weighted as the CLI weights it (main.cpp:546-570),
+    traj (T, 2, S) and dens (T, S) float32, the phantom (T, H, W); k-space by
+    the exact float64 NUDFT, complex Gaussian noise at noise_rel of max |k|."""
+    rng = np.random.default_rng(seed)
+    x = phantom_cine(H, W, T, rng, period=30)
+    b1 = coil_maps(H, W, C, rng)
+    traj, dens = golden_angle_radial(n_fe, spokes, T)
+    S = traj.shape[2]
+    k = np.empty((T, C, S), dtype=np.complex128)
+    for t in range(T):
+        k[t] = nudft(b1 * x[t], traj[t]) / np.sqrt(W * H)
+    sd = noise_rel * np.max(np.abs(k))
+    k += (sd / np.sqrt(2.0)) * (rng.standard_normal(k.shape) + 1j * rng.standard_normal(k.shape))
+    k *= np.sqrt(dens.astype(np.float64))[:, None, :]
+    return dict(kdata=k.astype(np.complex64), traj=traj, dens=dens, truth=x.astype(np.complex64), n_fe=n_fe,
+                spokes=spokes, b1_true=b1.astype(np.complex64))

@@ -290,9 +290,11 @@ avx_status avx_ictgv2_norm(const avx_cf32* d_x1, const avx_cf32* const* d_x2, co
  * they need it: the partial sums live in a fixed 64 KiB __device__ array that
  * every GPU loading the library holds until exit.  W*H*T must not exceed
  * 2,097,152 pixels (AVX_E_ARG otherwise).  The first call on a device resolves
- * the array's address and should precede any stream capture; calls that
- * overlap on the GPU race on the shared array.  Runs on the legacy default
- * stream and returns after the result reached *out. */
+ * the array's address and should precede any stream capture; the address is
+ * kept for the process, so the entry point must not be used on a device after
+ * cudaDeviceReset.  Calls that overlap on the GPU race on the shared array.
+ * Runs on the legacy default stream and returns after the result reached
+ * *out. */
 avx_status avx_tv_norm_noalloc(const avx_cf32* d_u, unsigned W, unsigned H, unsigned T, float dx, float dy,
                                float dt, double* out);
 

@@ -133,7 +133,7 @@ def tv_gap(p, op, x, y, z, d, b1, w):
     return abs(tv_gstar(p, op, x, y, z, d, b1, w) + st.tv_norm(x, *w))
 
 
-def tv(data, x, b1, op, p, trace=None):
+def tv(data, x, b1, op, p, trace=None, k0=0):
     """``TV::IterativeReconstruction`` (tv.cpp:99-200).  ``x`` is the initial
     image (T,H,W); returns the final image.  ``trace`` (a dict) collects the
     gap history ("PDGap") and the (sigma, tau) sequence."""
@@ -146,7 +146,7 @@ def tv(data, x, b1, op, p, trace=None):
     y = [np.zeros_like(x) for _ in range(3)]
     z = np.zeros_like(data, dtype=np.complex128)
     gaps, steps = [], []
-    k = 0
+    k = k0
     while k < p.maxIt:
         g = st.gradient(ext, *w)
         y = [y[i] + p.sigma * g[i] for i in range(3)]
@@ -205,7 +205,7 @@ def tgv2_gap(p, op, x1, x2, y1, y2, z, d, b1, w):
                + st.tgv2_norm(x1, x2, p.alpha0, p.alpha1, *w))
 
 
-def tgv2(data, x1, b1, op, p, trace=None):
+def tgv2(data, x1, b1, op, p, trace=None, k0=0):
     """``TGV2::IterativeReconstruction`` (tgv2.cpp:180-338)."""
     p = p.copy()
     ds, dt = st.time_space_weights(p.timeSpaceWeight)
@@ -219,7 +219,7 @@ def tgv2(data, x1, b1, op, p, trace=None):
     y2 = [np.zeros_like(x1) for _ in range(6)]
     z = np.zeros_like(data, dtype=np.complex128)
     gaps, steps = [], []
-    k = 0
+    k = k0
     while k < p.maxIt:
         g = st.gradient(ext1, *w)
         y1 = [y1[i] + p.sigma * (g[i] - ext2[i]) for i in range(3)]
@@ -306,7 +306,7 @@ def ictgv2_gap(p, op, x1, x2, x3, x4, y1, y2, y3, y4, z, d, b1, w1, w2):
     return abs(g + n)
 
 
-def ictgv2(data, x1, b1, op, p, trace=None):
+def ictgv2(data, x1, b1, op, p, trace=None, k0=0):
     """``ICTGV2::IterativeReconstruction`` (ictgv2.cpp:294-492)."""
     p = p.copy()
     w1, w2 = ictgv2_weights(p)
@@ -322,7 +322,7 @@ def ictgv2(data, x1, b1, op, p, trace=None):
     fid = [ictgv2_data_fidelity(p, op, x1, data, b1)]
     nrm = [st.ictgv2_norm(x1, x2, x3, x4, p.alpha0, p.alpha1, p.alpha, w1, w2)]
     gaps, steps = [], []
-    k = 0
+    k = k0
     while k < p.maxIt:
         g = st.gradient(ext1 - ext3, *w1)
         y1 = [y1[i] + p.sigma * (g[i] - ext2[i]) for i in range(3)]
@@ -394,7 +394,7 @@ def tvtemp_gap(p, op, x, y, z, d, b1):
     return abs(g1 + g2 + g3 + st.tv_norm(x, 1.0, 1.0, p.dt))
 
 
-def tvtemp(data, x, b1, op, p, trace=None):
+def tvtemp(data, x, b1, op, p, trace=None, k0=0):
     """``TVTEMP::IterativeReconstruction`` (tv_temp.cpp:95-182): TV along t
     only, no time-space weighting."""
     p = p.copy()
@@ -404,7 +404,7 @@ def tvtemp(data, x, b1, op, p, trace=None):
     y = [np.zeros_like(x)]
     z = np.zeros_like(data, dtype=np.complex128)
     gaps, steps = [], []
-    k = 0
+    k = k0
     while k < p.maxIt:
         g = st.gradient_temp(ext, p.dt)
         y = [y[0] + p.sigma * g[0]]
@@ -455,7 +455,7 @@ def ictv_gap(p, op, x1, x3, y1, y3, z, d, b1, w1, w2):
     return abs(g1 + g2 + g3 + g5 + st.ictv_norm(x1, x3, p.alpha1, p.alpha, w1, w2))
 
 
-def ictv(data, x1, b1, op, p, trace=None):
+def ictv(data, x1, b1, op, p, trace=None, k0=0):
     """``ICTV::IterativeReconstruction`` (ictv.cpp:202-370): infimal
     convolution of two TV functionals with their own time-space weights."""
     p = p.copy()
@@ -469,7 +469,7 @@ def ictv(data, x1, b1, op, p, trace=None):
     z = np.zeros_like(data, dtype=np.complex128)
     m = min(p.alpha, 1.0 - p.alpha)
     gaps, nrm, fid, steps = [], [], [], []
-    k = 0
+    k = k0
     while k < p.maxIt:
         g = st.gradient(ext1 - ext3, *w1)
         y1 = [y1[i] + p.sigma * g[i] for i in range(3)]
@@ -502,6 +502,9 @@ def ictv(data, x1, b1, op, p, trace=None):
     return x1
 
 
-def run(method, data, x0, b1, op, p, trace=None):
+def run(method, data, x0, b1, op, p, trace=None, k0=0):
+    """Runs ``method``'s loop with the iteration counter starting at k0 (the
+    step rule and the gap cadence read the counter; k0 > 0 runs iterations
+    k0 .. maxIt-1, which is how the CPU timings skip the step-rule start)."""
     return {"TV": tv, "TVTEMP": tvtemp, "TGV2": tgv2, "ICTV": ictv, "ICTGV2": ictgv2}[method.upper()](
-        data, x0, b1, op, p, trace)
+        data, x0, b1, op, p, trace, k0)
