@@ -47,3 +47,22 @@ def at(arr, pos):
     """arr (T,H,W) at reference position [x, y, t]."""
     x, y, t = pos
     return arr[t, y, x]
+
+
+def radial_fixture(k):
+    """The radial operator's test fixture (CUDA/test/noncartesian_operator.cc:17-101):
+    trajectory (T, 2, S) with sample cnt of spoke sp in frame f at
+    kx = cnt / nFE - 0.5, ky = (f spf + sp) / nSpokes - 0.5 (horizontal spokes),
+    density 1, and coil maps of constant value 1, 2, 3."""
+    W, H, C, T = k["width"], k["height"], k["coils"], k["frames"]
+    nfe, spf, nsp = k["nFE"], k["spokesPerFrame"], k["nSpokes"]
+    S = nfe * spf
+    traj = np.zeros((T, 2, S), dtype=np.float32)
+    for f in range(T):
+        for sp in range(spf):
+            for cnt in range(nfe):
+                traj[f, 0, sp * nfe + cnt] = np.float32(cnt / nfe) - np.float32(0.5)
+                traj[f, 1, sp * nfe + cnt] = np.float32((f * spf + sp) / nsp) - np.float32(0.5)
+    dens = np.ones((T, S), dtype=np.float32)
+    b1 = np.stack([np.full((H, W), v, dtype=np.complex128) for v in k["b1_per_coil"]])
+    return traj, dens, b1

@@ -245,3 +245,42 @@ def test_iteration_goldens(av, kats, method, dft):
     for pos, want in k["values"]:
         assert abs(abs(ki.at(xr, pos)) - want) < _tol(dft, want), (pos, abs(ki.at(xr, pos)), want)
     assert s.stats().iterations == k["maxIt"]
+
+
+# ---------------------------------------------------------------------------
+# radial operator (CUDA/test/noncartesian_operator.cc)
+# ---------------------------------------------------------------------------
+
+def _radial_op(av, kats, osf=2.0):
+    f = kats["radial_fixture"]
+    traj, dens, b1 = ki.radial_fixture(f)
+    op = av.RadialOperator(f["width"], f["height"], f["coils"], f["frames"], dev(traj), dev(dens),
+                           f["spokesPerFrame"], 3.0, 8.0, osf)
+    return op, b1
+
+
+def test_radial_adapt_lambda_kat(av, kats):
+    """NoncartesianOperator::AdaptLambda on the reference fixture = 6.636
+    (noncartesian_operator.cc:203-211)."""
+    op, _ = _radial_op(av, kats)
+    k = kats["radial_adapt_lambda"]
+    assert abs(op.adapt_lambda(k["k"], k["d"]) - k["value"]) < EPS
+
+
+@pytest.mark.parametrize("osf", [2.0, 1.5])
+def test_radial_adjointness_kat(av, kats, osf):
+    """The reference's adjointness test on its fixture (noncartesian_operator.cc:161-201):
+    <K^H y, x> = <y, K x> within 1e-3 absolute in both parts, here also
+    within 1e-5 relative."""
+    f, k = kats["radial_fixture"], kats["radial_adjointness"]
+    op, b1 = _radial_op(av, kats, osf)
+    W, H, C, T = f["width"], f["height"], f["coils"], f["frames"]
+    rng = np.random.default_rng(161)
+    x = (rng.random((T, C, op.S)) + 1j * rng.random((T, C, op.S))).astype(np.complex64)
+    y = (rng.random((T, H, W)) + 1j * rng.random((T, H, W))).astype(np.complex64)
+    b1d = dev(b1.astype(np.complex64))
+    kx = host(op.forward(dev(x), b1d)).astype(complex)
+    khy = host(op.backward(dev(y), b1d)).astype(complex)
+    d = np.vdot(y.astype(complex), kx) - np.vdot(khy, x.astype(complex))
+    assert abs(d.real) < k["tolerance"] and abs(d.imag) < k["tolerance"]
+    assert abs(d) < 1e-5 * abs(np.vdot(y.astype(complex), kx))

@@ -484,3 +484,39 @@ def test_coil_construction_loop_kat(kats):
         assert abs(b1[c, y, x].real - want) < EPS
     for (x, y, c), want in k["loop_u_real"]:
         assert abs(u[c, y, x].real - want) < EPS
+
+
+# ---------------------------------------------------------------------------
+# radial operator (CUDA/test/noncartesian_operator.cc)
+# ---------------------------------------------------------------------------
+
+def test_radial_adapt_lambda_kat(kats):
+    """NoncartesianOperator::AdaptLambda (noncartesian_operator.cpp:88-95) on the
+    reference fixture: W / (spokesPerFrame pi / 2) k + d = 6.636."""
+    from oracle import radial as rd
+    from tests import kat_inputs as ki
+    f, k = kats["radial_fixture"], kats["radial_adapt_lambda"]
+    traj, dens, _ = ki.radial_fixture(f)
+    op = rd.RadialOperator(f["width"], f["height"], f["coils"], f["frames"], traj.astype(float), dens.astype(float),
+                           3.0, 8.0, 2.0)
+    assert abs(op.adapt_lambda(k["k"], k["d"], f["spokesPerFrame"]) - k["value"]) < 1e-3
+
+
+def test_radial_adjointness_kat(kats):
+    """The reference's adjointness test (noncartesian_operator.cc:161-201) on its
+    fixture with the oracle's gridding (kernel width 3, sector width 8, osf 2,
+    the reference's defaults)."""
+    from oracle import radial as rd
+    from tests import kat_inputs as ki
+    f, k = kats["radial_fixture"], kats["radial_adjointness"]
+    traj, dens, b1 = ki.radial_fixture(f)
+    W, H, C, T = f["width"], f["height"], f["coils"], f["frames"]
+    op = rd.RadialOperator(W, H, C, T, traj.astype(float), dens.astype(float), 3.0, 8.0, 2.0)
+    rng = np.random.default_rng(161)
+    x = rng.random((T, C, op.S)) + 1j * rng.random((T, C, op.S))   # k-space
+    y = rng.random((T, H, W)) + 1j * rng.random((T, H, W))          # image
+    kx = op.forward(x.copy(), b1)    # ForwardOperation: k-space -> image
+    khy = op.backward(y, b1)         # BackwardOperation: image -> k-space
+    d = np.vdot(y, kx) - np.vdot(khy, x)
+    assert abs(d.real) < k["tolerance"] and abs(d.imag) < k["tolerance"]
+    assert abs(d) < 1e-12 * abs(np.vdot(y, kx))
