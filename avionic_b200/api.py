@@ -449,8 +449,11 @@ def query_workspace(request):
 
 
 class BatchEngine:
-    """Worker threads with their own streams and device workspaces; requests
-    start in submission order once their workspace fits the HBM budget."""
+    """Continuous batching at iteration granularity (avx_batch_*): queued
+    requests are admitted as their workspace fits the HBM budget, set up on
+    streams of their own, advanced together (at most ``workers`` at a time)
+    20 iterations at a time, and retired at their stop test or last
+    iteration; each result equals the request run alone."""
 
     def __init__(self, device=0, hbm_budget=150 << 30, workers=8):
         self.handle = ctypes.c_void_p()

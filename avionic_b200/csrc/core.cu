@@ -53,64 +53,45 @@ avx_status fail(avx_status s, const std::string& msg) {
                   std::string(#call) + ": " + cudaGetErrorString(e_));                       \
   } while (0)
 
-// Device memory of a batch worker thread: chunks obtained with cudaMalloc and
-// kept until the worker ends, handed out by a bump pointer that restarts for
-// every request.  (cudaFree synchronises the whole device, which would
-// serialise the reconstructions that other workers run concurrently.)
-struct DevArena {
-  struct Chunk {
-    char* p;
-    size_t size;
-  };
-  std::vector<Chunk> chunks;
-  size_t ci = 0, off = 0;
-  void reset() { ci = off = 0; }
-  void* take(size_t bytes) {
-    bytes = (bytes + 255) & ~(size_t)255;
-    for (; ci < chunks.size(); ++ci, off = 0)
-      if (off + bytes <= chunks[ci].size) {
-        void* r = chunks[ci].p + off;
-        off += bytes;
-        return r;
-      }
-    const size_t sz = std::max(bytes, (size_t)256 << 20);
-    char* p = nullptr;
-    if (cudaMalloc(&p, sz) != cudaSuccess) return nullptr;
-    chunks.push_back({p, sz});
-    ci = chunks.size() - 1;
-    off = bytes;
-    return p;
-  }
-  ~DevArena() {
-    for (const Chunk& c : chunks) cudaFree(c.p);
-  }
-};
-thread_local DevArena* t_arena = nullptr;  // set by a batch worker for its requests
+// Set by the batch engine while it builds a request's operator and solver:
+// their buffers come from the device's stream-ordered pool on that stream and
+// go back to it with cudaFreeAsync, so that retiring a request never waits
+// for the other requests' work (cudaFree would synchronise the device).
+thread_local cudaStream_t t_pool_stream = nullptr;
 
 template <class T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
-  bool from_arena = false;
+  cudaStream_t pool_stream = nullptr;  // non-null: allocated from the stream-ordered pool
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p && !from_arena) cudaFree(p);
+    if (p && pool_stream)
+      cudaFreeAsync(p, pool_stream);
+    else if (p)
+      cudaFree(p);
     p = nullptr;
     n = 0;
-    from_arena = false;
+    pool_stream = nullptr;
   }
   cudaError_t alloc(size_t count) {
     if (count <= n && p) return cudaSuccess;
     release();
     const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
-    if (t_arena) {
-      p = static_cast<T*>(t_arena->take(bytes));
-      if (!p) return cudaErrorMemoryAllocation;
+    if (t_pool_stream) {
+      cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&p), bytes, t_pool_stream);
+      // the set-up code fills some buffers with synchronous copies on the
+      // legacy stream: make the allocation visible to every stream first
+      if (e == cudaSuccess) e = cudaStreamSynchronize(t_pool_stream);
+      if (e != cudaSuccess) {
+        p = nullptr;
+        return e;
+      }
       n = count;
-      from_arena = true;
+      pool_stream = t_pool_stream;
       return cudaSuccess;
     }
     cudaError_t e = cudaMalloc(&p, bytes);
@@ -586,6 +567,7 @@ struct avx_solver {
   int primal_tile = 0, dual_block = 0;
   cudaStream_t user_stream = 0;
   cudaStream_t stream = 0;
+  bool own_stream = false;  // stream created by solver_alloc (else lent by the batch engine)
   // device state
   DevBuf<float2> prim, ext, dual, escr, z, d;
   DevBuf<float2> b1t;  // coil maps in column-tile order (tensor-core adjoint)
@@ -607,7 +589,7 @@ struct avx_solver {
   ~avx_solver() {
     drop_graphs();
     for (auto e : events) cudaEventDestroy(e);
-    if (stream) cudaStreamDestroy(stream);
+    if (stream && own_stream) cudaStreamDestroy(stream);
   }
   void drop_graphs() {
     for (auto& g : gexec)
@@ -639,7 +621,10 @@ static avx_status solver_alloc(avx_solver* s) {
   AVX_CK(s->pk.alloc((size_t)3 * std::max(nk, 1)));
   s->cap = (int)s->p.maxIt + 2;
   AVX_CK(s->hist.alloc((size_t)3 * (s->cap + 1)));
-  if (!s->stream) AVX_CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  if (!s->stream) {
+    AVX_CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->own_stream = true;
+  }
   return AVX_OK;
 }
 
@@ -940,7 +925,12 @@ static avx_status prepare_run(avx_solver* s, const float2* data, const float2* x
   return AVX_OK;
 }
 
-static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const float2* b1) {
+// Set-up of a run (tv.cpp:103-135 and twins): time-space weights, zeroed
+// duals and k-space, x and xbar from the initial image, the compact data,
+// launch-shape tuning, the tile-ordered coil maps and, with the debug export
+// of ICTGV2, the gap of the initial state.  Ends with the solver's stream
+// ordered after the caller's.
+static avx_status solver_begin(avx_solver* s, const float2* data, float2* x, const float2* b1) {
   avx_status r = solver_alloc(s);
   if (r != AVX_OK) return r;
   // the reference overwrites dx, dy, dt (and dx2..dt2) from the weights (tv.cpp:103-104)
@@ -955,13 +945,14 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
     if (!time_space_weights(s->p.timeSpaceWeight2, &ds, &dt)) return fail(AVX_E_ARG, "ComputeTimeSpaceWeights: invalid ratio");
     s->p.dx2 = (float)ds; s->p.dy2 = (float)ds; s->p.dt2 = (float)dt;
   }
-  // order the internal stream after the caller's stream
-  cudaEvent_t ev0, ev1, evin;
-  AVX_CK(cudaEventCreate(&ev0));
-  AVX_CK(cudaEventCreate(&ev1));
-  AVX_CK(cudaEventCreateWithFlags(&evin, cudaEventDisableTiming));
-  AVX_CK(cudaEventRecord(evin, s->user_stream));
-  AVX_CK(cudaStreamWaitEvent(s->stream, evin, 0));
+  if (s->stream != s->user_stream) {
+    // order the internal stream after the caller's stream
+    cudaEvent_t evin;
+    AVX_CK(cudaEventCreateWithFlags(&evin, cudaEventDisableTiming));
+    AVX_CK(cudaEventRecord(evin, s->user_stream));
+    AVX_CK(cudaStreamWaitEvent(s->stream, evin, 0));
+    cudaEventDestroy(evin);
+  }
   r = prepare_run(s, data, x);
   if (r != AVX_OK) return r;
   if (s->autotune && !s->tuned) {
@@ -998,6 +989,60 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
     s->drop_graphs();
     s->graph_key = key;
   }
+  return AVX_OK;
+}
+
+// The CUDA graph of iteration shape `shape` (bit 0: step rule, bit 1: gap),
+// captured on the solver's stream at first use.
+static avx_status solver_graph(avx_solver* s, int shape, const float2* b1) {
+  if (s->gexec[shape]) return AVX_OK;
+  cudaGraph_t g;
+  AVX_CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  enqueue_shape(s, shape, b1);
+  AVX_CK(cudaStreamEndCapture(s->stream, &g));
+  const cudaError_t e = cudaGraphInstantiate(&s->gexec[shape], g, 0);
+  cudaGraphDestroy(g);
+  AVX_CK(e);
+  return AVX_OK;
+}
+
+static int iter_shape(const avx_solver* s, unsigned k) { return (step_due(k) ? 1 : 0) | (gap_due(s, k) ? 2 : 0); }
+
+// Enqueues iterations [k0, k1) from the graphs of their shapes (no host
+// synchronisation); *launches receives the kernels they hold.
+static avx_status solver_enqueue(avx_solver* s, const float2* b1, unsigned k0, unsigned k1, unsigned* launches) {
+  for (unsigned k = k0; k < k1; ++k) {
+    const int shape = iter_shape(s, k);
+    avx_status r = solver_graph(s, shape, b1);
+    if (r != AVX_OK) return r;
+    AVX_CK(cudaGraphLaunch(s->gexec[shape], s->stream));
+    if (launches) *launches += shape_launches(s->op->kind, shape);
+  }
+  return AVX_OK;
+}
+
+// Statistics of a finished run from the device state it left in s->last.
+static avx_status solver_finish_stats(avx_solver* s, float ms, unsigned launches) {
+  s->p.sigma = (float)s->last.sigma;
+  s->p.tau = (float)s->last.tau;
+  s->stats.iterations = (unsigned)s->last.iters;
+  s->stats.sigma = (float)s->last.sigma;
+  s->stats.tau = (float)s->last.tau;
+  s->stats.gap_count = (unsigned)s->last.ngap;
+  s->stats.last_gap = s->last.gap;
+  s->stats.stopped_by_gap = s->last.stop;
+  s->stats.elapsed_ms = ms;
+  s->stats.kernel_launches = launches;
+  if (s->last.err) return fail(AVX_E_NUMERIC, "device-side check failed");
+  return AVX_OK;
+}
+
+static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const float2* b1) {
+  avx_status r = solver_begin(s, data, x, b1);
+  if (r != AVX_OK) return r;
+  cudaEvent_t ev0, ev1;
+  AVX_CK(cudaEventCreate(&ev0));
+  AVX_CK(cudaEventCreate(&ev1));
   constexpr size_t NEV = AVX_NSTAGE + 1;  // events per timed iteration
   if (s->timing && s->events.size() < NEV * s->p.maxIt) {
     const size_t need = NEV * s->p.maxIt;
@@ -1011,22 +1056,15 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
   AVX_CK(cudaEventRecord(ev0, s->stream));
   unsigned k = 0;
   for (; k < s->p.maxIt; ++k) {
-    const int shape = (step_due(k) ? 1 : 0) | (gap_due(s, k) ? 2 : 0);
-    launches += shape_launches(s->op->kind, shape);
+    const int shape = iter_shape(s, k);
     if (s->timing) {
+      launches += shape_launches(s->op->kind, shape);
       enqueue_shape(s, shape, b1, &s->events[NEV * k]);
       AVX_CK(cudaGetLastError());
       continue;
     }
-    if (!s->gexec[shape]) {
-      cudaGraph_t g;
-      AVX_CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-      enqueue_shape(s, shape, b1);
-      AVX_CK(cudaStreamEndCapture(s->stream, &g));
-      AVX_CK(cudaGraphInstantiate(&s->gexec[shape], g, 0));
-      cudaGraphDestroy(g);
-    }
-    AVX_CK(cudaGraphLaunch(s->gexec[shape], s->stream));
+    r = solver_enqueue(s, b1, k, k + 1, &launches);
+    if (r != AVX_OK) return r;
     if (stop_active(s) && (shape & 2) && (k % 100 == 0)) {
       int stop = 0;
       AVX_CK(cudaMemcpyAsync(&stop, &s->st.p->stop, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
@@ -1059,19 +1097,7 @@ static avx_status solver_run(avx_solver* s, const float2* data, float2* x, const
   }
   cudaEventDestroy(ev0);
   cudaEventDestroy(ev1);
-  cudaEventDestroy(evin);
-  s->p.sigma = (float)s->last.sigma;
-  s->p.tau = (float)s->last.tau;
-  s->stats.iterations = (unsigned)s->last.iters;
-  s->stats.sigma = (float)s->last.sigma;
-  s->stats.tau = (float)s->last.tau;
-  s->stats.gap_count = (unsigned)s->last.ngap;
-  s->stats.last_gap = s->last.gap;
-  s->stats.stopped_by_gap = s->last.stop;
-  s->stats.elapsed_ms = ms;
-  s->stats.kernel_launches = launches;
-  if (s->last.err) return fail(AVX_E_NUMERIC, "device-side check failed");
-  return AVX_OK;
+  return solver_finish_stats(s, ms, launches);
 }
 
 // ===========================================================================
@@ -2175,42 +2201,34 @@ void avx_reconstruct_host_release(void) {
 }  // extern "C"
 
 // ===========================================================================
-// Batched and served reconstructions: worker threads with their own streams
-// and device arenas, FIFO admission against an HBM budget.
+// Batched and served reconstructions: continuous batching at iteration
+// granularity.  Set-up threads admit queued requests against the HBM budget
+// and build each one's operator, solver, device state and iteration graphs on
+// a stream of its own (memory from the device's stream-ordered pool); one
+// scheduler thread advances every admitted request by slices of 20
+// iterations (the gap cadence), keeps two slices in flight per request,
+// reads each request's device state after every slice without blocking, and
+// retires a request at its stop test or its last iteration, freeing its
+// budget for the next admission.
 // ===========================================================================
 
 namespace {
 
-size_t request_workspace(const avx_request& r, avx_status* st) {
-  *st = AVX_OK;
+constexpr unsigned kSlice = 20;     // iterations per slice (the stop test's gap cadence)
+constexpr int kSetupThreads = 4;    // request set-up threads per engine
+constexpr double kStarveMs = 2000;  // queue head waits at most this long before it blocks later admissions
+
+// Device bytes of a request.  R < 0: no mask row count known yet, so the
+// Cartesian k-space is counted at every row (an upper bound).
+size_t request_workspace(const avx_request& r, long long R_known, int max_rows_known) {
   const size_t W = r.width, H = r.height, C = r.coils, T = r.frames, N = W * H * T;
   const size_t P = (size_t)method_P(r.method), D = (size_t)method_D(r.method);
   const size_t c8 = sizeof(float2);
   size_t b = 0;
   size_t kspace = 0;  // values of z (and of d)
   if (r.op_kind == 0) {
-    size_t R = H * T, max_rows = H;
-    if (r.d_mask) {
-      std::vector<float> m(N);
-      if (cudaMemcpy(m.data(), r.d_mask, N * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
-        *st = fail(AVX_E_CUDA, "cannot read the request's mask");
-        return 0;
-      }
-      R = max_rows = 0;
-      for (size_t t = 0; t < T; ++t) {
-        size_t rows = 0;
-        for (size_t y = 0; y < H; ++y) {
-          const float* row = m.data() + (t * H + y) * W;
-          for (size_t x = 0; x < W; ++x)
-            if (row[x] != 0.f) {
-              ++rows;
-              break;
-            }
-        }
-        R += rows;
-        max_rows = std::max(max_rows, rows);
-      }
-    }
+    const size_t R = R_known >= 0 ? (size_t)R_known : H * T;
+    const size_t max_rows = R_known >= 0 ? (size_t)max_rows_known : H;
     const size_t Rk = std::max<size_t>(R, 1);
     kspace = C * Rk * W;
     b += R * 4 + (T + 1) * 4 + R * W * 4 + (W + H) * c8 + kspace * c8 + N * c8 + (r.d_mask ? N * 4 : 0);
@@ -2226,44 +2244,79 @@ size_t request_workspace(const avx_request& r, avx_status* st) {
     const size_t sectors = T * ((Gx + isw - 1) / isw) * ((Gy + isw - 1) / isw) + 1;
     kspace = C * T * S;
     b += T * S * (2 * 4 + 4 + 4) + (W + H) * 4 + sectors * 4 + (Gx + Gy) * c8 + T * C * Gx * Gy * c8 + N * c8;
+    b += T * S * (8 + 2 * 8 * 4);  // window starts and Kaiser-Bessel weights
   }
   // solver: primal, extragradient and step scratch (3P), duals (D), z and d, reductions, history
   b += (3 * P + D) * N * c8 + 2 * kspace * c8;
   b += 8 * (size_t)std::max(AVX_RED_BLOCKS, avx::gap_img_blocks((int)W, (int)H, (int)T)) * 8;
   b += 3 * (std::max(C * T, (kspace + 255) / 256) + 1) * 8;
   b += 3 * ((size_t)r.params.maxIt + 3) * 8 + 4096;
-  return b + b / 20 + ((size_t)16 << 20);  // arena alignment and chunk slack
+  return b + b / 20 + ((size_t)4 << 20);  // pool granularity and slack
 }
 
 double ms_since(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
-avx_completion run_request(const avx_request& r, cudaStream_t stream) {
-  avx_completion c;
-  memset(&c, 0, sizeof(c));
-  c.tag = r.tag;
+// One admitted request.
+struct Job {
+  avx_request r{};
+  size_t ws = 0;  // bytes held against the budget
+  std::chrono::steady_clock::time_point t_submit, t_start;
+  int slot = -1;  // stream and pinned state slots
   avx_operator* op = nullptr;
   avx_solver* s = nullptr;
+  cudaStream_t stream = nullptr;
+  unsigned k = 0;          // iterations enqueued
+  unsigned launches = 0;   // kernels enqueued
+  int inflight = 0;        // slices in flight (0..2)
+  int head = 0;            // oldest slice in flight: index into ev / hs
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  DevState* hs[2] = {nullptr, nullptr};  // pinned copies of the device state after each slice
+  bool stopped = false;
+  avx_completion c{};
+};
+
+// Operator, solver, device state and iteration graphs of a request, built on
+// the job's stream (pool memory).  Returns the status of the set-up.
+avx_status job_setup(Job* j) {
+  const avx_request& r = j->r;
   avx_status e;
+  t_pool_stream = j->stream;
   if (r.op_kind == 0) {
-    e = avx_cartesian_operator_create(r.width, r.height, r.coils, r.frames, r.d_mask, r.centered, &op);
-    if (e == AVX_OK && avx_operator_set_dft_mode(op, r.dft_mode) != AVX_OK) avx_operator_set_dft_mode(op, AVX_DFT_FP32);
-    if (e == AVX_OK) avx_operator_get_dft_mode(op, &c.dft_mode);
+    e = avx_cartesian_operator_create(r.width, r.height, r.coils, r.frames, r.d_mask, r.centered, &j->op);
+    if (e == AVX_OK && avx_operator_set_dft_mode(j->op, r.dft_mode) != AVX_OK) avx_operator_set_dft_mode(j->op, AVX_DFT_FP32);
+    if (e == AVX_OK) avx_operator_get_dft_mode(j->op, &j->c.dft_mode);
   } else {
     e = avx_radial_operator_create(r.width, r.height, r.coils, r.frames, r.spokes_per_frame * r.frames, r.n_fe,
                                    r.spokes_per_frame, r.d_traj, r.d_dens, r.kernel_width, r.sector_width, r.osf,
-                                   &op);
+                                   &j->op);
   }
-  if (e == AVX_OK) e = avx_solver_create(r.method, r.width, r.height, r.coils, r.frames, &r.params, op, &s);
-  if (e == AVX_OK) e = avx_solver_set_stream(s, stream);
-  if (e == AVX_OK && r.stop_gap_rel > 0.f) e = avx_solver_set_relative_stop(s, r.stop_gap_rel);
-  if (e == AVX_OK) e = avx_solver_run(s, r.d_data, r.d_x, r.d_b1);
-  if (e == AVX_OK) avx_solver_get_stats(s, &c.stats);
-  c.status = (int)e;
-  if (s) avx_solver_destroy(s);
-  if (op) avx_operator_destroy(op);
-  return c;
+  if (e == AVX_OK) e = avx_solver_create(r.method, r.width, r.height, r.coils, r.frames, &r.params, j->op, &j->s);
+  if (e == AVX_OK) {
+    j->s->stream = j->stream;  // lent: the solver does not own it
+    j->s->user_stream = j->stream;
+    if (r.stop_gap_rel > 0.f) e = avx_solver_set_relative_stop(j->s, r.stop_gap_rel);
+  }
+  if (e == AVX_OK)
+    e = solver_begin(j->s, reinterpret_cast<const float2*>(r.d_data), reinterpret_cast<float2*>(r.d_x),
+                     reinterpret_cast<const float2*>(r.d_b1));
+  // the graphs of every iteration shape the run takes
+  for (unsigned k = 0; e == AVX_OK && k < j->s->p.maxIt; ++k) e = solver_graph(j->s, iter_shape(j->s, k),
+                                                                                reinterpret_cast<const float2*>(r.d_b1));
+  if (e == AVX_OK) {
+    const cudaError_t ce = cudaStreamSynchronize(j->stream);
+    if (ce != cudaSuccess) e = fail(AVX_E_CUDA, std::string("request set-up: ") + cudaGetErrorString(ce));
+  }
+  t_pool_stream = nullptr;
+  return e;
+}
+
+void job_release(Job* j) {
+  delete j->s;  // buffers go back to the pool on the job's stream
+  delete j->op;
+  j->s = nullptr;
+  j->op = nullptr;
 }
 
 }  // namespace
@@ -2271,54 +2324,190 @@ avx_completion run_request(const avx_request& r, cudaStream_t stream) {
 struct avx_batch {
   int device = 0;
   size_t budget = 0, used = 0;
-  int running = 0, pending = 0;
+  int max_active = 1;
+  int admitted = 0;  // in set-up, ready or running
+  int pending = 0;   // submitted and not yet polled
   bool stop = false;
   std::mutex mu;
-  std::condition_variable cv_work, cv_done;
+  std::condition_variable cv_setup, cv_sched, cv_done;
   struct Item {
     avx_request r;
     size_t ws;
     std::chrono::steady_clock::time_point t_submit;
   };
   std::deque<Item> queue;
+  std::deque<Job*> ready;
   std::deque<avx_completion> done;
-  std::vector<std::thread> workers;
+  std::vector<int> free_slots;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> events;  // 2 per slot
+  DevState* h_states = nullptr;     // 2 per slot, pinned
+  std::vector<std::thread> setup_threads;
+  std::thread sched;
 
-  void work() {
+  void complete(Job* j, avx_status st) {
+    j->c.status = (int)st;
+    j->c.workspace_bytes = j->ws;
+    std::lock_guard<std::mutex> lk(mu);
+    used -= j->ws;
+    --admitted;
+    free_slots.push_back(j->slot);
+    done.push_back(j->c);
+    delete j;
+    cv_setup.notify_all();
+    cv_done.notify_all();
+  }
+
+  // first queued request whose workspace fits; nothing while the head has
+  // waited longer than kStarveMs without fitting (it then gets the memory next)
+  int pick() const {
+    if (queue.empty() || free_slots.empty() || admitted >= max_active + kSetupThreads) return -1;
+    const auto now = std::chrono::steady_clock::now();
+    for (size_t i = 0; i < queue.size(); ++i) {
+      if (used + queue[i].ws <= budget) return (int)i;
+      if (i == 0 && ms_since(queue[0].t_submit, now) > kStarveMs) return -1;
+    }
+    return -1;
+  }
+
+  void setup_loop() {
     cudaSetDevice(device);
-    DevArena arena;
-    cudaStream_t stream = nullptr;
-    cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
     for (;;) {
-      Item it;
+      Job* j = new Job();
       {
         std::unique_lock<std::mutex> lk(mu);
-        cv_work.wait(lk, [&] { return stop || (!queue.empty() && used + queue.front().ws <= budget); });
-        if (stop) break;
-        it = queue.front();
-        queue.pop_front();
-        used += it.ws;
-        ++running;
+        int i = -1;
+        while (!stop && (i = pick()) < 0) cv_setup.wait_for(lk, std::chrono::milliseconds(50));
+        if (stop) {
+          delete j;
+          break;
+        }
+        j->r = queue[i].r;
+        j->ws = queue[i].ws;
+        j->t_submit = queue[i].t_submit;
+        queue.erase(queue.begin() + i);
+        used += j->ws;
+        ++admitted;
+        j->slot = free_slots.back();
+        free_slots.pop_back();
       }
-      const auto t0 = std::chrono::steady_clock::now();
-      arena.reset();
-      t_arena = &arena;
-      avx_completion c = run_request(it.r, stream);
-      t_arena = nullptr;
-      const auto t1 = std::chrono::steady_clock::now();
-      c.queue_ms = ms_since(it.t_submit, t0);
-      c.run_ms = ms_since(t0, t1);
-      c.workspace_bytes = it.ws;
+      j->t_start = std::chrono::steady_clock::now();
+      j->c.tag = j->r.tag;
+      j->c.queue_ms = ms_since(j->t_submit, j->t_start);
+      j->stream = streams[j->slot];
+      for (int q = 0; q < 2; ++q) {
+        j->ev[q] = events[2 * j->slot + q];
+        j->hs[q] = h_states + 2 * j->slot + q;
+      }
+      avx_status st = job_setup(j);
+      if (st == AVX_OK && j->op->kind == 0) {
+        // the exact footprint now that the sampled rows are known
+        int max_rows = 0;
+        for (int t = 0; t < j->op->T; ++t) max_rows = std::max(max_rows, j->op->row_off[t + 1] - j->op->row_off[t]);
+        const size_t exact = request_workspace(j->r, j->op->R, max_rows);
+        if (exact < j->ws) {
+          std::lock_guard<std::mutex> lk(mu);
+          used -= j->ws - exact;
+          j->ws = exact;
+          cv_setup.notify_all();
+        }
+      }
+      if (st != AVX_OK) {
+        job_release(j);
+        j->c.run_ms = ms_since(j->t_start, std::chrono::steady_clock::now());
+        complete(j, st);
+        continue;
+      }
       {
         std::lock_guard<std::mutex> lk(mu);
-        used -= it.ws;
-        --running;
-        done.push_back(c);
+        ready.push_back(j);
       }
-      cv_work.notify_all();
-      cv_done.notify_all();
+      cv_sched.notify_all();
     }
-    if (stream) cudaStreamDestroy(stream);
+  }
+
+  // enqueue the next slice of j and a copy of its device state after it
+  avx_status launch_slice(Job* j) {
+    const unsigned k1 = std::min(j->s->p.maxIt, (j->k / kSlice + 1) * kSlice);
+    avx_status r = solver_enqueue(j->s, reinterpret_cast<const float2*>(j->r.d_b1), j->k, k1, &j->launches);
+    if (r != AVX_OK) return r;
+    const int q = (j->head + j->inflight) & 1;
+    AVX_CK(cudaMemcpyAsync(j->hs[q], j->s->st.p, sizeof(DevState), cudaMemcpyDeviceToHost, j->stream));
+    AVX_CK(cudaEventRecord(j->ev[q], j->stream));
+    j->k = k1;
+    ++j->inflight;
+    return AVX_OK;
+  }
+
+  avx_status retire(Job* j) {
+    avx_solver* s = j->s;
+    AVX_CK(cudaMemcpyAsync(j->r.d_x, s->primc(0), (size_t)s->N() * sizeof(float2), cudaMemcpyDeviceToDevice,
+                           j->stream));
+    AVX_CK(cudaMemcpyAsync(&s->last, s->st.p, sizeof(DevState), cudaMemcpyDeviceToHost, j->stream));
+    AVX_CK(cudaStreamSynchronize(j->stream));
+    const float ms = (float)ms_since(j->t_start, std::chrono::steady_clock::now());
+    const avx_status st = solver_finish_stats(s, ms, j->launches);
+    j->c.stats = s->stats;
+    return st;
+  }
+
+  void sched_loop() {
+    cudaSetDevice(device);
+    std::vector<Job*> active;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        while (!ready.empty() && (int)active.size() < max_active) {
+          active.push_back(ready.front());
+          ready.pop_front();
+        }
+        if (stop && active.empty()) break;
+        if (active.empty()) {
+          cv_sched.wait_for(lk, std::chrono::milliseconds(20));
+          continue;
+        }
+      }
+      bool progressed = false;
+      for (size_t i = 0; i < active.size();) {
+        Job* j = active[i];
+        avx_status st = AVX_OK;
+        bool finished = false;
+        // completed slices: read the device state they left
+        while (j->inflight > 0) {
+          const cudaError_t q = cudaEventQuery(j->ev[j->head]);
+          if (q == cudaErrorNotReady) break;
+          if (q != cudaSuccess) {
+            st = fail(AVX_E_CUDA, std::string("request slice failed: ") + cudaGetErrorString(q));
+            finished = true;
+            break;
+          }
+          const DevState& h = *j->hs[j->head];
+          if (h.stop || h.err) j->stopped = true;
+          j->head ^= 1;
+          --j->inflight;
+          progressed = true;
+        }
+        // keep two slices in flight until the run ends
+        while (!finished && !j->stopped && j->inflight < 2 && j->k < j->s->p.maxIt) {
+          st = launch_slice(j);
+          if (st != AVX_OK) finished = true;
+          progressed = true;
+        }
+        if (!finished && j->inflight == 0 && (j->stopped || j->k >= j->s->p.maxIt)) finished = true;
+        if (finished) {
+          const avx_status rs = retire(j);
+          if (st == AVX_OK) st = rs;
+          job_release(j);
+          j->c.run_ms = ms_since(j->t_start, std::chrono::steady_clock::now());
+          complete(j, st);
+          active.erase(active.begin() + i);
+          progressed = true;
+          continue;
+        }
+        ++i;
+      }
+      if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
   }
 };
 
@@ -2331,9 +2520,8 @@ avx_status avx_query_workspace(const avx_request* r, size_t* bytes) {
   if (!r->width || !r->height || !r->coils || !r->frames) return fail(AVX_E_ARG, "dimensions must be positive");
   if (r->op_kind == 1 && (!r->d_traj || !r->d_dens || !r->n_fe || !r->spokes_per_frame))
     return fail(AVX_E_ARG, "radial request needs trajectory, density and sample counts");
-  avx_status st;
-  *bytes = request_workspace(*r, &st);
-  return st;
+  *bytes = request_workspace(*r, -1, 0);
+  return AVX_OK;
 }
 
 avx_status avx_batch_create(int device, size_t hbm_budget, int workers, avx_batch** out) {
@@ -2344,10 +2532,42 @@ avx_status avx_batch_create(int device, size_t hbm_budget, int workers, avx_batc
   AVX_CK(cudaSetDevice(device));
   avx_status r = configure_once();
   if (r != AVX_OK) return r;
+  // keep freed pool memory for the next requests instead of returning it to the driver
+  cudaMemPool_t pool;
+  AVX_CK(cudaDeviceGetDefaultMemPool(&pool, device));
+  unsigned long long keep = ~0ull;
+  AVX_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
   avx_batch* b = new avx_batch();
   b->device = device;
   b->budget = hbm_budget;
-  for (int i = 0; i < workers; ++i) b->workers.emplace_back([b] { b->work(); });
+  b->max_active = workers;
+  const int slots = workers + kSetupThreads;
+  avx_status st = AVX_OK;
+  for (int i = 0; i < slots && st == AVX_OK; ++i) {
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+      st = fail(AVX_E_CUDA, "cannot create the engine's streams");
+      break;
+    }
+    b->streams.push_back(s);
+    b->free_slots.push_back(slots - 1 - i);
+    for (int q = 0; q < 2; ++q) {
+      cudaEvent_t e;
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) st = fail(AVX_E_CUDA, "cannot create events");
+      else b->events.push_back(e);
+    }
+  }
+  if (st == AVX_OK && cudaMallocHost(reinterpret_cast<void**>(&b->h_states), sizeof(DevState) * 2 * slots) != cudaSuccess)
+    st = fail(AVX_E_NOMEM, "cannot allocate pinned state slots");
+  if (st != AVX_OK) {
+    for (cudaStream_t s : b->streams) cudaStreamDestroy(s);
+    for (cudaEvent_t e : b->events) cudaEventDestroy(e);
+    delete b;
+    return st;
+  }
+  memset(b->h_states, 0, sizeof(DevState) * 2 * slots);
+  for (int i = 0; i < kSetupThreads; ++i) b->setup_threads.emplace_back([b] { b->setup_loop(); });
+  b->sched = std::thread([b] { b->sched_loop(); });
   *out = b;
   return AVX_OK;
 }
@@ -2356,7 +2576,6 @@ avx_status avx_batch_submit(avx_batch* b, const avx_request* r) {
   if (!b || !r) return fail(AVX_E_ARG, "null argument");
   if (!r->d_data || !r->d_x || !r->d_b1) return fail(AVX_E_ARG, "request without data, image or coil maps");
   size_t ws = 0;
-  AVX_CK(cudaSetDevice(b->device));
   avx_status st = avx_query_workspace(r, &ws);
   if (st != AVX_OK) return st;
   if (ws > b->budget) return fail(AVX_E_NOMEM, "request workspace exceeds the engine's HBM budget");
@@ -2365,7 +2584,7 @@ avx_status avx_batch_submit(avx_batch* b, const avx_request* r) {
     b->queue.push_back({*r, ws, std::chrono::steady_clock::now()});
     ++b->pending;
   }
-  b->cv_work.notify_all();
+  b->cv_setup.notify_all();
   return AVX_OK;
 }
 
@@ -2390,7 +2609,7 @@ avx_status avx_serve_poll(avx_batch* b, avx_completion* out, int max, int* n, in
 avx_status avx_batch_drain(avx_batch* b) {
   if (!b) return fail(AVX_E_ARG, "null engine");
   std::unique_lock<std::mutex> lk(b->mu);
-  b->cv_done.wait(lk, [&] { return b->queue.empty() && b->running == 0; });
+  b->cv_done.wait(lk, [&] { return b->queue.empty() && b->admitted == 0; });
   return AVX_OK;
 }
 
@@ -2403,12 +2622,22 @@ int avx_batch_pending(const avx_batch* b) {
 void avx_batch_destroy(avx_batch* b) {
   if (!b) return;
   {
-    std::lock_guard<std::mutex> lk(b->mu);
-    b->stop = true;
+    // queued requests are dropped; admitted ones run to their end
+    std::unique_lock<std::mutex> lk(b->mu);
     b->queue.clear();
+    b->cv_done.wait(lk, [&] { return b->admitted == 0; });
+    b->stop = true;
   }
-  b->cv_work.notify_all();
-  for (std::thread& t : b->workers) t.join();
+  b->cv_setup.notify_all();
+  b->cv_sched.notify_all();
+  for (std::thread& t : b->setup_threads) t.join();
+  b->sched.join();
+  for (cudaStream_t s : b->streams) {
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+  }
+  for (cudaEvent_t e : b->events) cudaEventDestroy(e);
+  cudaFreeHost(b->h_states);
   delete b;
 }
 

@@ -330,8 +330,10 @@ def run_batched(av, torch, workers, n=64, iters=800, rank=0, world=1, dist=None)
 def run_serving(av, torch, workers, n, rates, max_it=1500, rel_gap=1e-4):
     """The serving configuration on a bounded sample: n requests (50/30/20 %
     TV/TGV2/ICTGV2, 70/30 % Cartesian/radial) arriving as a Poisson stream at
-    each rate; every request stops at a relative primal-dual gap of rel_gap or
-    at max_it iterations."""
+    each rate; every request stops at max_it iterations or once its
+    normalised primal-dual gap (the gap over the pixel count, the reference's
+    stop test, tgv2.cpp:317-330) falls below rel_gap, evaluated every 20
+    iterations."""
     from avionic_b200 import synth
     specs = synth.serving_stream(4, n, 1.0)
     items = []
@@ -345,12 +347,13 @@ def run_serving(av, torch, workers, n, rates, max_it=1500, rel_gap=1e-4):
         sp = it["spec"]
         p = av.default_params(av.METHODS[sp["method"]])
         p.maxIt = max_it
+        p.stopPDGap = rel_gap
         if sp["kind"] == "cartesian":
             return av.cartesian_request(sp["method"], it["kdata"], out, it["b1"], mask=it["mask"], params=p,
-                                        dft_mode=dft, tag=tag, stop_gap_rel=rel_gap)
+                                        dft_mode=dft, tag=tag)
         return av.radial_request(sp["method"], it["kdata"], out, it["b1"], it["traj"], it["dens"], it["spokes"],
                                  it["n_fe"], params=p, kernel_width=it["kernel_width"],
-                                 sector_width=it["sector_width"], osf=it["osf"], tag=tag, stop_gap_rel=rel_gap)
+                                 sector_width=it["sector_width"], osf=it["osf"], tag=tag)
 
     unit_arrivals = np.array([sp["arrival"] for sp in specs])
     res = {}
@@ -373,8 +376,8 @@ def run_serving(av, torch, workers, n, rates, max_it=1500, rel_gap=1e-4):
     torch.cuda.empty_cache()
     return {"workload": "%d requests (sample of the 2000-request stream): 50/30/20%% TV/TGV2/ICTGV2, 70%% Cartesian "
                         "(matrix 96-320, frames 8-48, coils 4-32) / 30%% radial (128x128, 256 readout samples, 13-34 "
-                        "spokes/frame, 20-60 frames, 12 coils), stop at relative gap %g or %d iterations, HBM budget "
-                        "150 GB" % (n, rel_gap, max_it),
+                        "spokes/frame, 20-60 frames, 12 coils), stop at normalised gap %g (gap / pixels) or %d "
+                        "iterations, HBM budget 150 GB" % (n, rel_gap, max_it),
             "forms": res,
             "timing": "host wall clock; latency = submission (arrival) to completion"}
 
@@ -606,7 +609,8 @@ def main():
     ap.add_argument("--parts", default="headline,tv128,radial,batched,serving",
                     help="comma list: headline (the 192x192x30 cine ICTGV2 line), tv128, radial, batched, serving "
                          "(added to the line at N=1; batched at every N)")
-    ap.add_argument("--batch-workers", type=int, default=8, help="concurrent reconstructions of the batched forms")
+    ap.add_argument("--batch-workers", type=int, default=64,
+                    help="requests the engine advances together in the batched and served forms")
     ap.add_argument("--batch-size", type=int, default=64)
     ap.add_argument("--serve-requests", type=int, default=24,
                     help="requests per rate (bounded sample of the 2000-request stream)")

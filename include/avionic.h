@@ -386,13 +386,20 @@ avx_status avx_normalize_data(unsigned W, unsigned H, unsigned C, unsigned T, un
 /* ------------------------------------------------------------------ */
 
 /* No reference counterpart: the reference runs one reconstruction per
- * process (main.cpp:789).  An engine owns worker threads, each with its own
- * CUDA stream and device workspace; submitted requests wait in a FIFO queue
- * and start, in order, as soon as their workspace fits the engine's HBM
- * budget, so independent reconstructions of any mix of sizes, methods and
- * operators run concurrently on one GPU.  Every request is an ordinary
- * operator + solver run with the given parameters (the result equals
- * avx_solver_run on the same inputs).  Buffers are the caller's device
+ * process (main.cpp:789).  An engine batches reconstructions continuously, at
+ * iteration granularity.  Submitted requests wait in a queue; set-up threads
+ * admit the first one whose device workspace fits the engine's HBM budget (a
+ * request that has waited 2 s blocks later ones until it fits) and build its
+ * operator, solver, device state and iteration graphs on a stream of its own,
+ * with memory from the device's stream-ordered pool.  One scheduler thread
+ * advances up to `workers` admitted requests together, 20 iterations (one
+ * gap cadence) at a time with two such slices in flight per request, reads
+ * each request's device state after every slice without blocking, and
+ * retires a request at its stop test (stopPDGap, the normalised gap of the
+ * reference, tgv2.cpp:317-330, or stop_gap_rel) or at maxIt, which frees its
+ * budget for the next admission.  Requests of any mix of sizes, methods and
+ * operators share the GPU this way; each result equals avx_solver_run on the
+ * same inputs and parameters, bit for bit.  Buffers are the caller's device
  * buffers and must stay valid until the request's completion is polled. */
 typedef struct avx_request {
   int method;                /* AVX_METHOD_TV / _TVTEMP / _TGV2 / _ICTV / _ICTGV2 */
@@ -419,16 +426,20 @@ typedef struct avx_completion {
   int dft_mode;              /* form the Cartesian operator used */
   avx_run_stats stats;
   double queue_ms;           /* submit -> start (host clock) */
-  double run_ms;             /* start -> finished, operator set-up included (host clock) */
+  double run_ms;             /* admission -> finished, set-up included (host clock) */
   size_t workspace_bytes;    /* the admission estimate */
 } avx_completion;
 
 typedef struct avx_batch avx_batch;
 
-/* Device bytes a request needs while it runs (operator, solver, tables). */
+/* Device bytes a request needs while it runs (operator, solver, tables): an
+ * upper bound that counts the Cartesian k-space at every row, since the mask
+ * is not read at submission; admission holds this much until the request's
+ * operator is built and then only its exact footprint. */
 avx_status avx_query_workspace(const avx_request* r, size_t* bytes);
-/* device: CUDA ordinal; hbm_budget: bytes the running requests may hold
- * together; workers: concurrent reconstructions at most (>= 1). */
+/* device: CUDA ordinal; hbm_budget: bytes the admitted requests may hold
+ * together; workers: requests advanced together at most (>= 1; 1 runs them
+ * one after another, each set up while the previous one runs). */
 avx_status avx_batch_create(int device, size_t hbm_budget, int workers, avx_batch** out);
 /* Queues a copy of *r.  AVX_E_NOMEM when its workspace exceeds the whole budget. */
 avx_status avx_batch_submit(avx_batch* b, const avx_request* r);
@@ -440,7 +451,7 @@ avx_status avx_serve_poll(avx_batch* b, avx_completion* out, int max, int* n, in
 avx_status avx_batch_drain(avx_batch* b);
 /* Requests submitted and not yet polled. */
 int avx_batch_pending(const avx_batch* b);
-/* Stops the workers after the running requests; queued requests are dropped. */
+/* Drops the queued requests, waits for the admitted ones and stops the engine's threads. */
 void avx_batch_destroy(avx_batch* b);
 
 /* ------------------------------------------------------------------ */
