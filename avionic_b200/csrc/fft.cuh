@@ -3,6 +3,11 @@
 
 #include "common.cuh"
 
+// Row pitch (in complex values) of the [x][pitch] sequence buffers: KC + 1.
+// An odd pitch spreads the x-strided accesses (the transposing loads and
+// stores around the passes) over all 32 banks.
+#define AVX_FFT_PITCH(KC) ((KC) + 1)
+
 // ---------------------------------------------------------------------------
 // KC independent length-W sequences stored [x][KCP] (row index kk
 // fastest), mixed-radix Stockham autosort passes ping-ponging between two
@@ -60,7 +65,7 @@ AVX_D void stage_plan(const int (&rad)[12], int* splan) {
 // whose prime factors are at most 5), which keeps the register count down.
 template <int KC, bool LARGE = true>
 __device__ float2* row_fft(float2* src, float2* dst, const float2* tw, int W, int nrad, const int* rad, int sign) {
-  constexpr int KCP = KC + 2;
+  constexpr int KCP = AVX_FFT_PITCH(KC);
   int Ns = 1;
   // kk is fixed per thread when the block size is a multiple of KC
   for (int p = 0; p < nrad; ++p) {
@@ -192,7 +197,7 @@ AVX_D void butterfly_fixed(float2 (&v)[R], const float2* tw, int nb) {
 
 template <int KC, int NT, int W, int SIGN, int NS, int R>
 AVX_D void fft_pass_fixed(const float2* src, float2* dst, const float2* tw) {
-  constexpr int KCP = KC + 2, NB = W / R, TWS = W / (NS * R), TOTAL = NB * KC;
+  constexpr int KCP = AVX_FFT_PITCH(KC), NB = W / R, TWS = W / (NS * R), TOTAL = NB * KC;
 #pragma unroll
   for (int e0 = 0; e0 < TOTAL; e0 += NT) {
     const int e = e0 + (int)threadIdx.x;

@@ -6,7 +6,7 @@ namespace avx {
 #define FFT2D_KC 16
 
 __global__ void __launch_bounds__(256) fft2d_rows_kernel(Fft2dPlan p, float2* data, int sign) {
-  constexpr int KC = FFT2D_KC, KCP = KC + 2;
+  constexpr int KC = FFT2D_KC, KCP = AVX_FFT_PITCH(KC);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int G = p.W;
   float2* A = reinterpret_cast<float2*>(smem_raw);
@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(256) fft2d_rows_kernel(Fft2dPlan p, float2* da
 }
 
 __global__ void __launch_bounds__(256) fft2d_cols_kernel(Fft2dPlan p, float2* data, int sign) {
-  constexpr int KC = FFT2D_KC, KCP = KC + 2;
+  constexpr int KC = FFT2D_KC, KCP = AVX_FFT_PITCH(KC);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int G = p.H;
   float2* A = reinterpret_cast<float2*>(smem_raw);
@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(256) fft2d_cols_kernel(Fft2dPlan p, float2* da
   }
 }
 
-size_t fft2d_smem_bytes(int n) { return sizeof(float2) * (2 * (size_t)n * (FFT2D_KC + 2) + n); }
+size_t fft2d_smem_bytes(int n) { return sizeof(float2) * (2 * (size_t)n * AVX_FFT_PITCH(FFT2D_KC) + n); }
 
 cudaError_t configure_fft2d_kernels() {
   cudaError_t e = cudaFuncSetAttribute(fft2d_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);

@@ -234,7 +234,7 @@ size_t ydft_smem_bytes(int H) { return sizeof(float2) * (size_t)H * (YD_XS + KSP
 template <int KC, int PLAN>
 __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
   if (a.st && a.st->stop && mode != 3) return;
-  constexpr int KCP = KC + 2;
+  constexpr int KCP = AVX_FFT_PITCH(KC);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const CartGeomDev& g = a.g;
   const int W = PLAN > 1 ? PLAN : g.W, C = g.C;  // W compile-time with a fixed plan
@@ -301,20 +301,15 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
         int jj = (step * ((W - g.sx) % W)) % W;  // index for x = 0
         for (int x = 0; x < W; ++x) {
           const float2 tw = twx[jj];
-          const float4* pr = reinterpret_cast<const float4*>(P + x * KCP);
+          const float2* pr = P + x * KCP;
 #pragma unroll
-          for (int kk = 0; kk < KC; kk += 2) {
-            float4 q = pr[kk >> 1];
-            cfma(acc[kk], tw, make_float2(q.x, q.y));
-            cfma(acc[kk + 1], tw, make_float2(q.z, q.w));
-          }
+          for (int kk = 0; kk < KC; ++kk) cfma(acc[kk], tw, pr[kk]);
           jj += step;
           if (jj >= W) jj -= W;
         }
-        float4* xr = reinterpret_cast<float4*>(X + kx * KCP);
+        float2* xr = X + kx * KCP;
 #pragma unroll
-        for (int kk = 0; kk < KC; kk += 2)
-          xr[kk >> 1] = make_float4(acc[kk].x, acc[kk].y, acc[kk + 1].x, acc[kk + 1].y);
+        for (int kk = 0; kk < KC; ++kk) xr[kk] = acc[kk];
       }
       __syncthreads();
     }
@@ -402,13 +397,9 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
       for (int kx = 0; kx < W; ++kx) {
         const float2 tw = twx[jj];
         const float2 twc = make_float2(tw.x, -tw.y);
-        const float4* xr = reinterpret_cast<const float4*>(X + kx * KCP);
+        const float2* xr = X + kx * KCP;
 #pragma unroll
-        for (int kk = 0; kk < KC; kk += 2) {
-          float4 q = xr[kk >> 1];
-          cfma(acc[kk], twc, make_float2(q.x, q.y));
-          cfma(acc[kk + 1], twc, make_float2(q.z, q.w));
-        }
+        for (int kk = 0; kk < KC; ++kk) cfma(acc[kk], twc, xr[kk]);
         jj += step;
         if (jj >= W) jj -= W;
       }
@@ -429,7 +420,7 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
 }
 
 size_t rows_smem_bytes(int W) {
-  const int KCP = KSPACE_KC + 2;
+  const int KCP = AVX_FFT_PITCH(KSPACE_KC);
   return sizeof(float2) * (2 * (size_t)W * KCP + W) + sizeof(double) * 32 * 3;
 }
 

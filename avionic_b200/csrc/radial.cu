@@ -48,7 +48,7 @@ AVX_D int grid_to_img(int m, int d, int G) {
 // sign -1.  Chunks without image rows store zeros.
 template <int PLAN>
 __global__ void __launch_bounds__(256) rad_rows_fwd_kernel(RArgs a) {
-  constexpr int KC = RAD_FFT_KC, KCP = KC + 2;
+  constexpr int KC = RAD_FFT_KC, KCP = AVX_FFT_PITCH(KC);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RadialGeomDev& g = a.g;
   const int G = PLAN > 1 ? PLAN : g.Gx;  // compile-time with a fixed plan
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(256) rad_rows_fwd_kernel(RArgs a) {
 template <int PLAN>
 __global__ void __launch_bounds__(256) rad_rows_adj_kernel(RArgs a, float2* img) {
   if (a.st && a.st->stop) return;
-  constexpr int KC = RAD_ADJ_KC, KCP = KC + 2;
+  constexpr int KC = RAD_ADJ_KC, KCP = AVX_FFT_PITCH(KC);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RadialGeomDev& g = a.g;
   const int G = PLAN > 1 ? PLAN : g.Gx, W = g.W;  // G compile-time with a fixed plan
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(256) rad_rows_adj_kernel(RArgs a, float2* img)
 // columns (along y) of 16 grid columns per CTA, in place
 template <int PLAN, int SIGN>
 __global__ void __launch_bounds__(256) rad_fft_cols_kernel(RArgs a) {
-  constexpr int KC = RAD_FFT_KC, KCP = KC + 2;
+  constexpr int KC = RAD_FFT_KC, KCP = AVX_FFT_PITCH(KC);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RadialGeomDev& g = a.g;
   const int G = PLAN > 1 ? PLAN : g.Gy;  // compile-time with a fixed plan
@@ -382,9 +382,9 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
 
 // ---------------------------------------------------------------------------
 
-size_t radial_fft_smem_bytes(int G) { return sizeof(float2) * (2 * (size_t)G * (RAD_FFT_KC + 2) + G); }
+size_t radial_fft_smem_bytes(int G) { return sizeof(float2) * (2 * (size_t)G * AVX_FFT_PITCH(RAD_FFT_KC) + G); }
 size_t radial_adj_smem_bytes(int G, int W) {
-  return sizeof(float2) * (2 * (size_t)G * (RAD_ADJ_KC + 2) + G + (size_t)RAD_ADJ_KC * W);
+  return sizeof(float2) * (2 * (size_t)G * AVX_FFT_PITCH(RAD_ADJ_KC) + G + (size_t)RAD_ADJ_KC * W);
 }
 
 int radial_interp_blocks(const RadialGeomDev& g) { return (int)(((long long)g.T * g.C * g.S + 255) / 256); }

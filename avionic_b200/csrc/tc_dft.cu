@@ -114,7 +114,7 @@ AVX_D uint32_t packhi(uint32_t lo, uint32_t hi) { return __byte_perm(lo, hi, 0x7
 
 size_t tc_ytab_bytes(int H, int T, int np) { return (size_t)T * tc_nstage(H) * 3 * tc_piece_bytes(np); }
 
-size_t tc_ydft_smem_bytes(int np) { return 2 * (size_t)(3 * kPieceA + 3 * tc_piece_bytes(np)) + 64; }
+size_t tc_ydft_smem_bytes(int np) { return 2 * (size_t)3 * kPieceA + 3 * (size_t)3 * tc_piece_bytes(np) + 64; }
 
 static unsigned short host_bf16(float f) {
   uint32_t u;
@@ -165,7 +165,16 @@ void tc_build_ytab(int W, int H, int T, int sx, int sy, const int* rows, const i
   }
 }
 
-template <bool U2>
+// Producer layout: thread tid owns the tile rows m = 2 (tid % 64) and m + 1
+// (adjacent columns x, x + 1 of one coil when W is even, loaded as one
+// 16-byte vector) and the four image rows 4 g .. 4 g + 3 of every stage,
+// g = tid / 64, which fill core-matrix column g of the stage's A tile.  The
+// coefficient pieces run through a three-stage ring filled one stage ahead by
+// cp.async, so their L2 latency hides behind the production of A; A itself
+// is double-buffered.  The MMAs of stage s are committed to bar[s % 2]; stage
+// s + 2 waits on that barrier (one lane per warp polls it) before it reuses
+// the A buffer and the coefficient buffer of stage s + 3.
+template <bool U2, bool VEC>
 __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   if (a.st && a.st->stop) return;
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -177,15 +186,21 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   if (S == 0) return;
   const int np = a.tc_np;
   const int pieceB = tc_piece_bytes(np);
-  const int stage_bytes = 3 * kPieceA + 3 * pieceB;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * stage_bytes);
+  const int stageA = 3 * kPieceA, stageB = 3 * pieceB;
+  unsigned char* sA = smem;               // 2 stages
+  unsigned char* sB = smem + 2 * stageA;  // 3 stages
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sB + 3 * stageB);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int m = tid & (TC_M - 1), half = tid >> 7;
-  const int mg = blockIdx.x * TC_M + m;
-  const bool valid = mg < C * W;
-  const int c = valid ? mg / W : 0, x = valid ? mg - c * W : 0;
-  const long long HW = (long long)W * H;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int half = tid >> 7;  // epilogue: TMEM column half
+  const int rp = tid & 63, grp = tid >> 6;
+  const int mrow = 2 * rp;                      // first of this thread's two tile rows
+  const int mg = blockIdx.x * TC_M + mrow;      // global (c, x) row index
+  const int CW = C * W;
+  const bool v0 = mg < CW, v1 = mg + 1 < CW;
+  const int c0 = v0 ? mg / W : 0, x0 = v0 ? mg - c0 * W : 0;
+  const int c1 = v1 ? (mg + 1) / W : 0, x1 = v1 ? mg + 1 - c1 * W : 0;
+  const int HW = W * H;
   const uint32_t ncols = np <= 32 ? 32u : (np <= 64 ? 64u : 128u);
 
   if (warp == 0) {
@@ -205,65 +220,101 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   const uint32_t tmem = *tslot;
   const uint32_t idesc = idesc_bf16(np);
 
-  const float2* __restrict__ bc = a.b1 + (long long)c * HW + x;
-  const float2* __restrict__ uc = a.in + (long long)t * HW + x;
-  const float2* __restrict__ uc2 = a.in2 ? a.in2 + (long long)t * HW + x : nullptr;
+  // this thread's columns: image rows are W apart
+  const float2* __restrict__ pb0 = a.b1 + (long long)c0 * HW + x0;
+  const float2* __restrict__ pb1 = a.b1 + (long long)c1 * HW + x1;
+  const float2* __restrict__ pu0 = a.in + (long long)t * HW + x0;
+  const float2* __restrict__ pu1 = a.in + (long long)t * HW + x1;
+  const float2* __restrict__ pw0 = U2 ? a.in2 + (long long)t * HW + x0 : nullptr;
+  const float2* __restrict__ pw1 = U2 ? a.in2 + (long long)t * HW + x1 : nullptr;
   const uint4* __restrict__ btab = a.tc_ytab + (size_t)t * tc_nstage(H) * 3 * (pieceB / 16);
   const int nst = tc_nstage(H);
+  const int nbt = stageB / 16;
   bool ok = true;
 
-  // register prefetch of one stage: this thread's 8 image rows of b1, u (, u2)
-  // and its share of the coefficient pieces, loaded one stage ahead
-  float2 pb[8], pu[8], pu2[U2 ? 8 : 1];
-  const int nbt = 3 * pieceB / 16;
+  auto issue_b = [&](int st) {
+    const uint4* src = btab + (size_t)st * nbt;
+    unsigned char* dst = sB + (st % 3) * stageB;
+    for (int e = tid; e < nbt; e += TC_THREADS)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst + 16 * e)), "l"(src + e) : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+
+  // register prefetch of one stage: b1 and u (, u2) of both columns at 4 image rows
+  float2 pb[2][4], pu[2][4], pw[2][U2 ? 4 : 1];
   auto load_stage = [&](int st) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int y = st * (TC_KS / 2) + 8 * half + i;
-      const bool in = valid && y < H;
-      pb[i] = in ? __ldg(bc + (long long)y * W) : make_float2(0.f, 0.f);
-      pu[i] = in ? uc[(long long)y * W] : make_float2(0.f, 0.f);
-      if (U2) pu2[i] = in ? uc2[(long long)y * W] : make_float2(0.f, 0.f);
+    for (int i = 0; i < 4; ++i) {
+      const int y = st * (TC_KS / 2) + 4 * grp + i;
+      const bool in = y < H;
+      const int off = y * W;
+      if (VEC) {
+        // W even: x0 even and x1 = x0 + 1 in the same coil, 16-byte aligned
+        const float4 zb = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 qb = (in && v0) ? __ldg(reinterpret_cast<const float4*>(pb0 + off)) : zb;
+        const float4 qu = (in && v0) ? *reinterpret_cast<const float4*>(pu0 + off) : zb;
+        pb[0][i] = make_float2(qb.x, qb.y);
+        pb[1][i] = make_float2(qb.z, qb.w);
+        pu[0][i] = make_float2(qu.x, qu.y);
+        pu[1][i] = make_float2(qu.z, qu.w);
+        if (U2) {
+          const float4 qw = (in && v0) ? *reinterpret_cast<const float4*>(pw0 + off) : zb;
+          pw[0][i] = make_float2(qw.x, qw.y);
+          pw[1][i] = make_float2(qw.z, qw.w);
+        }
+      } else {
+        pb[0][i] = (in && v0) ? __ldg(pb0 + off) : czero();
+        pb[1][i] = (in && v1) ? __ldg(pb1 + off) : czero();
+        pu[0][i] = (in && v0) ? pu0[off] : czero();
+        pu[1][i] = (in && v1) ? pu1[off] : czero();
+        if (U2) {
+          pw[0][i] = (in && v0) ? pw0[off] : czero();
+          pw[1][i] = (in && v1) ? pw1[off] : czero();
+        }
+      }
     }
   };
-  load_stage(0);
 
+  issue_b(0);
+  load_stage(0);
   for (int s = 0; s < nst; ++s) {
-    const int buf = s & 1;
-    unsigned char* sa = smem + buf * stage_bytes;
-    unsigned char* sb = sa + 3 * kPieceA;
-    if (s >= 2) ok = mbar_wait(&bar[buf], (uint32_t)((s - 2) >> 1) & 1u) && ok;
-    // B: asynchronous 16-byte copies of the stage's coefficient pieces
-    {
-      const uint4* src = btab + (size_t)s * nbt;
-      for (int e = tid; e < nbt; e += TC_THREADS)
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sb + 16 * e)), "l"(src + e)
-                     : "memory");
-      asm volatile("cp.async.commit_group;" ::: "memory");
+    unsigned char* sa = sA + (s & 1) * stageA;
+    unsigned char* sb = sB + (s % 3) * stageB;
+    if (s >= 2) {
+      // MMAs of stage s - 2 done: its A buffer and the coefficient buffer of stage s + 1 are free
+      bool w = true;
+      if (lane == 0) w = mbar_wait(&bar[s & 1], (uint32_t)((s - 2) >> 1) & 1u);
+      ok = __shfl_sync(0xffffffffu, w ? 1 : 0, 0) && ok;
     }
-    // A values of this stage from the prefetched registers
-    float2 v[8];
+    if (s + 1 < nst) issue_b(s + 1);
+    float2 v[2][4];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) v[i] = cmul(pb[i], U2 ? csub(pu[i], pu2[i]) : pu[i]);
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) v[r][i] = cmul(pb[r][i], U2 ? csub(pu[r][i], pw[r][i]) : pu[r][i]);
     if (s + 1 < nst) load_stage(s + 1);
-    // split and store: core-matrix columns j = 2 half + q (4 image rows each)
+    // split and store: row mrow + r, core-matrix column grp (k = 8 grp .. 8 grp + 7)
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int j = 2 * half + q;
+    for (int r = 0; r < 2; ++r) {
       uint32_t re[4][3], im[4][3];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        split3t(v[4 * q + i].x, re[i]);
-        split3t(v[4 * q + i].y, im[i]);
+        split3t(v[r][i].x, re[i]);
+        split3t(v[r][i].y, im[i]);
       }
-      const int off = (m >> 3) * kSBO + j * kLBO + (m & 7) * 16;
+      const int m = mrow + r;
+      const int off = (m >> 3) * kSBO + grp * kLBO + (m & 7) * 16;
 #pragma unroll
       for (int p = 0; p < 3; ++p)
         *reinterpret_cast<uint4*>(sa + p * kPieceA + off) =
             make_uint4(packhi(re[0][p], im[0][p]), packhi(re[1][p], im[1][p]), packhi(re[2][p], im[2][p]),
                        packhi(re[3][p], im[3][p]));
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    // this stage's coefficients have landed (the next stage's may be in flight)
+    if (s + 1 < nst)
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    else
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (tid == 0) {
@@ -281,27 +332,31 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
           mma_bf16(tmem, da, db, idesc, (s | ks | pr) != 0);
         }
       }
-      mma_commit(&bar[buf]);
+      mma_commit(&bar[s & 1]);
     }
   }
   const int last = nst - 1;
   ok = mbar_wait(&bar[last & 1], (uint32_t)(last >> 1) & 1u) && ok;
   if (nst >= 2) ok = mbar_wait(&bar[(last - 1) & 1], (uint32_t)((last - 1) >> 1) & 1u) && ok;
   tc_fence_after();
-  if (!ok) {
-    if (a.st && tid == 0) atomicExch(&a.st->err, 2);
+  if (!__all_sync(0xffffffffu, ok)) {
+    if (a.st && lane == 0) atomicExch(&a.st->err, 2);
   } else {
-    // epilogue: TMEM lane (warp % 4) * 32 + laneid = row m; this half's columns
+    // epilogue: TMEM lane (warp % 4) * 32 + laneid = tile row m; this half's columns
     const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
     const int ncol_half = np / 2;
-    float2* out = a.qp + kbase(g, t, c, r0, r1) + x;
-    for (int c0 = half * ncol_half; c0 < (half + 1) * ncol_half; c0 += 8) {
-      float v[8];
-      tmem_ld(tmem + lane_base + (uint32_t)c0, v);
+    const int m = (warp & 3) * 32 + lane;
+    const int me = blockIdx.x * TC_M + m;
+    const bool valid = me < CW;
+    const int ce = valid ? me / W : 0, xe = valid ? me - ce * W : 0;
+    float2* out = a.qp + kbase(g, t, ce, r0, r1) + xe;
+    for (int cc = half * ncol_half; cc < (half + 1) * ncol_half; cc += 8) {
+      float vv[8];
+      tmem_ld(tmem + lane_base + (uint32_t)cc, vv);
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        const int kk = (c0 >> 1) + i;
-        if (valid && kk < S) out[(long long)kk * W] = make_float2(v[2 * i], v[2 * i + 1]);
+        const int kk = (cc >> 1) + i;
+        if (valid && kk < S) out[(long long)kk * W] = make_float2(vv[2 * i], vv[2 * i + 1]);
       }
     }
   }
@@ -387,7 +442,7 @@ AVX_D void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__global__ void __launch_bounds__(TC_THREADS) coladj_tc_kernel(KArgs k, float2* img) {
+__global__ void __launch_bounds__(TC_THREADS, 2) coladj_tc_kernel(KArgs k, float2* img) {
   if (k.st && k.st->stop) return;
   constexpr int XT = CA_TC_XT;        // columns per tile
   constexpr int XH = XT / 2;          // columns per thread in the epilogue
@@ -442,9 +497,31 @@ __global__ void __launch_bounds__(TC_THREADS) coladj_tc_kernel(KArgs k, float2* 
     bool ok = true;
     int phase = 0;
 
+    // coil maps of four coils ahead of the combine, in registers (their L2
+    // latency hides behind the split, the MMAs and three combines)
+    float2 pb0[XH], pb1[XH], pb2[XH], pb3[XH];
+    auto load_b1 = [&](int cc, int cend, float2 (&pb)[XH]) {
+      // column-tile order: consecutive rows y of one column are adjacent
+      const float2* bc = k.b1t + (((long long)blockIdx.x * C + cc) * XT + XH * half) * H + y;
+#pragma unroll
+      for (int i = 0; i < XH; ++i)
+        pb[i] = (cc < cend && y < H) ? __ldg(bc + (long long)i * H) : make_float2(0.f, 0.f);
+    };
+    auto combine = [&](int cl, const float2 (&pb)[XH]) {
+      float v[XT];
+      static_assert(XT == 8 || XT == 16, "the epilogue reads 8 or 16 accumulator columns per thread");
+      tmem_ld(tmem + lane_base + (uint32_t)(2 * XT * cl + half * XT), v);
+#pragma unroll
+      for (int i = 0; i < XH; ++i) acc[i] = cadd(acc[i], cmulc(pb[i], make_float2(v[2 * i], v[2 * i + 1])));
+    };
     for (int c0 = 0; c0 < C; c0 += CC) {
       const int ncc = min(CC, C - c0);
       const int nbc = ((2 * XT * ncc + 15) / 16) * 16;
+      const int cend = c0 + ncc;
+      load_b1(c0, cend, pb0);
+      load_b1(c0 + 1, cend, pb1);
+      load_b1(c0 + 2, cend, pb2);
+      load_b1(c0 + 3, cend, pb3);
       // B rows n = 16 cl + 2 xl + part for coil c0 + cl; items (coil, column, 4 compact rows)
       const int items = ncc * XT * (kc / 8);
       for (int it = tid; it < items; it += TC_THREADS) {
@@ -505,32 +582,23 @@ __global__ void __launch_bounds__(TC_THREADS) coladj_tc_kernel(KArgs k, float2* 
         }
         mma_commit(&bar[0]);
       }
-      // b1 of the first two coils while the MMAs run
-      float2 pbA[XH], pbB[XH];
-      auto load_b1 = [&](int cc, float2 (&pb)[XH]) {
-        // column-tile order: consecutive rows y of one column are adjacent
-        const float2* bc = k.b1t + (((long long)blockIdx.x * C + cc) * XT + XH * half) * H + y;
-#pragma unroll
-        for (int i = 0; i < XH; ++i)
-          pb[i] = (cc < c0 + ncc && y < H) ? __ldg(bc + (long long)i * H) : make_float2(0.f, 0.f);
-      };
-      auto combine = [&](int cl, const float2 (&pb)[XH]) {
-        float v[XT];
-        static_assert(XT == 8 || XT == 16, "the epilogue reads 8 or 16 accumulator columns per thread");
-        tmem_ld(tmem + lane_base + (uint32_t)(2 * XT * cl + half * XT), v);
-#pragma unroll
-        for (int i = 0; i < XH; ++i) acc[i] = cadd(acc[i], cmulc(pb[i], make_float2(v[2 * i], v[2 * i + 1])));
-      };
-      load_b1(c0, pbA);
-      load_b1(c0 + 1, pbB);
-      ok = mbar_wait(&bar[0], (uint32_t)phase) && ok;
+      {
+        // one lane per warp polls the MMAs' barrier
+        bool w = true;
+        if ((tid & 31) == 0) w = mbar_wait(&bar[0], (uint32_t)phase);
+        ok = __shfl_sync(0xffffffffu, w ? 1 : 0, 0) && ok;
+      }
       phase ^= 1;
       tc_fence_after();
-      for (int cl = 0; cl < ncc; cl += 2) {
-        combine(cl, pbA);
-        load_b1(c0 + cl + 2, pbA);
-        if (cl + 1 < ncc) combine(cl + 1, pbB);
-        load_b1(c0 + cl + 3, pbB);
+      for (int cl = 0; cl < ncc; cl += 4) {
+        combine(cl, pb0);
+        load_b1(c0 + cl + 4, cend, pb0);
+        if (cl + 1 < ncc) combine(cl + 1, pb1);
+        load_b1(c0 + cl + 5, cend, pb1);
+        if (cl + 2 < ncc) combine(cl + 2, pb2);
+        load_b1(c0 + cl + 6, cend, pb2);
+        if (cl + 3 < ncc) combine(cl + 3, pb3);
+        load_b1(c0 + cl + 7, cend, pb3);
       }
       tc_fence_before();
       __syncthreads();  // TMEM and B are reused by the next chunk
@@ -570,9 +638,14 @@ void launch_b1_tile_transpose(const float2* b1, float2* b1t, int W, int H, int C
 }
 
 cudaError_t configure_tc_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(ydft_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
-  if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(ydft_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
+  cudaError_t e = cudaFuncSetAttribute(ydft_tc_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       AVX_DYN_SMEM_MAX);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ydft_tc_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ydft_tc_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ydft_tc_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(coladj_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
 }
@@ -584,10 +657,19 @@ void launch_coladj_tc(const KArgs& k, float2* img, cudaStream_t s) {
 
 void launch_ydft_tc(const KArgs& k, cudaStream_t s) {
   dim3 gr((k.g.C * k.g.W + TC_M - 1) / TC_M, k.g.T);
-  if (k.in2)
-    ydft_tc_kernel<true><<<gr, TC_THREADS, tc_ydft_smem_bytes(k.tc_np), s>>>(k);
-  else
-    ydft_tc_kernel<false><<<gr, TC_THREADS, tc_ydft_smem_bytes(k.tc_np), s>>>(k);
+  const size_t sm = tc_ydft_smem_bytes(k.tc_np);
+  const bool vec = (k.g.W & 1) == 0;  // two adjacent columns of one coil per 16-byte load
+  if (k.in2) {
+    if (vec)
+      ydft_tc_kernel<true, true><<<gr, TC_THREADS, sm, s>>>(k);
+    else
+      ydft_tc_kernel<true, false><<<gr, TC_THREADS, sm, s>>>(k);
+  } else {
+    if (vec)
+      ydft_tc_kernel<false, true><<<gr, TC_THREADS, sm, s>>>(k);
+    else
+      ydft_tc_kernel<false, false><<<gr, TC_THREADS, sm, s>>>(k);
+  }
 }
 
 }  // namespace avx
