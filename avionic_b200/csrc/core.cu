@@ -1164,15 +1164,67 @@ avx_status coil_b1_from_u_h1(int W, int H, int C, const avx_coil_params& p, cons
   return AVX_OK;
 }
 
-avx_status coil_utgv2(int W, int H, const avx_coil_params& p, const float2* b10, const float2* crec0,
-                      const std::vector<int>& inds, float2* x1, cudaStream_t s) {
-  const int N = W * H;
-  DevBuf<float2> buf;
+// Buffers of one coil-construction loop (UTGV2Recon or B1Recon) and the CUDA
+// graph of its iterations.  Held across the greedy steps of
+// PerformCoilConstruction, which call the same loop with the same sizes
+// eleven times: the buffers are allocated once, and the iterations, whose
+// kernels read every input through the fixed buffers, are captured once and
+// replayed.  A loop used once (the C-ABI entry points, the final B1Recon)
+// launches its iterations directly.
+struct CoilLoop {
+  bool use_graph = false;
+  int N = 0, coils = 0;
+  unsigned iters = 0;
+  DevBuf<float2> buf, xw, Ib;
   DevBuf<int> dind;
-  AVX_CK(buf.alloc((size_t)11 * N));
-  AVX_CK(dind.alloc(inds.size()));
-  AVX_CK(cudaMemcpyAsync(dind.p, inds.data(), inds.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-  AVX_CK(cudaMemsetAsync(buf.p, 0, (size_t)11 * N * sizeof(float2), s));
+  DevBuf<unsigned> umax;
+  cudaGraphExec_t g = nullptr;
+  ~CoilLoop() {
+    if (g) cudaGraphExecDestroy(g);
+  }
+};
+
+// Runs `iters` iterations of the loop through `launch` on stream s: from the
+// loop's graph when it keeps one (captured on the first call), else directly.
+template <class F>
+static avx_status coil_iterate(CoilLoop& l, unsigned iters, cudaStream_t s, F launch) {
+  if (!l.use_graph || s == 0) {
+    for (unsigned it = 0; it < iters; ++it) launch();
+    AVX_CK(cudaGetLastError());
+    return AVX_OK;
+  }
+  if (l.g && l.iters != iters) {
+    cudaGraphExecDestroy(l.g);
+    l.g = nullptr;
+  }
+  if (!l.g) {
+    cudaGraph_t gr;
+    AVX_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    for (unsigned it = 0; it < iters; ++it) launch();
+    AVX_CK(cudaStreamEndCapture(s, &gr));
+    const cudaError_t e = cudaGraphInstantiate(&l.g, gr, 0);
+    cudaGraphDestroy(gr);
+    AVX_CK(e);
+    l.iters = iters;
+  }
+  AVX_CK(cudaGraphLaunch(l.g, s));
+  return AVX_OK;
+}
+
+avx_status coil_utgv2(int W, int H, const avx_coil_params& p, const float2* b10, const float2* crec0,
+                      const std::vector<int>& inds, float2* x1, cudaStream_t s, CoilLoop* loop = nullptr) {
+  const int N = W * H;
+  CoilLoop local;
+  CoilLoop& l = loop ? *loop : local;
+  if (l.N != N) {
+    AVX_CK(l.buf.alloc((size_t)11 * N));
+    AVX_CK(l.xw.alloc(N));
+    AVX_CK(l.Ib.alloc(N));
+    l.N = N;
+  }
+  AVX_CK(l.dind.alloc(std::max<size_t>(inds.size(), 1)));
+  AVX_CK(cudaMemcpyAsync(l.dind.p, inds.data(), inds.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  AVX_CK(cudaMemsetAsync(l.buf.p, 0, (size_t)11 * N * sizeof(float2), s));
   CoilPD a;
   memset(&a, 0, sizeof(a));
   a.W = W;
@@ -1181,40 +1233,46 @@ avx_status coil_utgv2(int W, int H, const avx_coil_params& p, const float2* b10,
   a.tau = p.uTau;
   a.s1 = (float)(1.0 / ((double)p.uAlpha1 * p.uReg));
   a.s2 = (float)(1.0 / ((double)p.uAlpha0 * p.uReg));
-  a.x1 = x1;
-  a.x1n = x1;
-  a.ext1 = buf.p;
-  a.ext1n = buf.p;
+  a.x1 = l.xw.p;
+  a.x1n = l.xw.p;
+  a.ext1 = l.buf.p;
+  a.ext1n = l.buf.p;
   for (int k = 0; k < 2; ++k) {
-    a.x2[k] = buf.p + (size_t)(1 + k) * N;
-    a.ext2[k] = buf.p + (size_t)(3 + k) * N;
+    a.x2[k] = l.buf.p + (size_t)(1 + k) * N;
+    a.ext2[k] = l.buf.p + (size_t)(3 + k) * N;
     a.ext2n[k] = a.ext2[k];
-    a.y1[k] = buf.p + (size_t)(5 + k) * N;
+    a.y1[k] = l.buf.p + (size_t)(5 + k) * N;
   }
-  for (int k = 0; k < 3; ++k) a.y2[k] = buf.p + (size_t)(7 + k) * N;
-  float2* Lw = buf.p + (size_t)10 * N;
-  DevBuf<float2> Ib;
-  AVX_CK(Ib.alloc(N));
+  for (int k = 0; k < 3; ++k) a.y2[k] = l.buf.p + (size_t)(7 + k) * N;
+  float2* Lw = l.buf.p + (size_t)10 * N;
   a.Lw = Lw;
-  a.Ib = Ib.p;
+  a.Ib = l.Ib.p;
+  AVX_CK(cudaMemcpyAsync(l.xw.p, x1, N * sizeof(float2), cudaMemcpyDeviceToDevice, s));
   AVX_CK(cudaMemcpyAsync(a.ext1, x1, N * sizeof(float2), cudaMemcpyDeviceToDevice, s));
-  avx::launch_utgv_prep(b10, crec0, dind.p, (int)inds.size(), p.uTau, N, Lw, Ib.p, s);
-  for (unsigned it = 0; it < p.uNrIt; ++it) avx::launch_utgv_iter(a, s);
+  avx::launch_utgv_prep(b10, crec0, l.dind.p, (int)inds.size(), p.uTau, N, Lw, l.Ib.p, s);
+  avx_status r = coil_iterate(l, p.uNrIt, s, [&] { avx::launch_utgv_iter(a, s); });
+  if (r != AVX_OK) return r;
+  AVX_CK(cudaMemcpyAsync(x1, l.xw.p, N * sizeof(float2), cudaMemcpyDeviceToDevice, s));
   AVX_CK(cudaGetLastError());
   AVX_CK(cudaStreamSynchronize(s));
   return AVX_OK;
 }
 
 avx_status coil_b1_recon(int W, int H, int coils, unsigned max_it, float mu, const avx_coil_params& p,
-                         const float2* u0, const float2* crec, float2* out, cudaStream_t s) {
+                         const float2* u0, const float2* crec, float2* out, cudaStream_t s,
+                         CoilLoop* loop = nullptr) {
   const int N = W * H;
   const size_t CN = (size_t)coils * N;
-  DevBuf<float2> buf;
-  DevBuf<unsigned> umax;
-  AVX_CK(buf.alloc(6 * CN));
-  AVX_CK(umax.alloc(1));
-  AVX_CK(cudaMemsetAsync(buf.p, 0, 6 * CN * sizeof(float2), s));
-  AVX_CK(cudaMemsetAsync(umax.p, 0, sizeof(unsigned), s));
+  CoilLoop local;
+  CoilLoop& l = loop ? *loop : local;
+  if (l.N != N || l.coils != coils) {
+    AVX_CK(l.buf.alloc(6 * CN));
+    AVX_CK(l.umax.alloc(1));
+    l.N = N;
+    l.coils = coils;
+  }
+  AVX_CK(cudaMemsetAsync(l.buf.p, 0, 6 * CN * sizeof(float2), s));
+  AVX_CK(cudaMemsetAsync(l.umax.p, 0, sizeof(unsigned), s));
   CoilPD a;
   memset(&a, 0, sizeof(a));
   a.W = W;
@@ -1222,33 +1280,45 @@ avx_status coil_b1_recon(int W, int H, int coils, unsigned max_it, float mu, con
   a.sigma = p.b1Sigma;
   a.tau = p.b1Tau;
   a.mu = mu;
-  a.x1 = a.x1n = buf.p;
-  a.ext1 = a.ext1n = buf.p + CN;
-  a.y1[0] = buf.p + 2 * CN;
-  a.y1[1] = buf.p + 3 * CN;
-  float2* Lw = buf.p + 4 * CN;
-  float2* Iu = buf.p + 5 * CN;
+  a.x1 = a.x1n = l.buf.p;
+  a.ext1 = a.ext1n = l.buf.p + CN;
+  a.y1[0] = l.buf.p + 2 * CN;
+  a.y1[1] = l.buf.p + 3 * CN;
+  float2* Lw = l.buf.p + 4 * CN;
+  float2* Iu = l.buf.p + 5 * CN;
   a.Lw = Lw;
   a.Ib = Iu;
-  avx::launch_absmax(u0, N, umax.p, s);
-  avx::launch_b1r_prep(u0, umax.p, crec, coils, N, p.b1Tau, Lw, Iu, s);
-  for (unsigned it = 0; it < max_it; ++it) avx::launch_b1r_iter(a, coils, s);
+  avx::launch_absmax(u0, N, l.umax.p, s);
+  avx::launch_b1r_prep(u0, l.umax.p, crec, coils, N, p.b1Tau, Lw, Iu, s);
+  avx_status r = coil_iterate(l, max_it, s, [&] { avx::launch_b1r_iter(a, coils, s); });
+  if (r != AVX_OK) return r;
   avx::launch_b1r_normalize(a.x1, out, N, coils, s);
   AVX_CK(cudaGetLastError());
   AVX_CK(cudaStreamSynchronize(s));
   return AVX_OK;
 }
 
-avx_status abs_sum(const float2* a, const float2* b, int N, cudaStream_t s, double* out) {
-  DevBuf<double> part;
-  AVX_CK(part.alloc(64));
-  avx::launch_abs_sum(a, b, N, part.p, 64, s);
-  std::vector<double> h(64);
-  AVX_CK(cudaMemcpyAsync(h.data(), part.p, 64 * sizeof(double), cudaMemcpyDeviceToHost, s));
+// FP64 sums for the greedy coil order (coil_construction.cpp:55-73, 471-520):
+// out[j] = sum_i |a_i| |crec_{ks[j]},i| (sum_i |crec_{ks[j]},i| when a is null),
+// one reduction per coil into its own partials, one copy back for all of them.
+avx_status abs_sums(const float2* a, const float2* crec, const std::vector<int>& ks, int N, DevBuf<double>& part,
+                    cudaStream_t s, std::vector<double>& out) {
+  constexpr int NB = 64;
+  AVX_CK(part.alloc(std::max<size_t>(ks.size(), 1) * NB));
+  for (size_t j = 0; j < ks.size(); ++j) {
+    const float2* c = crec + (size_t)ks[j] * N;
+    avx::launch_abs_sum(a ? a : c, a ? c : nullptr, N, part.p + j * NB, NB, s);
+  }
+  AVX_CK(cudaGetLastError());
+  std::vector<double> h(ks.size() * NB);
+  AVX_CK(cudaMemcpyAsync(h.data(), part.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
   AVX_CK(cudaStreamSynchronize(s));
-  double acc = 0.0;
-  for (double v : h) acc += v;
-  *out = acc;
+  out.assign(ks.size(), 0.0);
+  for (size_t j = 0; j < ks.size(); ++j) {
+    double acc = 0.0;
+    for (int i = 0; i < NB; ++i) acc += h[j * NB + i];
+    out[j] = acc;
+  }
   return AVX_OK;
 }
 
@@ -1298,78 +1368,99 @@ avx_status coil_time_averaged_radial(int W, int H, int C, int T, int S, const fl
   return AVX_OK;
 }
 
-// PerformCoilConstruction after the time-averaged reconstruction
-// (coil_construction.cpp:447-556): u0 (W*H, replaced by |u0|) and crec (C*W*H)
-avx_status coil_estimate(int W, int H, int C, const avx_coil_params& p, float2* u0p, float2* crecp, float2* u,
-                         float2* b1, cudaStream_t s) {
+avx_status coil_estimate_on(int W, int H, int C, const avx_coil_params& p, float2* u0p, float2* crecp, float2* u,
+                            float2* b1, cudaStream_t s) {
   const int N = W * H;
   DevBuf<float2> absb1, w, uin, cin, x1;
+  DevBuf<double> part;
   AVX_CK(absb1.alloc((size_t)C * N));
   AVX_CK(w.alloc(N));
   AVX_CK(uin.alloc(N));
   AVX_CK(cin.alloc(N));
   AVX_CK(x1.alloc(N));
-  struct {
-    float2* p;
-  } u0{u0p}, crec{crecp};
+  CoilLoop lu, lb;  // the greedy steps' UTGV2 and single-coil B1 loops
+  lu.use_graph = lb.use_graph = true;
+  float2* u0 = u0p;
+  const float2* crec = crecp;
   avx_status r;
-  abs_inplace_kernel<<<(N + 255) / 256, 256, 0, s>>>(u0.p, N);
-  r = coil_b1_from_u_h1(W, H, C, p, u0.p, crec.p, absb1.p, s);
+  abs_inplace_kernel<<<(N + 255) / 256, 256, 0, s>>>(u0, N);
+  r = coil_b1_from_u_h1(W, H, C, p, u0, crec, absb1.p, s);
   if (r != AVX_OK) return r;
   // FindMaximumSum (coil_construction.cpp:55-73)
-  std::vector<int> inds;
+  std::vector<int> inds, all(C);
+  std::vector<double> sums;
+  for (int c = 0; c < C; ++c) all[c] = c;
+  r = abs_sums(nullptr, crec, all, N, part, s, sums);
+  if (r != AVX_OK) return r;
   {
     double best = -1.0;
     int bi = 0;
-    for (int c = 0; c < C; ++c) {
-      double v;
-      r = abs_sum(crec.p + (size_t)c * N, nullptr, N, s, &v);
-      if (r != AVX_OK) return r;
-      if (v > best) {
-        best = v;
+    for (int c = 0; c < C; ++c)
+      if (sums[c] > best) {
+        best = sums[c];
         bi = c;
       }
-    }
     inds.push_back(bi);
   }
   AVX_CK(cudaMemsetAsync(b1, 0, (size_t)C * N * sizeof(float2), s));
   AVX_CK(cudaMemsetAsync(u, 0, (size_t)C * N * sizeof(float2), s));
   AVX_CK(cudaMemcpyAsync(b1 + (size_t)inds[0] * N, absb1.p + (size_t)inds[0] * N, N * sizeof(float2),
                          cudaMemcpyDeviceToDevice, s));
-  r = coil_utgv2(W, H, p, b1, crec.p, inds, u, s);  // u[0] starts at zero
+  r = coil_utgv2(W, H, p, b1, crec, inds, u, s, &lu);  // u[0] starts at zero
   if (r != AVX_OK) return r;
   AVX_CK(cudaMemsetAsync(w.p, 0, N * sizeof(float2), s));
   float2* uMax = u;
   for (int cnt = 1; cnt < C; ++cnt) {
     const int prev = inds[cnt - 1];
     avx::launch_weight_update(w.p, absb1.p + (size_t)prev * N, N, s);
+    std::vector<int> cand;
+    for (int k = 0; k < C; ++k)
+      if (std::find(inds.begin(), inds.end(), k) == inds.end()) cand.push_back(k);
+    r = abs_sums(crec + (size_t)prev * N, crec, cand, N, part, s, sums);
+    if (r != AVX_OK) return r;
     double best = -1.0;
     int mi = -1;
-    for (int k = 0; k < C; ++k) {
-      if (std::find(inds.begin(), inds.end(), k) != inds.end()) continue;
-      double v;
-      r = abs_sum(crec.p + (size_t)prev * N, crec.p + (size_t)k * N, N, s, &v);
-      if (r != AVX_OK) return r;
-      if (v > best) {
-        best = v;
-        mi = k;
+    for (size_t j = 0; j < cand.size(); ++j)
+      if (sums[j] > best) {
+        best = sums[j];
+        mi = cand[j];
       }
-    }
     inds.push_back(mi);
-    avx::launch_greedy_inputs(absb1.p + (size_t)mi * N, u + (size_t)(cnt - 1) * N, w.p, crec.p + (size_t)mi * N,
+    avx::launch_greedy_inputs(absb1.p + (size_t)mi * N, u + (size_t)(cnt - 1) * N, w.p, crec + (size_t)mi * N,
                               uin.p, cin.p, N, s);
-    r = coil_b1_recon(W, H, 1, p.b1NrIt, p.b1Reg, p, uin.p, cin.p, x1.p, s);
+    r = coil_b1_recon(W, H, 1, p.b1NrIt, p.b1Reg, p, uin.p, cin.p, x1.p, s, &lb);
     if (r != AVX_OK) return r;
     avx::launch_phase_apply(absb1.p + (size_t)mi * N, x1.p, b1 + (size_t)mi * N, N, s);
     uMax = u + (size_t)cnt * N;
     AVX_CK(cudaMemcpyAsync(uMax, u + (size_t)(cnt - 1) * N, N * sizeof(float2), cudaMemcpyDeviceToDevice, s));
-    r = coil_utgv2(W, H, p, b1, crec.p, inds, uMax, s);
+    r = coil_utgv2(W, H, p, b1, crec, inds, uMax, s, &lu);
     if (r != AVX_OK) return r;
   }
   // final correction of all coils (coil_construction.cpp:555)
-  r = coil_b1_recon(W, H, C, p.b1FinalNrIt, p.b1FinalReg, p, uMax, crec.p, b1, s);
+  r = coil_b1_recon(W, H, C, p.b1FinalNrIt, p.b1FinalReg, p, uMax, crec, b1, s);
   if (r != AVX_OK) return r;
   AVX_CK(cudaGetLastError());
+  return AVX_OK;
+}
+
+// PerformCoilConstruction after the time-averaged reconstruction
+// (coil_construction.cpp:447-556): u0 (W*H, replaced by |u0|) and crec
+// (C*W*H).  Runs on a stream of its own (the loops' graphs need one), ordered
+// after s, and returns when it is done.
+avx_status coil_estimate(int W, int H, int C, const avx_coil_params& p, float2* u0p, float2* crecp, float2* u,
+                         float2* b1, cudaStream_t s) {
+  cudaStream_t cs;
+  cudaEvent_t ev;
+  AVX_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  AVX_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  AVX_CK(cudaEventRecord(ev, s));
+  AVX_CK(cudaStreamWaitEvent(cs, ev, 0));
+  avx_status r = coil_estimate_on(W, H, C, p, u0p, crecp, u, b1, cs);
+  const cudaError_t e = cudaStreamSynchronize(cs);
+  cudaEventDestroy(ev);
+  cudaStreamDestroy(cs);
+  if (r != AVX_OK) return r;
+  AVX_CK(e);
   return AVX_OK;
 }
 

@@ -165,6 +165,13 @@ void tc_build_ytab(int W, int H, int T, int sx, int sy, const int* rows, const i
   }
 }
 
+// With CAT (3 np <= 128 TMEM columns) the six piece products run as three
+// MMAs per K step that each read their A piece once: A0 x [B0 B1 B2] (N =
+// 3 np), A1 x [B0 B1] (N = 2 np) and A2 x [B0] (N = np) into three column
+// blocks of the accumulator (the coefficient pieces of a stage lie one after
+// another, so the stacked operand is one descriptor); the epilogue adds the
+// blocks.  Without CAT each of the six products is its own MMA of N = np.
+//
 // Producer layout: thread tid owns the tile rows m = 2 (tid % 64) and m + 1
 // (adjacent columns x, x + 1 of one coil when W is even, loaded as one
 // 16-byte vector) and the four image rows 4 g .. 4 g + 3 of every stage,
@@ -174,7 +181,7 @@ void tc_build_ytab(int W, int H, int T, int sx, int sy, const int* rows, const i
 // is double-buffered.  The MMAs of stage s are committed to bar[s % 2]; stage
 // s + 2 waits on that barrier (one lane per warp polls it) before it reuses
 // the A buffer and the coefficient buffer of stage s + 3.
-template <bool U2, bool VEC>
+template <bool U2, bool VEC, bool CAT>
 __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   if (a.st && a.st->stop) return;
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -201,7 +208,8 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   const int c0 = v0 ? mg / W : 0, x0 = v0 ? mg - c0 * W : 0;
   const int c1 = v1 ? (mg + 1) / W : 0, x1 = v1 ? mg + 1 - c1 * W : 0;
   const int HW = W * H;
-  const uint32_t ncols = np <= 32 ? 32u : (np <= 64 ? 64u : 128u);
+  const int acc_cols = CAT ? 3 * np : np;
+  const uint32_t ncols = acc_cols <= 32 ? 32u : (acc_cols <= 64 ? 64u : 128u);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
@@ -293,7 +301,18 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
 #pragma unroll
       for (int i = 0; i < 4; ++i) v[r][i] = cmul(pb[r][i], U2 ? csub(pu[r][i], pw[r][i]) : pu[r][i]);
     if (s + 1 < nst) load_stage(s + 1);
-    // split and store: row mrow + r, core-matrix column grp (k = 8 grp .. 8 grp + 7)
+    // split and store: row mrow + r, core-matrix column grp (k = 8 grp .. 8 grp + 7).
+    // Odd lanes store their second row first, so that each store instruction
+    // of the warp covers all 32 banks evenly.
+    const int odd = lane & 1;
+    if (odd) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float2 tmp = v[0][i];
+        v[0][i] = v[1][i];
+        v[1][i] = tmp;
+      }
+    }
 #pragma unroll
     for (int r = 0; r < 2; ++r) {
       uint32_t re[4][3], im[4][3];
@@ -302,7 +321,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
         split3t(v[r][i].x, re[i]);
         split3t(v[r][i].y, im[i]);
       }
-      const int m = mrow + r;
+      const int m = mrow + (r ^ odd);
       const int off = (m >> 3) * kSBO + grp * kLBO + (m & 7) * 16;
 #pragma unroll
       for (int p = 0; p < 3; ++p)
@@ -322,14 +341,24 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
       const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
 #pragma unroll
       for (int ks = 0; ks < TC_KS / 16; ++ks) {
-        // piece products (pa, pb) with pa + pb <= 2
-        const int pa[6] = {0, 0, 1, 0, 1, 2};
-        const int pbk[6] = {0, 1, 0, 2, 1, 0};
+        if (CAT) {
+          // A_p x [B_0 .. B_{2-p}] into column blocks 0 .. 2-p
 #pragma unroll
-        for (int pr = 0; pr < 6; ++pr) {
-          const uint64_t da = smem_desc(a0 + pa[pr] * kPieceA + ks * 2 * kLBO);
-          const uint64_t db = smem_desc(b0 + pbk[pr] * pieceB + ks * 2 * kLBO);
-          mma_bf16(tmem, da, db, idesc, (s | ks | pr) != 0);
+          for (int p = 0; p < 3; ++p) {
+            const uint64_t da = smem_desc(a0 + p * kPieceA + ks * 2 * kLBO);
+            const uint64_t db = smem_desc(b0 + ks * 2 * kLBO);
+            mma_bf16(tmem, da, db, idesc_bf16((3 - p) * np), (s | ks | p) != 0);
+          }
+        } else {
+          // piece products (pa, pb) with pa + pb <= 2
+          const int pa[6] = {0, 0, 1, 0, 1, 2};
+          const int pbk[6] = {0, 1, 0, 2, 1, 0};
+#pragma unroll
+          for (int pr = 0; pr < 6; ++pr) {
+            const uint64_t da = smem_desc(a0 + pa[pr] * kPieceA + ks * 2 * kLBO);
+            const uint64_t db = smem_desc(b0 + pbk[pr] * pieceB + ks * 2 * kLBO);
+            mma_bf16(tmem, da, db, idesc, (s | ks | pr) != 0);
+          }
         }
       }
       mma_commit(&bar[s & 1]);
@@ -353,6 +382,13 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
     for (int cc = half * ncol_half; cc < (half + 1) * ncol_half; cc += 8) {
       float vv[8];
       tmem_ld(tmem + lane_base + (uint32_t)cc, vv);
+      if (CAT) {
+        float v1[8], v2[8];
+        tmem_ld(tmem + lane_base + (uint32_t)(cc + np), v1);
+        tmem_ld(tmem + lane_base + (uint32_t)(cc + 2 * np), v2);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) vv[i] = (vv[i] + v1[i]) + v2[i];
+      }
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int kk = (cc >> 1) + i;
@@ -638,14 +674,18 @@ void launch_b1_tile_transpose(const float2* b1, float2* b1t, int W, int H, int C
 }
 
 cudaError_t configure_tc_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(ydft_tc_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       AVX_DYN_SMEM_MAX);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(ydft_tc_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(ydft_tc_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(ydft_tc_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
+  cudaError_t e = cudaSuccess;
+  auto attr = [&](const void* f) {
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
+  };
+  attr((const void*)ydft_tc_kernel<false, false, false>);
+  attr((const void*)ydft_tc_kernel<true, false, false>);
+  attr((const void*)ydft_tc_kernel<false, true, false>);
+  attr((const void*)ydft_tc_kernel<true, true, false>);
+  attr((const void*)ydft_tc_kernel<false, false, true>);
+  attr((const void*)ydft_tc_kernel<true, false, true>);
+  attr((const void*)ydft_tc_kernel<false, true, true>);
+  attr((const void*)ydft_tc_kernel<true, true, true>);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(coladj_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
 }
@@ -658,18 +698,21 @@ void launch_coladj_tc(const KArgs& k, float2* img, cudaStream_t s) {
 void launch_ydft_tc(const KArgs& k, cudaStream_t s) {
   dim3 gr((k.g.C * k.g.W + TC_M - 1) / TC_M, k.g.T);
   const size_t sm = tc_ydft_smem_bytes(k.tc_np);
-  const bool vec = (k.g.W & 1) == 0;  // two adjacent columns of one coil per 16-byte load
+  const bool vec = (k.g.W & 1) == 0;   // two adjacent columns of one coil per 16-byte load
+  const bool cat = 3 * k.tc_np <= 128;  // grouped piece products fit 128 TMEM columns
+#define AVX_YDFT_LAUNCH(U2, VEC, CAT) ydft_tc_kernel<U2, VEC, CAT><<<gr, TC_THREADS, sm, s>>>(k)
   if (k.in2) {
     if (vec)
-      ydft_tc_kernel<true, true><<<gr, TC_THREADS, sm, s>>>(k);
+      cat ? AVX_YDFT_LAUNCH(true, true, true) : AVX_YDFT_LAUNCH(true, true, false);
     else
-      ydft_tc_kernel<true, false><<<gr, TC_THREADS, sm, s>>>(k);
+      cat ? AVX_YDFT_LAUNCH(true, false, true) : AVX_YDFT_LAUNCH(true, false, false);
   } else {
     if (vec)
-      ydft_tc_kernel<false, true><<<gr, TC_THREADS, sm, s>>>(k);
+      cat ? AVX_YDFT_LAUNCH(false, true, true) : AVX_YDFT_LAUNCH(false, true, false);
     else
-      ydft_tc_kernel<false, false><<<gr, TC_THREADS, sm, s>>>(k);
+      cat ? AVX_YDFT_LAUNCH(false, false, true) : AVX_YDFT_LAUNCH(false, false, false);
   }
+#undef AVX_YDFT_LAUNCH
 }
 
 }  // namespace avx

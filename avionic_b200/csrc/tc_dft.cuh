@@ -15,7 +15,7 @@
 #define TC_THREADS 256  // threads per CTA
 #define TC_MAX_NP 96    // largest MMA N of the y-transform / K of the adjoint (48 sampled rows
                         // per frame): the adjoint's shared memory, 2304 kc bytes, stays within 227 KB
-#define CA_TC_XT 16     // image columns per tile of the tensor-core column adjoint
+#define CA_TC_XT 8      // image columns per tile of the tensor-core column adjoint (16 coils per MMA)
 
 namespace avx {
 
