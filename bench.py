@@ -318,8 +318,21 @@ def run_batched(av, torch, workers, n=64, iters=800, rank=0, world=1, dist=None)
         forms[name]["oracle_instances"] = int(sum_over_ranks(dist, len(errs), "cuda"))
     del items, outs
     torch.cuda.empty_cache()
+    # the whole set's compulsory HBM traffic (each field read and written once per iteration, k-space at
+    # its sampled rows) at the measured copy bandwidth: the time no form can beat
+    peak, _ = load_peaks()
+    ideal_bytes = 0
+    for sp in specs:
+        Ns = sp["W"] * sp["H"] * sp["T"]
+        rows = sp["T"] * max(1, int(round(sp["H"] / sp["R"])))
+        Ss = sp["C"] * rows * sp["W"]
+        ideal_bytes += 8 * (4 * 4 * Ns + 2 * 9 * Ns + 3 * Ss) + 8 * sp["C"] * sp["W"] * sp["H"] + 4 * rows * sp["W"]
+    ideal_s = ideal_bytes * iters / (peak * 1e9) / world
+    for name in forms:
+        forms[name]["frac_of_hbm_roofline"] = ideal_s / forms[name]["wall_s"]
     return {"workload": "%d TGV2 Cartesian reconstructions of uneven size (matrix 96-320, frames 8-48, coils 4-32, "
                         "acceleration 6-16), %d iterations each, submitted at once" % (n, iters),
+            "hbm_roofline_s": ideal_s,
             "forms": forms,
             "speedup_split_batched_vs_plain_fp32_single": forms["split_batched"]["recons_per_s"] /
             forms["plain_fp32_single"]["recons_per_s"],
@@ -363,11 +376,14 @@ def run_serving(av, torch, workers, n, rates, max_it=1500, rel_gap=1e-4):
         for rate in rates:
             comps, o, wall = _batch_pass(av, torch, items, make_request, w, dft, arrivals=unit_arrivals / rate)
             lat = [c.queue_ms + c.run_ms for c in comps]
+            gaps = [c.stats.last_gap for c in comps if c.stats.gap_count > 0]
             per_rate.append({"rate_req_per_s": rate, "recons_per_s": n / wall, "wall_s": wall,
                              "latency_ms": {q: float(np.percentile(lat, v)) for q, v in
                                             (("p50", 50), ("p95", 95), ("p99", 99))},
                              "iterations_mean": float(np.mean([c.stats.iterations for c in comps])),
-                             "stopped_by_gap": int(sum(c.stats.stopped_by_gap for c in comps))})
+                             "stopped_by_gap": int(sum(c.stats.stopped_by_gap for c in comps)),
+                             "last_normalised_gap": {"min": float(np.min(gaps)), "p50": float(np.median(gaps))}
+                             if gaps else None})
             outs[name] = o
         res[name] = {"workers": w, "per_rate": per_rate}
     res["max_rel_l2_split_batched_vs_plain_fp32"] = max(
@@ -612,7 +628,7 @@ def main():
     ap.add_argument("--batch-workers", type=int, default=64,
                     help="requests the engine advances together in the batched and served forms")
     ap.add_argument("--batch-size", type=int, default=64)
-    ap.add_argument("--serve-requests", type=int, default=24,
+    ap.add_argument("--serve-requests", type=int, default=48,
                     help="requests per rate (bounded sample of the 2000-request stream)")
     ap.add_argument("--serve-rates", default="20,200",
                     help="comma list of arrival rates in requests/s (the configuration sweeps 20-200)")
