@@ -25,7 +25,6 @@ namespace {
 
 constexpr int kLBO = 128;  // bytes between core matrices adjacent along K
 constexpr int kSBO = 512;  // bytes between 8-row groups (TC_KS / 8 core matrices)
-constexpr int kPieceA = TC_M * TC_KS * 2;
 constexpr unsigned kWaitLimit = 1u << 22;  // mbarrier polls before giving up
 
 AVX_D uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -114,7 +113,7 @@ AVX_D uint32_t packhi(uint32_t lo, uint32_t hi) { return __byte_perm(lo, hi, 0x7
 
 size_t tc_ytab_bytes(int H, int T, int np) { return (size_t)T * tc_nstage(H) * 3 * tc_piece_bytes(np); }
 
-size_t tc_ydft_smem_bytes(int np) { return 2 * (size_t)3 * kPieceA + 3 * (size_t)3 * tc_piece_bytes(np) + 64; }
+size_t tc_ydft_smem_bytes(int np) { return 3 * (size_t)3 * tc_piece_bytes(np) + 64; }
 
 static unsigned short host_bf16(float f) {
   uint32_t u;
@@ -165,23 +164,34 @@ void tc_build_ytab(int W, int H, int T, int sx, int sy, const int* rows, const i
   }
 }
 
-// With CAT (3 np <= 128 TMEM columns) the six piece products run as three
-// MMAs per K step that each read their A piece once: A0 x [B0 B1 B2] (N =
-// 3 np), A1 x [B0 B1] (N = 2 np) and A2 x [B0] (N = np) into three column
-// blocks of the accumulator (the coefficient pieces of a stage lie one after
-// another, so the stacked operand is one descriptor); the epilogue adds the
-// blocks.  Without CAT each of the six products is its own MMA of N = np.
-//
-// Producer layout: thread tid owns the tile rows m = 2 (tid % 64) and m + 1
-// (adjacent columns x, x + 1 of one coil when W is even, loaded as one
-// 16-byte vector) and the four image rows 4 g .. 4 g + 3 of every stage,
-// g = tid / 64, which fill core-matrix column g of the stage's A tile.  The
-// coefficient pieces run through a three-stage ring filled one stage ahead by
-// cp.async, so their L2 latency hides behind the production of A; A itself
-// is double-buffered.  The MMAs of stage s are committed to bar[s % 2]; stage
-// s + 2 waits on that barrier (one lane per warp polls it) before it reuses
-// the A buffer and the coefficient buffer of stage s + 3.
-template <bool U2, bool VEC, bool CAT>
+// A operand in tensor memory.  Warp w owns TMEM lane quadrant q = w % 4, so
+// thread (w, lane) produces tile row m = 32 q + lane, image rows 8 kh .. 8 kh
+// + 7 of every stage (kh = w / 4, the stage's K step kh), and writes the three
+// bf16 pieces of its 16 K values with one tcgen05.st each: A never touches
+// shared memory, and the MMAs read it from TMEM.  TMEM columns: the fp32
+// accumulator [0, np), then per A buffer b, K step ks and piece p the 8
+// columns (16 bf16 per lane) at np_al + ((2 b + ks) 3 + p) 8.  The
+// coefficient pieces (B) run through a three-stage shared-memory ring filled
+// one stage ahead by cp.async.  The MMAs of stage s are committed to
+// bar[s % 2]; stage s + 2 waits on that barrier (one lane per warp polls it)
+// before it overwrites the A buffer and the coefficient buffer of stage s + 3.
+AVX_D void tmem_st8(uint32_t taddr, const uint32_t (&v)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+               "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+               : "memory");
+}
+
+// D (tmem) += A (tmem) x B (smem descriptor)^T, kind::f16
+AVX_D void mma_bf16_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+template <bool U2>
 __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   if (a.st && a.st->stop) return;
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -193,23 +203,20 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   if (S == 0) return;
   const int np = a.tc_np;
   const int pieceB = tc_piece_bytes(np);
-  const int stageA = 3 * kPieceA, stageB = 3 * pieceB;
-  unsigned char* sA = smem;               // 2 stages
-  unsigned char* sB = smem + 2 * stageA;  // 3 stages
+  const int stageB = 3 * pieceB;
+  unsigned char* sB = smem;  // 3 stages
   uint64_t* bar = reinterpret_cast<uint64_t*>(sB + 3 * stageB);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int half = tid >> 7;  // epilogue: TMEM column half
-  const int rp = tid & 63, grp = tid >> 6;
-  const int mrow = 2 * rp;                      // first of this thread's two tile rows
-  const int mg = blockIdx.x * TC_M + mrow;      // global (c, x) row index
+  const int q = warp & 3, kh = warp >> 2;
+  const int m = 32 * q + lane;              // tile row of this thread
+  const int mg = blockIdx.x * TC_M + m;     // global (c, x) row index
   const int CW = C * W;
-  const bool v0 = mg < CW, v1 = mg + 1 < CW;
-  const int c0 = v0 ? mg / W : 0, x0 = v0 ? mg - c0 * W : 0;
-  const int c1 = v1 ? (mg + 1) / W : 0, x1 = v1 ? mg + 1 - c1 * W : 0;
+  const bool valid = mg < CW;
+  const int c = valid ? mg / W : 0, x = valid ? mg - c * W : 0;
   const int HW = W * H;
-  const int acc_cols = CAT ? 3 * np : np;
-  const uint32_t ncols = acc_cols <= 32 ? 32u : (acc_cols <= 64 ? 64u : 128u);
+  const int np_al = (np + 7) & ~7;
+  const uint32_t ncols = np_al + 96 <= 128 ? 128u : 256u;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
@@ -227,14 +234,11 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   tc_fence_after();
   const uint32_t tmem = *tslot;
   const uint32_t idesc = idesc_bf16(np);
+  const uint32_t lane_base = (uint32_t)(q * 32) << 16;
 
-  // this thread's columns: image rows are W apart
-  const float2* __restrict__ pb0 = a.b1 + (long long)c0 * HW + x0;
-  const float2* __restrict__ pb1 = a.b1 + (long long)c1 * HW + x1;
-  const float2* __restrict__ pu0 = a.in + (long long)t * HW + x0;
-  const float2* __restrict__ pu1 = a.in + (long long)t * HW + x1;
-  const float2* __restrict__ pw0 = U2 ? a.in2 + (long long)t * HW + x0 : nullptr;
-  const float2* __restrict__ pw1 = U2 ? a.in2 + (long long)t * HW + x1 : nullptr;
+  const float2* __restrict__ pb = a.b1 + (long long)c * HW + x;
+  const float2* __restrict__ pu = a.in + (long long)t * HW + x;
+  const float2* __restrict__ pw = U2 ? a.in2 + (long long)t * HW + x : nullptr;
   const uint4* __restrict__ btab = a.tc_ytab + (size_t)t * tc_nstage(H) * 3 * (pieceB / 16);
   const int nst = tc_nstage(H);
   const int nbt = stageB / 16;
@@ -248,120 +252,74 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
 
-  // register prefetch of one stage: b1 and u (, u2) of both columns at 4 image rows
-  float2 pb[2][4], pu[2][4], pw[2][U2 ? 4 : 1];
+  // register prefetch of one stage: b1 and u (, u2) at this thread's 8 image rows
+  float2 rb[8], ru[8], rw[U2 ? 8 : 1];
   auto load_stage = [&](int st) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int y = st * (TC_KS / 2) + 4 * grp + i;
-      const bool in = y < H;
+    for (int i = 0; i < 8; ++i) {
+      const int y = st * (TC_KS / 2) + 8 * kh + i;
+      const bool in = valid && y < H;
       const int off = y * W;
-      if (VEC) {
-        // W even: x0 even and x1 = x0 + 1 in the same coil, 16-byte aligned
-        const float4 zb = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 qb = (in && v0) ? __ldg(reinterpret_cast<const float4*>(pb0 + off)) : zb;
-        const float4 qu = (in && v0) ? *reinterpret_cast<const float4*>(pu0 + off) : zb;
-        pb[0][i] = make_float2(qb.x, qb.y);
-        pb[1][i] = make_float2(qb.z, qb.w);
-        pu[0][i] = make_float2(qu.x, qu.y);
-        pu[1][i] = make_float2(qu.z, qu.w);
-        if (U2) {
-          const float4 qw = (in && v0) ? *reinterpret_cast<const float4*>(pw0 + off) : zb;
-          pw[0][i] = make_float2(qw.x, qw.y);
-          pw[1][i] = make_float2(qw.z, qw.w);
-        }
-      } else {
-        pb[0][i] = (in && v0) ? __ldg(pb0 + off) : czero();
-        pb[1][i] = (in && v1) ? __ldg(pb1 + off) : czero();
-        pu[0][i] = (in && v0) ? pu0[off] : czero();
-        pu[1][i] = (in && v1) ? pu1[off] : czero();
-        if (U2) {
-          pw[0][i] = (in && v0) ? pw0[off] : czero();
-          pw[1][i] = (in && v1) ? pw1[off] : czero();
-        }
-      }
+      rb[i] = in ? __ldg(pb + off) : czero();
+      ru[i] = in ? pu[off] : czero();
+      if (U2) rw[i] = in ? pw[off] : czero();
     }
   };
 
   issue_b(0);
   load_stage(0);
   for (int s = 0; s < nst; ++s) {
-    unsigned char* sa = sA + (s & 1) * stageA;
+    const int buf = s & 1;
     unsigned char* sb = sB + (s % 3) * stageB;
     if (s >= 2) {
       // MMAs of stage s - 2 done: its A buffer and the coefficient buffer of stage s + 1 are free
       bool w = true;
-      if (lane == 0) w = mbar_wait(&bar[s & 1], (uint32_t)((s - 2) >> 1) & 1u);
+      if (lane == 0) w = mbar_wait(&bar[buf], (uint32_t)((s - 2) >> 1) & 1u);
       ok = __shfl_sync(0xffffffffu, w ? 1 : 0, 0) && ok;
     }
     if (s + 1 < nst) issue_b(s + 1);
-    float2 v[2][4];
+    float2 v[8];
 #pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-      for (int i = 0; i < 4; ++i) v[r][i] = cmul(pb[r][i], U2 ? csub(pu[r][i], pw[r][i]) : pu[r][i]);
+    for (int i = 0; i < 8; ++i) v[i] = cmul(rb[i], U2 ? csub(ru[i], rw[i]) : ru[i]);
     if (s + 1 < nst) load_stage(s + 1);
-    // split and store: row mrow + r, core-matrix column grp (k = 8 grp .. 8 grp + 7).
-    // Odd lanes store their second row first, so that each store instruction
-    // of the warp covers all 32 banks evenly.
-    const int odd = lane & 1;
-    if (odd) {
+    // split: word i of piece p holds (re, im) of image row 8 kh + i, i.e. K = 16 kh + 2 i, + 1
+    uint32_t pw3[3][8];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const float2 tmp = v[0][i];
-        v[0][i] = v[1][i];
-        v[1][i] = tmp;
-      }
+    for (int i = 0; i < 8; ++i) {
+      uint32_t re[3], im[3];
+      split3t(v[i].x, re);
+      split3t(v[i].y, im);
+#pragma unroll
+      for (int p = 0; p < 3; ++p) pw3[p][i] = packhi(re[p], im[p]);
     }
+    const uint32_t acol = (uint32_t)(np_al + ((2 * buf + kh) * 3) * 8);
 #pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      uint32_t re[4][3], im[4][3];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        split3t(v[r][i].x, re[i]);
-        split3t(v[r][i].y, im[i]);
-      }
-      const int m = mrow + (r ^ odd);
-      const int off = (m >> 3) * kSBO + grp * kLBO + (m & 7) * 16;
-#pragma unroll
-      for (int p = 0; p < 3; ++p)
-        *reinterpret_cast<uint4*>(sa + p * kPieceA + off) =
-            make_uint4(packhi(re[0][p], im[0][p]), packhi(re[1][p], im[1][p]), packhi(re[2][p], im[2][p]),
-                       packhi(re[3][p], im[3][p]));
-    }
+    for (int p = 0; p < 3; ++p) tmem_st8(tmem + lane_base + acol + (uint32_t)(p * 8), pw3[p]);
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
     // this stage's coefficients have landed (the next stage's may be in flight)
     if (s + 1 < nst)
       asm volatile("cp.async.wait_group 1;" ::: "memory");
     else
       asm volatile("cp.async.wait_group 0;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
     __syncthreads();
     if (tid == 0) {
       tc_fence_after();
-      const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
+      const uint32_t b0 = smem_u32(sb);
 #pragma unroll
       for (int ks = 0; ks < TC_KS / 16; ++ks) {
-        if (CAT) {
-          // A_p x [B_0 .. B_{2-p}] into column blocks 0 .. 2-p
+        // piece products (pa, pb) with pa + pb <= 2
+        const int pa[6] = {0, 0, 1, 0, 1, 2};
+        const int pbk[6] = {0, 1, 0, 2, 1, 0};
 #pragma unroll
-          for (int p = 0; p < 3; ++p) {
-            const uint64_t da = smem_desc(a0 + p * kPieceA + ks * 2 * kLBO);
-            const uint64_t db = smem_desc(b0 + ks * 2 * kLBO);
-            mma_bf16(tmem, da, db, idesc_bf16((3 - p) * np), (s | ks | p) != 0);
-          }
-        } else {
-          // piece products (pa, pb) with pa + pb <= 2
-          const int pa[6] = {0, 0, 1, 0, 1, 2};
-          const int pbk[6] = {0, 1, 0, 2, 1, 0};
-#pragma unroll
-          for (int pr = 0; pr < 6; ++pr) {
-            const uint64_t da = smem_desc(a0 + pa[pr] * kPieceA + ks * 2 * kLBO);
-            const uint64_t db = smem_desc(b0 + pbk[pr] * pieceB + ks * 2 * kLBO);
-            mma_bf16(tmem, da, db, idesc, (s | ks | pr) != 0);
-          }
+        for (int pr = 0; pr < 6; ++pr) {
+          const uint32_t ta = tmem + (uint32_t)(np_al + ((2 * buf + ks) * 3 + pa[pr]) * 8);
+          const uint64_t db = smem_desc(b0 + pbk[pr] * pieceB + ks * 2 * kLBO);
+          mma_bf16_ta(tmem, ta, db, idesc, (s | ks | pr) != 0);
         }
       }
-      mma_commit(&bar[s & 1]);
+      mma_commit(&bar[buf]);
     }
   }
   const int last = nst - 1;
@@ -371,24 +329,12 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   if (!__all_sync(0xffffffffu, ok)) {
     if (a.st && lane == 0) atomicExch(&a.st->err, 2);
   } else {
-    // epilogue: TMEM lane (warp % 4) * 32 + laneid = tile row m; this half's columns
-    const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+    // epilogue: this thread's row m, columns of its half (kh) of the accumulator
     const int ncol_half = np / 2;
-    const int m = (warp & 3) * 32 + lane;
-    const int me = blockIdx.x * TC_M + m;
-    const bool valid = me < CW;
-    const int ce = valid ? me / W : 0, xe = valid ? me - ce * W : 0;
-    float2* out = a.qp + kbase(g, t, ce, r0, r1) + xe;
-    for (int cc = half * ncol_half; cc < (half + 1) * ncol_half; cc += 8) {
+    float2* out = a.qp + kbase(g, t, c, r0, r1) + x;
+    for (int cc = kh * ncol_half; cc < (kh + 1) * ncol_half; cc += 8) {
       float vv[8];
       tmem_ld(tmem + lane_base + (uint32_t)cc, vv);
-      if (CAT) {
-        float v1[8], v2[8];
-        tmem_ld(tmem + lane_base + (uint32_t)(cc + np), v1);
-        tmem_ld(tmem + lane_base + (uint32_t)(cc + 2 * np), v2);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) vv[i] = (vv[i] + v1[i]) + v2[i];
-      }
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const int kk = (cc >> 1) + i;
@@ -674,18 +620,10 @@ void launch_b1_tile_transpose(const float2* b1, float2* b1t, int W, int H, int C
 }
 
 cudaError_t configure_tc_kernels() {
-  cudaError_t e = cudaSuccess;
-  auto attr = [&](const void* f) {
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
-  };
-  attr((const void*)ydft_tc_kernel<false, false, false>);
-  attr((const void*)ydft_tc_kernel<true, false, false>);
-  attr((const void*)ydft_tc_kernel<false, true, false>);
-  attr((const void*)ydft_tc_kernel<true, true, false>);
-  attr((const void*)ydft_tc_kernel<false, false, true>);
-  attr((const void*)ydft_tc_kernel<true, false, true>);
-  attr((const void*)ydft_tc_kernel<false, true, true>);
-  attr((const void*)ydft_tc_kernel<true, true, true>);
+  cudaError_t e = cudaFuncSetAttribute(ydft_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       AVX_DYN_SMEM_MAX);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(ydft_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(coladj_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
 }
@@ -698,21 +636,10 @@ void launch_coladj_tc(const KArgs& k, float2* img, cudaStream_t s) {
 void launch_ydft_tc(const KArgs& k, cudaStream_t s) {
   dim3 gr((k.g.C * k.g.W + TC_M - 1) / TC_M, k.g.T);
   const size_t sm = tc_ydft_smem_bytes(k.tc_np);
-  const bool vec = (k.g.W & 1) == 0;   // two adjacent columns of one coil per 16-byte load
-  const bool cat = 3 * k.tc_np <= 128;  // grouped piece products fit 128 TMEM columns
-#define AVX_YDFT_LAUNCH(U2, VEC, CAT) ydft_tc_kernel<U2, VEC, CAT><<<gr, TC_THREADS, sm, s>>>(k)
-  if (k.in2) {
-    if (vec)
-      cat ? AVX_YDFT_LAUNCH(true, true, true) : AVX_YDFT_LAUNCH(true, true, false);
-    else
-      cat ? AVX_YDFT_LAUNCH(true, false, true) : AVX_YDFT_LAUNCH(true, false, false);
-  } else {
-    if (vec)
-      cat ? AVX_YDFT_LAUNCH(false, true, true) : AVX_YDFT_LAUNCH(false, true, false);
-    else
-      cat ? AVX_YDFT_LAUNCH(false, false, true) : AVX_YDFT_LAUNCH(false, false, false);
-  }
-#undef AVX_YDFT_LAUNCH
+  if (k.in2)
+    ydft_tc_kernel<true><<<gr, TC_THREADS, sm, s>>>(k);
+  else
+    ydft_tc_kernel<false><<<gr, TC_THREADS, sm, s>>>(k);
 }
 
 }  // namespace avx
