@@ -20,6 +20,7 @@
 #include <condition_variable>
 #include <deque>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <tuple>
@@ -685,8 +686,16 @@ struct TuneKey {
     return std::tie(dev, method, W, H, T) < std::tie(o.dev, o.method, o.W, o.H, o.T);
   }
 };
+// one entry per shape: the map's lock covers lookups only, and each shape's
+// own lock is held while that shape is tuned, so shapes tune in parallel and
+// solvers of one shape on several threads all take the one choice
+struct TuneEntry {
+  std::mutex mu;
+  bool done = false;
+  int primal_tile = 0, dual_block = 0;
+};
 static std::mutex g_tune_mu;
-static std::map<TuneKey, std::pair<int, int>> g_tune;
+static std::map<TuneKey, std::unique_ptr<TuneEntry>> g_tune;
 
 static avx_status time_launches(avx_solver* s, void (*launch)(int, const PDArgs&, cudaStream_t), const PDArgs& a,
                                 float* ms) {
@@ -709,13 +718,17 @@ static avx_status autotune(avx_solver* s) {
   int dev = 0;
   AVX_CK(cudaGetDevice(&dev));
   const TuneKey key{dev, s->method, s->W, s->H, s->T};
-  // held while tuning, so that solvers of one shape on several threads (the
-  // batch engine's workers) all take the one choice
-  std::lock_guard<std::mutex> lk(g_tune_mu);
-  auto it = g_tune.find(key);
-  if (it != g_tune.end()) {
-    s->primal_tile = it->second.first;
-    s->dual_block = it->second.second;
+  TuneEntry* ent;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    std::unique_ptr<TuneEntry>& slot = g_tune[key];
+    if (!slot) slot.reset(new TuneEntry());
+    ent = slot.get();
+  }
+  std::lock_guard<std::mutex> lk(ent->mu);
+  if (ent->done) {
+    s->primal_tile = ent->primal_tile;
+    s->dual_block = ent->dual_block;
     s->tuned = true;
     return AVX_OK;
   }
@@ -743,7 +756,9 @@ static avx_status autotune(avx_solver* s) {
     }
   }
   s->tuned = true;
-  g_tune[key] = {s->primal_tile, s->dual_block};
+  ent->primal_tile = s->primal_tile;
+  ent->dual_block = s->dual_block;
+  ent->done = true;
   return AVX_OK;
 }
 
@@ -1436,8 +1451,11 @@ avx_status coil_estimate_on(int W, int H, int C, const avx_coil_params& p, float
     r = coil_utgv2(W, H, p, b1, crec, inds, uMax, s, &lu);
     if (r != AVX_OK) return r;
   }
-  // final correction of all coils (coil_construction.cpp:555)
-  r = coil_b1_recon(W, H, C, p.b1FinalNrIt, p.b1FinalReg, p, uMax, crec, b1, s);
+  // final correction of all coils (coil_construction.cpp:555), its 1000
+  // iterations replayed from one graph as well
+  CoilLoop lf;
+  lf.use_graph = true;
+  r = coil_b1_recon(W, H, C, p.b1FinalNrIt, p.b1FinalReg, p, uMax, crec, b1, s, &lf);
   if (r != AVX_OK) return r;
   AVX_CK(cudaGetLastError());
   return AVX_OK;
