@@ -1451,11 +1451,9 @@ avx_status coil_estimate_on(int W, int H, int C, const avx_coil_params& p, float
     r = coil_utgv2(W, H, p, b1, crec, inds, uMax, s, &lu);
     if (r != AVX_OK) return r;
   }
-  // final correction of all coils (coil_construction.cpp:555), its 1000
-  // iterations replayed from one graph as well
-  CoilLoop lf;
-  lf.use_graph = true;
-  r = coil_b1_recon(W, H, C, p.b1FinalNrIt, p.b1FinalReg, p, uMax, crec, b1, s, &lf);
+  // final correction of all coils (coil_construction.cpp:555); run once, so
+  // its iterations launch directly (capturing them would cost more than it saves)
+  r = coil_b1_recon(W, H, C, p.b1FinalNrIt, p.b1FinalReg, p, uMax, crec, b1, s);
   if (r != AVX_OK) return r;
   AVX_CK(cudaGetLastError());
   return AVX_OK;

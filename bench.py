@@ -626,7 +626,10 @@ def main():
                     help="comma list: headline (the 192x192x30 cine ICTGV2 line), tv128, radial, batched, serving "
                          "(added to the line at N=1; batched at every N)")
     ap.add_argument("--batch-workers", type=int, default=64,
-                    help="requests the engine advances together in the batched and served forms")
+                    help="requests the engine advances together in the batched form")
+    ap.add_argument("--serve-workers", type=int, default=16,
+                    help="requests the engine advances together in the served form (fewer finish in arrival order "
+                         "sooner; more overlap small requests)")
     ap.add_argument("--batch-size", type=int, default=64)
     ap.add_argument("--serve-requests", type=int, default=48,
                     help="requests per rate (bounded sample of the 2000-request stream)")
@@ -661,7 +664,7 @@ def main():
     if world == 1 and "radial" in parts:
         extra["radial"] = run_radial(av, torch)
     if world == 1 and "serving" in parts:
-        extra["serving"] = run_serving(av, torch, args.batch_workers, args.serve_requests,
+        extra["serving"] = run_serving(av, torch, args.serve_workers, args.serve_requests,
                                        [float(r) for r in args.serve_rates.split(",")])
     if "headline" not in parts:
         if dist is not None:
