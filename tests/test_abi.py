@@ -99,3 +99,20 @@ def test_struct_layouts_match_the_header(tmp_path):
         assert got[(ctype, "sizeof")] == ctypes.sizeof(cls), ctype
         for fname, _ in cls._fields_:
             assert got[(ctype, fname)] == getattr(cls, fname).offset, (ctype, fname)
+
+
+def test_generators_import_without_the_library():
+    """The numpy problem generators (and so the CPU reference arm of the
+    bench) run in a process that never loads libavionic_core.so; the first
+    library name used through the package loads it."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "from avionic_b200 import synth\n"
+            "p = synth.small(1)\n"
+            "assert 'avionic_b200.api' not in sys.modules\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'libavionic_core' not in maps\n"
+            "print('ok')\n") % ROOT
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0 and out.stdout.strip() == "ok", out.stderr
