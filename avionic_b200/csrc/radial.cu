@@ -17,6 +17,7 @@ namespace avx {
 #define RAD_FFT_KC 16
 #define RAD_ADJ_KC 8  // image rows per CTA of the adjoint's fused row pass
 #define RAD_SPREAD_BATCH 64
+#define RAD_MAX_SW 32  // largest sector width (the operator accepts 2..32; one thread per cell)
 
 // tapered Kaiser-Bessel weight at offset u (grid units); zero for |u| >= J/2
 AVX_D float kbw(float u, const RadialGeomDev& g) {
@@ -275,7 +276,9 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
   __shared__ int s_g0x[NB], s_g0y[NB];
   __shared__ float s_wx[NW][NBP], s_wy[NW][NBP];
   __shared__ float2 s_v[CC][NB];
-  __shared__ unsigned long long s_mask[2];  // staged samples whose window reaches this sector
+  // per sector row: the staged samples whose window covers that row (two
+  // batches' worth, alternating), so that a cell visits only those
+  __shared__ unsigned long long s_rowm[2][RAD_MAX_SW];
   const int f = blockIdx.y;
   const int sec = blockIdx.x;
   const int sxi = sec % g.nsx, syi = sec / g.nsx;
@@ -313,14 +316,14 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
       }
     s_nr = nr;
     s_tot = tot;
-    s_mask[0] = s_mask[1] = 0ull;
   }
+  for (int i = threadIdx.x; i < RAD_MAX_SW; i += blockDim.x) s_rowm[0][i] = s_rowm[1][i] = 0ull;
   __syncthreads();
   const int nr = s_nr, tot = s_tot;
   // the sector's cells, per axis: window offsets (cell - g0) mod G run over
   // [d0, d0 + sw); the window reaches them when one of those is below NW
   const int swx = min(g.sw, g.Gx - X0), swy = min(g.sw, g.Gy - Y0);
-  int bi = 0;  // batch counter over all coil passes (selects s_mask)
+  int bi = 0;  // batch counter over all coil passes (selects s_rowm)
   for (int c0 = 0; c0 < g.C; c0 += CC) {
     const int cc = min(CC, g.C - c0);
     float2 acc[CC];
@@ -328,7 +331,7 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
     for (int k = 0; k < CC; ++k) acc[k] = czero();
     for (int b0 = 0; b0 < tot; b0 += NB, ++bi) {
       const int nb = min(NB, tot - b0);
-      unsigned long long* mask = &s_mask[bi & 1];
+      unsigned long long* rowm = s_rowm[bi & 1];
       __syncthreads();
       for (int e = threadIdx.x; e < nb; e += blockDim.x) {
         int q = b0 + e, k = 0;
@@ -339,7 +342,12 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
         const int dx0 = wrap1(X0 - g0.x, g.Gx), dy0 = wrap1(Y0 - g0.y, g.Gy);
         const bool hit = (dx0 < NW || dx0 + swx > g.Gx) && (dy0 < NW || dy0 + swy > g.Gy);
         if (!hit) continue;
-        atomicOr(mask, 1ull << e);  // bitwise OR: the result does not depend on the order
+        // the sector rows the window covers (bitwise OR: the result does not depend on the order)
+#pragma unroll
+        for (int o = 0; o < NW; ++o) {
+          const int ly = wrap1(g0.y + o, g.Gy) - Y0;
+          if (ly >= 0 && ly < swy) atomicOr(&rowm[ly], 1ull << e);
+        }
         s_g0x[e] = g0.x;
         s_g0y[e] = g0.y;
 #pragma unroll
@@ -353,11 +361,12 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
           s_v[kc][e] = kc < cc ? cscale(samples[((long long)f * g.C + c0 + kc) * g.S + j], sc) : czero();
       }
       __syncthreads();
-      unsigned long long m = *mask;
-      // the other mask is free again (every thread read it before this batch's first barrier)
-      if (threadIdx.x == 0) s_mask[(bi + 1) & 1] = 0ull;
+      unsigned long long m = active ? rowm[ly] : 0ull;
+      // the other batch's row masks are free again (every thread read them
+      // before this batch's first barrier)
+      for (int i = threadIdx.x; i < RAD_MAX_SW; i += blockDim.x) s_rowm[(bi + 1) & 1][i] = 0ull;
       if (!active) continue;
-      while (m) {  // staged samples in order
+      while (m) {  // the staged samples covering this row, in staging order
         const int e = __ffsll((long long)m) - 1;
         m &= m - 1;
         // window starts lie within J of the grid, so one wrap suffices
