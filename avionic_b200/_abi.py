@@ -65,6 +65,7 @@ SIGNATURES = {
     "avx_operator_backward": (I, [VP, VP, VP, VP]),
     "avx_operator_forward": (I, [VP, VP, VP, VP]),
     "avx_operator_adapt_lambda": (I, [VP, F, F, C.POINTER(F)]),
+    "avx_operator_opnorm": (I, [VP, VP, VP, U, C.POINTER(D), C.POINTER(D)]),
     "avx_operator_destroy": (None, [VP]),
     "avx_default_params": (I, [I, C.POINTER(PDParams)]),
     "avx_solver_create": (I, [I, U, U, U, U, C.POINTER(PDParams), VP, C.POINTER(VP)]),
@@ -79,6 +80,7 @@ SIGNATURES = {
     "avx_solver_run": (I, [VP, VP, VP, VP]),
     "avx_solver_adapt_step_size": (I, [VP, C.POINTER(VP), VP]),
     "avx_solver_compute_gap": (I, [VP, C.POINTER(VP), C.POINTER(VP), VP, VP, VP, C.POINTER(D), C.POINTER(D)]),
+    "avx_solver_opnorm": (I, [VP, VP, VP, U, I, C.POINTER(D), C.POINTER(D)]),
     "avx_solver_export": (I, [VP, C.c_char_p, EXPORT_CB, VP]),
     "avx_solver_get_stats": (I, [VP, C.POINTER(RunStats)]),
     "avx_solver_destroy": (None, [VP]),

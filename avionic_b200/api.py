@@ -135,6 +135,16 @@ class CartesianOperator:
         check(lib.avx_operator_forward(self.handle, _cptr(k), _cptr(out), _cptr(b1)))
         return out
 
+    def opnorm(self, x0, b1, iters=10, history=False):
+        """getopnorm (matlab/getopnorm.m:1-17): power-iteration estimate of
+        ||K||^2 for this encoding operator, started from the image x0
+        (T,H,W).  With history=True also returns |y^H x| after each of the
+        iters + 1 applications of K^H K."""
+        v = ctypes.c_double()
+        h = (ctypes.c_double * (iters + 1))()
+        check(lib.avx_operator_opnorm(self.handle, _cptr(x0), _cptr(b1), int(iters), ctypes.byref(v), h))
+        return (v.value, list(h)) if history else v.value
+
     def adapt_lambda(self, k, d):
         lam = ctypes.c_float()
         check(lib.avx_operator_adapt_lambda(self.handle, ctypes.c_float(k), ctypes.c_float(d), ctypes.byref(lam)))
@@ -231,6 +241,18 @@ class Solver:
         check(lib.avx_solver_compute_gap(self.handle, _ptr_array(xs), _ptr_array(ys), _cptr(z), _cptr(data),
                                          _cptr(b1), ctypes.byref(gs), ctypes.byref(gap)))
         return gs.value, gap.value
+
+    def opnorm(self, x0, b1, iters=10, set_steps=False, history=False):
+        """Power-iteration estimate of ||K||^2 for the solver's whole
+        primal-dual operator (regularisation part stacked on the encoding
+        operator), started from the image x0 with the auxiliary components
+        at zero.  set_steps=True makes the initial steps sigma = r/||K||,
+        tau = 1/(r ||K||) (r = sigmaTauRatio)."""
+        v = ctypes.c_double()
+        h = (ctypes.c_double * (iters + 1))()
+        check(lib.avx_solver_opnorm(self.handle, _cptr(x0), _cptr(b1), int(iters), int(bool(set_steps)),
+                                    ctypes.byref(v), h))
+        return (v.value, list(h)) if history else v.value
 
     def set_timing(self, on):
         check(lib.avx_solver_set_timing(self.handle, int(on)))

@@ -18,6 +18,7 @@
 #include <cstdio>
 #include <cstring>
 #include <iostream>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -254,6 +255,23 @@ int main(int argc, char** argv) {
     std::cout << "Using lambda: " << q.lambda << std::endl;
   avx_solver_set_verbose(s, o.verbose);
   avx_solver_set_debug(s, o.debugstep > 0, o.debugstep);
+  if (o.opnorm_steps) {
+    // getopnorm (matlab/getopnorm.m) from a seeded Gaussian image, as the
+    // reference starts it from randn
+    std::mt19937 gen(0);
+    std::normal_distribution<float> nd(0.f, 1.f);
+    std::vector<cf> r(N);
+    for (auto& v : r) v = cf(nd(gen), nd(gen));
+    Dev dr;
+    if (cudaMalloc(&dr.p, N * sizeof(cf)) != cudaSuccess) return die("cudaMalloc failed");
+    cudaMemcpy(dr.p, r.data(), N * sizeof(cf), cudaMemcpyHostToDevice);
+    double l = 0.0;
+    if (avx_solver_opnorm(s, (const avx_cf32*)dr.p, (const avx_cf32*)db.p, o.opnorm_steps, 1, &l, nullptr) != AVX_OK)
+      return die(avx_last_error());
+    avx_solver_get_params(s, &q);
+    std::cout << "Operator norm estimate ||K||^2: " << l << " -> sigma " << q.sigma << ", tau " << q.tau
+              << std::endl;
+  }
   const auto t_init = std::chrono::steady_clock::now();
   std::cout << "Initialization time: " << std::chrono::duration<double>(t_init - t_start).count() << "s" << std::endl;
   if (avx_solver_run(s, (const avx_cf32*)dk.p, (avx_cf32*)dx.p, (const avx_cf32*)db.p) != AVX_OK)

@@ -72,6 +72,7 @@ const std::map<char, Flag>& short_flags() {
 }
 
 bool long_takes_value(const std::string& n) {
+  if (n == "opnormSteps") return true;
   for (auto& kv : short_flags())
     if (n == kv.second.name) return kv.second.value;
   return known_keys().count(n) > 0;
@@ -94,6 +95,7 @@ bool set_option(Options& o, const std::string& name, const std::string& val, std
     else if (name == "uzero") o.u0 = val;
     else if (name == "labeldata") o.labeldata = val;
     else if (name == "tpat") o.tpat = std::stoi(val);
+    else if (name == "opnormSteps") o.opnorm_steps = (unsigned)std::stoul(val);
     else if (name == "slice") o.slice = (unsigned)std::stoul(val);
     else if (name == "gpudevice") o.gpu = std::stoi(val);
     else if (name == "dataBS") o.data_bs = val;
@@ -295,7 +297,9 @@ void print_usage() {
             << "  -b [ --gpudevice ] arg (=-1)  GPU device number\n"
             << "  -m [ --method ] arg (=ICTGV2) TV, TVTEMP, TGV2, ICTV, ICTGV2\n"
             << "  -i [ --maxIt ] arg (=500)  maximum number of iterations\n"
-            << "  -j [ --stopPDGap ] arg (=0) stop at this normalised PD gap\n";
+            << "  -j [ --stopPDGap ] arg (=0) stop at this normalised PD gap\n"
+            << "  --opnormSteps arg (=0)     initial steps from arg power iterations of ||K|| (0: the\n"
+            << "                             configured sigma, tau)\n";
 }
 
 }  // namespace avcli

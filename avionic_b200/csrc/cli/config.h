@@ -22,6 +22,7 @@ struct Options {
   int debugstep = 10;
   int gpu = -1;
   int tpat = 1;
+  unsigned opnorm_steps = 0;  // --opnormSteps: power iterations of the initial-step estimate (0: off)
   unsigned slice = 0;
   std::string dens, params_file, sens, u0, labeldata, data_bs, mask_bs, final_bs;
   bool have_dims = false;

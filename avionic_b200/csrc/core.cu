@@ -30,6 +30,7 @@
 #include "../../include/avionic.h"
 #include "coils.cuh"
 #include "fft2d.cuh"
+#include "opnorm.cuh"
 #include "pd_kernels.cuh"
 #include "radial.cuh"
 #include "tc_dft.cuh"
@@ -945,11 +946,9 @@ static avx_status prepare_run(avx_solver* s, const float2* data, const float2* x
 // launch-shape tuning, the tile-ordered coil maps and, with the debug export
 // of ICTGV2, the gap of the initial state.  Ends with the solver's stream
 // ordered after the caller's.
-static avx_status solver_begin(avx_solver* s, const float2* data, float2* x, const float2* b1) {
-  avx_status r = solver_alloc(s);
-  if (r != AVX_OK) return r;
-  // the reference overwrites dx, dy, dt (and dx2..dt2) from the weights (tv.cpp:103-104)
-  // (TVtemp uses its configured dt as it is, tv_temp.cpp:98-103)
+// the reference overwrites dx, dy, dt (and dx2..dt2) from the weights (tv.cpp:103-104)
+// (TVtemp uses its configured dt as it is, tv_temp.cpp:98-103)
+static avx_status solver_run_weights(avx_solver* s) {
   double ds, dt;
   if (s->method != AVX_METHOD_TVTEMP) {
     if (!time_space_weights(s->p.timeSpaceWeight, &ds, &dt))
@@ -960,6 +959,14 @@ static avx_status solver_begin(avx_solver* s, const float2* data, float2* x, con
     if (!time_space_weights(s->p.timeSpaceWeight2, &ds, &dt)) return fail(AVX_E_ARG, "ComputeTimeSpaceWeights: invalid ratio");
     s->p.dx2 = (float)ds; s->p.dy2 = (float)ds; s->p.dt2 = (float)dt;
   }
+  return AVX_OK;
+}
+
+static avx_status solver_begin(avx_solver* s, const float2* data, float2* x, const float2* b1) {
+  avx_status r = solver_alloc(s);
+  if (r != AVX_OK) return r;
+  r = solver_run_weights(s);
+  if (r != AVX_OK) return r;
   if (s->stream != s->user_stream) {
     // order the internal stream after the caller's stream
     cudaEvent_t evin;
@@ -1872,6 +1879,154 @@ avx_status avx_solver_compute_gap(avx_solver* s, const avx_cf32* const* d_x, con
     reg = gc.ic_a * (s->p.alpha1 * v[7] + s->p.alpha0 * v[8]) + gc.ic_b * (s->p.alpha1 * v[9] + s->p.alpha0 * v[10]);
   if (gstar) *gstar = g;
   if (gap) *gap = std::fabs(g + reg);
+  return AVX_OK;
+}
+
+// ===========================================================================
+// Operator-norm estimate: getopnorm (matlab/getopnorm.m:1-17)
+// ===========================================================================
+
+// A^H A u into img with the operator's own kernels: the compact sampled rows,
+// in the operator's y-transform arithmetic, for the Cartesian operator
+// (row mode 4 applies mask^2 between the transforms); gridding, interpolation,
+// spreading and the adjoint grid transform for the radial one.
+static avx_status encoding_normal(avx_operator* op, const float2* b1, const float2* b1t, const float2* u, float2* img,
+                                  float2* kbuf, DevState* st, cudaStream_t s) {
+  if (op->kind == 1) {
+    RArgs r = make_rargs(op, b1, u, nullptr);
+    r.st = st;
+    r.out = kbuf;
+    avx::launch_rad_forward_grid(r, s);
+    avx::launch_rad_interp(r, 3, s);
+    avx::launch_rad_spread(r, kbuf, s);
+    avx::launch_rad_adjoint_image(r, img, s);
+    return AVX_OK;
+  }
+  if (!op->R) {
+    AVX_CK(cudaMemsetAsync(img, 0, (size_t)op->W * op->H * op->T * sizeof(float2), s));
+    return AVX_OK;
+  }
+  KArgs k;
+  memset(&k, 0, sizeof(k));
+  k.g = op->geom();
+  k.b1 = b1;
+  k.in = u;
+  k.qp = op->d_qp.p;
+  k.st = st;
+  set_tc(&k, op);
+  k.b1t = b1t;
+  avx::launch_kspace(k, 4, s);
+  avx::launch_adjoint(k, img, s);
+  return AVX_OK;
+}
+
+// Power iteration over K^H K, K = (K_reg, A) of `method` (AVX_M_ENCODING: A
+// alone), as getopnorm.m runs it:
+//   y = K^H K x0;  iters times: x = y / ||y|| (y when ||y|| = 0), y = K^H K x, l = y^H x
+// and *opnorm = |l|.  x0 starts the image component, the auxiliary primal
+// components start at zero.  The operator applications run in fp32 (the
+// operator's own arithmetic), the norms and inner products in FP64 on the
+// device; the iterate is normalised on the device, so the loop reads the
+// device once, at its end.  hist (optional) receives |y^H x| after each of
+// the iters + 1 applications.
+static avx_status power_iteration(avx_operator* op, int method, const Wts& w1, const Wts& w2, const float2* b1,
+                                  const float2* b1t, const float2* x0, unsigned iters, cudaStream_t s, double* opnorm,
+                                  double* hist) {
+  const int P = method == AVX_M_ENCODING ? 1 : method_P(method);
+  const int D = method == AVX_M_ENCODING ? 0 : method_D(method);
+  const size_t N = (size_t)op->W * op->H * op->T;
+  DevBuf<float2> x, y, d, khk, kbuf;
+  DevBuf<double> partial, sums;
+  DevBuf<DevState> st;
+  AVX_CK(x.alloc(P * N));
+  AVX_CK(y.alloc(P * N));
+  AVX_CK(d.alloc(std::max(D, 1) * N));
+  AVX_CK(khk.alloc(N));
+  AVX_CK(kbuf.alloc(op->kind == 1 ? (size_t)op->C * op->T * op->S : 1));
+  AVX_CK(partial.alloc(3 * AVX_RED_BLOCKS));
+  AVX_CK(sums.alloc(3 * ((size_t)iters + 1)));
+  AVX_CK(st.alloc(1));
+  AVX_CK(cudaMemsetAsync(st.p, 0, sizeof(DevState), s));
+  AVX_CK(cudaMemcpyAsync(x.p, x0, N * sizeof(float2), cudaMemcpyDeviceToDevice, s));
+  if (P > 1) AVX_CK(cudaMemsetAsync(x.p + N, 0, (P - 1) * N * sizeof(float2), s));
+  avx::OpnArgs a;
+  memset(&a, 0, sizeof(a));
+  a.W = op->W; a.H = op->H; a.T = op->T; a.N = (long long)N;
+  float2* xs[8] = {};
+  for (int c = 0; c < P; ++c) {
+    xs[c] = x.p + c * N;
+    a.x[c] = xs[c];
+    a.y[c] = y.p + c * N;
+  }
+  for (int c = 0; c < D; ++c) a.d[c] = d.p + c * N;
+  a.khk = khk.p;
+  a.w1 = w1;
+  a.w2 = w2;
+  a.partial = partial.p;
+  for (unsigned i = 0; i <= iters; ++i) {
+    if (i > 0) avx::launch_opn_normalise(a, P, xs, sums.p + 3 * (i - 1), s);
+    if (D) avx::launch_opn_dual(method, a, s);
+    avx_status r = encoding_normal(op, b1, b1t, a.x[0], khk.p, kbuf.p, st.p, s);
+    if (r != AVX_OK) return r;
+    avx::launch_opn_primal(method, a, s);
+    avx::launch_opn_finalize(partial.p, sums.p + 3 * i, s);
+  }
+  AVX_CK(cudaGetLastError());
+  std::vector<double> h(3 * ((size_t)iters + 1));
+  DevState hs;
+  AVX_CK(cudaMemcpyAsync(h.data(), sums.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  AVX_CK(cudaMemcpyAsync(&hs, st.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
+  AVX_CK(cudaStreamSynchronize(s));
+  if (hs.err) return fail(AVX_E_NUMERIC, "tensor-core y-transform: a pipeline wait timed out");
+  for (unsigned i = 0; i <= iters; ++i) {
+    const double l = std::hypot(h[3 * i + 1], h[3 * i + 2]);
+    if (hist) hist[i] = l;
+    if (i == iters) *opnorm = l;
+  }
+  return AVX_OK;
+}
+
+avx_status avx_operator_opnorm(avx_operator* op, const avx_cf32* d_x0, const avx_cf32* d_b1, unsigned iters,
+                               double* opnorm, double* hist) {
+  if (!op || !d_x0 || !d_b1 || !opnorm) return fail(AVX_E_ARG, "null argument");
+  if (iters < 1) return fail(AVX_E_ARG, "the power iteration needs at least one iteration");
+  const float2* b1 = reinterpret_cast<const float2*>(d_b1);
+  const float2* b1t = nullptr;
+  if (op->kind == 0 && op->dft_mode == AVX_DFT_SPLIT_BF16X3 && op->tc_np > 0) {
+    AVX_CK(op->tc_b1t.alloc(avx::b1t_count(op->W, op->H, op->C)));
+    avx::launch_b1_tile_transpose(b1, op->tc_b1t.p, op->W, op->H, op->C, 0);
+    b1t = op->tc_b1t.p;
+  }
+  const Wts w0 = make_wts(1.f, 1.f, 1.f);
+  return power_iteration(op, AVX_M_ENCODING, w0, w0, b1, b1t, reinterpret_cast<const float2*>(d_x0), iters, 0,
+                         opnorm, hist);
+}
+
+avx_status avx_solver_opnorm(avx_solver* s, const avx_cf32* d_x0, const avx_cf32* d_b1, unsigned iters, int set_steps,
+                             double* opnorm, double* hist) {
+  if (!s || !d_x0 || !d_b1 || !opnorm) return fail(AVX_E_ARG, "null argument");
+  if (iters < 1) return fail(AVX_E_ARG, "the power iteration needs at least one iteration");
+  avx_status r = solver_alloc(s);
+  if (r != AVX_OK) return r;
+  r = solver_run_weights(s);
+  if (r != AVX_OK) return r;
+  const float2* b1 = reinterpret_cast<const float2*>(d_b1);
+  r = prepare_b1t(s, b1);
+  if (r != AVX_OK) return r;
+  Wts w1, w2;
+  solver_weights(s, &w1, &w2);
+  double l = 0.0;
+  r = power_iteration(s->op, s->method, w1, w2, b1, s->b1t.p, reinterpret_cast<const float2*>(d_x0), iters, s->stream,
+                      &l, hist);
+  if (r != AVX_OK) return r;
+  *opnorm = l;
+  if (set_steps) {
+    if (!(l > 0.0) || !std::isfinite(l)) return fail(AVX_E_NUMERIC, "operator-norm estimate is not positive");
+    // sig = s r, tau = s / r with s = 1 / ||K|| in place of 1/3 (tgv2_dmri.m:96-99)
+    const double L = std::sqrt(l), ratio = s->p.sigmaTauRatio;
+    s->p.sigma = (float)(ratio / L);
+    s->p.tau = (float)(1.0 / (ratio * L));
+  }
   return AVX_OK;
 }
 

@@ -368,6 +368,8 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
           const float2 zm = cscale(zo, m);
           if (!a.binary_mask) a.z[gi] = zm;
           Xb[n * KCP + kk] = zm;
+        } else if (mode == 4) {
+          Xb[n * KCP + kk] = cscale(mX, m);
         } else {
           const int ky = g.rows[r0 + k0 + kk];
           a.dense_out[(((long long)t * C + c) * g.H + ky) * W + kx] = mX;

@@ -58,7 +58,8 @@ void launch_step_finalize(const PDArgs& a, double* pimg, double* pk, int nk, dou
 void launch_gap_tail(int method, const PDArgs& a, const KArgs& k_x, double* pimg, double* pk, int nk,
                      const GapConst& gc, double* hg, double* hn, double* hf, int cap, int init_only,
                      cudaStream_t s);
-// y-transform followed by the row kernel in the given mode (0 PD step, 1 step-rule norm, 2 gap, 3 apply)
+// y-transform followed by the row kernel in the given mode (0 PD step, 1 step-rule norm, 2 gap, 3 apply,
+// 4 normal operator: Q' = row-IFFT(mask^2 X), for A^H A by the column adjoint)
 void launch_kspace(const KArgs& k, int mode, cudaStream_t s);
 // img[t] = sum_c conj(b1_c) column-IDFT of the compact rows in k.qp
 void launch_adjoint(const KArgs& k, float2* img, cudaStream_t s);

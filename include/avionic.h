@@ -231,6 +231,32 @@ avx_status avx_solver_compute_gap(avx_solver* s, const avx_cf32* const* d_x, con
                                   const avx_cf32* d_z, const avx_cf32* d_data, const avx_cf32* d_b1,
                                   double* gstar, double* gap);
 
+/* Operator-norm estimate by power iteration, getopnorm (matlab/getopnorm.m:1-17;
+ * its call in matlab/ls_pd.m:43-56 passes the encoding operator):
+ *   y = K^H K x0;  iters times: x = y / ||y|| (y when ||y|| = 0), y = K^H K x, l = y^H x;
+ *   *opnorm = |l|, an estimate of ||K||^2 (the largest eigenvalue of K^H K).
+ * avx_operator_opnorm: K is the encoding operator (coil maps d_b1, transform,
+ * mask or gridding; image -> k-space), d_x0 the start image (W*H*T values;
+ * the reference draws it from randn).
+ * avx_solver_opnorm: K is the solver's whole primal-dual operator, the
+ * method's regularisation part (with the time-space weights a run would use)
+ * stacked on the encoding operator, K^H the map of its primal update; the
+ * symmetrised gradient's off-diagonal entries count twice in the dual inner
+ * product, as in the step rule.  d_x0 starts the image component; the
+ * auxiliary primal components start at zero.  With set_steps nonzero the
+ * solver's initial steps become sigma = r / sqrt(l), tau = 1 / (r sqrt(l))
+ * (r = sigmaTauRatio: the reference's sig = s r, tau = s / r with
+ * s = 1 / ||K|| in place of 1/3, matlab/tgv2_dmri.m:96-99); a run still adapts
+ * them by AdaptStepSize.
+ * Operator applications run in the operator's arithmetic (fp32, or the split
+ * form), norms and inner products in FP64 on the device.  iters >= 1 (the
+ * reference uses 10).  hist (optional) receives |y^H x| after each of the
+ * iters + 1 applications. */
+avx_status avx_operator_opnorm(avx_operator* op, const avx_cf32* d_x0, const avx_cf32* d_b1, unsigned iters,
+                               double* opnorm, double* hist);
+avx_status avx_solver_opnorm(avx_solver* s, const avx_cf32* d_x0, const avx_cf32* d_b1, unsigned iters,
+                             int set_steps, double* opnorm, double* hist);
+
 /* ExportAdditionalResults (tv.cpp:237-248, tv_temp.cpp:226-236,
  * tgv2.cpp:340-355, ictv.cpp:372-391, ictgv2.cpp:494-516): x3_component
  * (ICTV, ICTGV2), and with debug on PDGap, ICTGVnorm and DATAfidelity

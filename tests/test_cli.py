@@ -40,6 +40,7 @@ def write_problem(tmp, prob, with_u0=True):
 def test_usage_and_errors(tmp_path):
     r = run(["-h"])
     assert r.returncode == 255 and "Usage: avionic" in r.stdout
+    assert "--opnormSteps" in r.stdout
     r = run([])
     assert r.returncode == 255
     rng = np.random.default_rng(0)
@@ -51,6 +52,8 @@ def test_usage_and_errors(tmp_path):
     assert r.returncode == 255 and "invalid method" in r.stderr
     r = run(["-m", "TGV2_3D", "-d", dims, "-s", paths["b1"], paths["kdata"], paths["mask"], out])
     assert r.returncode == 255 and "not provided" in r.stderr
+    r = run(["--opnormSteps", "many", "-m", "TV", "-d", dims, "-s", paths["b1"], paths["kdata"], paths["mask"], out])
+    assert r.returncode == 255 and "invalid value 'many' for option 'opnormSteps'" in r.stderr
     cfg = tmp_path / "bad.cfg"
     cfg.write_text("[tv]\nlambdaa = 3\n")
     r = run(["-p", str(cfg), "-m", "TV", "-d", dims, "-s", paths["b1"], paths["kdata"], paths["mask"], out])
@@ -139,6 +142,48 @@ def test_cli_reconstruction_matches_oracle(tmp_path, method):
     if method == "ICTV":
         assert binfmt.read_bin(str(tmp_path / "x3_component")).size == T * H * W
         assert np.allclose(binfmt.read_bin(str(tmp_path / "ictvnorm")).real, tr["ictvnorm"], rtol=1e-3)
+
+
+@needs_exe
+@pytest.mark.gpu
+def test_cli_opnorm_steps(tmp_path):
+    """--opnormSteps 10: the initial steps come from the power-iteration
+    estimate l of ||K||^2 (sigma = tau = 1/sqrt(l) at sigmaTauRatio 1); the
+    estimate lies below the largest eigenvalue of K^H K (the oracle's
+    estimate after 300 iterations, from another start) and the image equals
+    the oracle's reconstruction from the printed steps."""
+    import re
+    from avionic_b200 import synth
+    from oracle import opnorm as on
+    from oracle import solvers as so
+    from oracle.cartesian import CartesianOperator
+    prob = synth.small(22)
+    T, C, H, W = prob["kdata"].shape
+    paths, dims = write_problem(tmp_path, prob)
+    out = str(tmp_path / "recon.bin")
+    cfg = tmp_path / "run.cfg"
+    cfg.write_text("maxIt = 100\n[tgv2]\nlambda = 2.5\nsigmaTauRatio = 1.0\ntimeSpaceWeight = 1.4\n"
+                   "alpha0 = 1.41421356\nalpha1 = 1.0\n")
+    r = run(["-m", "TGV2", "-p", str(cfg), "--opnormSteps", "10", "-d", dims, "-s", paths["b1"], "-u", paths["u0"],
+             paths["kdata"], paths["mask"], out])
+    assert r.returncode == 0, r.stderr + r.stdout
+    m = re.search(r"Operator norm estimate \|\|K\|\|\^2: (\S+) -> sigma (\S+), tau (\S+)", r.stdout)
+    assert m, r.stdout
+    l, sig, tau = (float(v) for v in m.groups())
+    assert abs(sig * tau * l - 1.0) < 1e-4 and abs(sig / tau - 1.0) < 1e-6
+    op = CartesianOperator(W, H, C, T, mask=prob["mask"], centered=False)
+    p = so.init_params("TGV2")
+    p.maxIt, p.lam, p.timeSpaceWeight, p.alpha0, p.alpha1 = 100, 2.5, 1.4, 1.41421356, 1.0
+    rng = np.random.default_rng(0)
+    top = on.getopnorm(on.method_normal("TGV2", op, prob["b1"].astype(complex), p),
+                       [rng.standard_normal((T, H, W)) + 1j * rng.standard_normal((T, H, W))] +
+                       [np.zeros((T, H, W), complex)] * 3, 300)
+    assert 0.5 * top < l <= top * (1 + 1e-4)
+    p.sigma, p.tau = np.float32(sig), np.float32(tau)
+    xo = so.run("TGV2", prob["kdata"].astype(complex), np.zeros((T, H, W), complex), prob["b1"].astype(complex),
+                op, p)
+    x = binfmt.read_bin(out).reshape(T, H, W)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-4
 
 
 @needs_exe
