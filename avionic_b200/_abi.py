@@ -77,6 +77,8 @@ SIGNATURES = {
     "avx_solver_set_stream": (I, [VP, VP]),
     "avx_solver_set_tuning": (I, [VP, I, I, I]),
     "avx_solver_get_tuning": (I, [VP, C.POINTER(I), C.POINTER(I), C.POINTER(C.c_char_p), C.POINTER(I)]),
+    "avx_solver_set_kspace_schedule": (I, [VP, I, I]),
+    "avx_solver_get_kspace_schedule": (I, [VP, C.POINTER(I), C.POINTER(I)]),
     "avx_solver_run": (I, [VP, VP, VP, VP]),
     "avx_solver_adapt_step_size": (I, [VP, C.POINTER(VP), VP]),
     "avx_solver_compute_gap": (I, [VP, C.POINTER(VP), C.POINTER(VP), VP, VP, VP, C.POINTER(D), C.POINTER(D)]),

@@ -223,6 +223,16 @@ class Solver:
                                         ctypes.byref(t)))
         return p.value, d.value, name.value.decode(), t.value
 
+    def set_kspace_schedule(self, rows_per_pass=16, runtime_plan=False):
+        """Row-FFT schedule of the Cartesian row kernel (avx_solver_set_kspace_schedule)."""
+        check(lib.avx_solver_set_kspace_schedule(self.handle, int(rows_per_pass), int(bool(runtime_plan))))
+
+    def kspace_schedule(self):
+        """(rows per pass, run-time radix plan) in use."""
+        k, r = ctypes.c_int(), ctypes.c_int()
+        check(lib.avx_solver_get_kspace_schedule(self.handle, ctypes.byref(k), ctypes.byref(r)))
+        return k.value, bool(r.value)
+
     def set_stream(self, stream):
         check(lib.avx_solver_set_stream(self.handle, ctypes.c_void_p(stream)))
 

@@ -29,6 +29,7 @@
 
 #include "../../include/avionic.h"
 #include "coils.cuh"
+#include "fft.cuh"
 #include "fft2d.cuh"
 #include "opnorm.cuh"
 #include "pd_kernels.cuh"
@@ -567,6 +568,7 @@ struct avx_solver {
   // launch shapes of the dual and primal kernels (avx_solver_set_tuning)
   bool autotune = true, tuned = false;
   int primal_tile = 0, dual_block = 0;
+  int rows_kc = KSPACE_KC, rows_rt = 0;  // row-FFT schedule (avx_solver_set_kspace_schedule)
   cudaStream_t user_stream = 0;
   cudaStream_t stream = 0;
   bool own_stream = false;  // stream created by solver_alloc (else lent by the batch engine)
@@ -676,15 +678,16 @@ static PDArgs make_pdargs(avx_solver* s) {
   return a;
 }
 
-// Autotuner of the two field-streaming kernels' launch shapes.  The first run
-// of a (device, method, W, H, T) times every candidate shape on the solver's
-// own fields (3 warm-up and 5 timed launches each, CUDA events on its stream)
-// and keeps the fastest; later runs and solvers of that shape reuse it.  The
-// trial launches overwrite the fields, so the caller prepares them again.
+// Autotuner of the field-streaming kernels' launch shapes and of the row
+// kernel's FFT schedule.  The first run of a (device, method, W, H, T, C,
+// sampled rows per frame) times every candidate on the solver's own fields
+// (3 warm-up and 5 timed launches each, CUDA events on its stream) and keeps
+// the fastest; later runs and solvers of that shape reuse it.  The trial
+// launches overwrite the fields, so the caller prepares them again.
 struct TuneKey {
-  int dev, method, W, H, T;
+  int dev, method, W, H, T, C, rows;
   bool operator<(const TuneKey& o) const {
-    return std::tie(dev, method, W, H, T) < std::tie(o.dev, o.method, o.W, o.H, o.T);
+    return std::tie(dev, method, W, H, T, C, rows) < std::tie(o.dev, o.method, o.W, o.H, o.T, o.C, o.rows);
   }
 };
 // one entry per shape: the map's lock covers lookups only, and each shape's
@@ -694,6 +697,7 @@ struct TuneEntry {
   std::mutex mu;
   bool done = false;
   int primal_tile = 0, dual_block = 0;
+  int rows_kc = KSPACE_KC, rows_rt = 0;
 };
 static std::mutex g_tune_mu;
 static std::map<TuneKey, std::unique_ptr<TuneEntry>> g_tune;
@@ -715,10 +719,61 @@ static avx_status time_launches(avx_solver* s, void (*launch)(int, const PDArgs&
   return AVX_OK;
 }
 
-static avx_status autotune(avx_solver* s) {
+static KArgs make_kargs(avx_solver* s, const float2* b1, const float2* in, const float2* in2);
+
+// Row-FFT schedules the tuner tries: rows per pass (8, 12, 16) with the
+// compile-time radix plan of the length, and 16 rows per pass with the
+// run-time plan when the length has a compile-time one.  Rows per pass
+// change the schedule only (every sequence goes through the same passes); the
+// two radix plans round differently.
+static avx_status tune_rows(avx_solver* s, const float2* b1) {
+  KArgs k = make_kargs(s, b1, s->extc(0), nullptr);
+  const CartGeomDev& g = k.g;
+  const bool has_fixed = fft_plan_id(g.W, g.nrad, g.rad) != fft_plan_id_runtime(g.nrad, g.rad);
+  const int cand[4][2] = {{KSPACE_KC, 0}, {12, 0}, {8, 0}, {KSPACE_KC, 1}};
+  const int ncand = has_fixed ? 4 : 3;
+  avx::launch_ydft(k, s->stream);  // compact rows for the trial launches to transform
+  cudaEvent_t e0, e1;
+  AVX_CK(cudaEventCreate(&e0));
+  AVX_CK(cudaEventCreate(&e1));
+  float best = 0.f;
+  for (int i = 0; i < ncand; ++i) {
+    k.rows_kc = cand[i][0];
+    k.rows_rt = cand[i][1];
+    for (int w = 0; w < 3; ++w) avx::launch_rows(k, 0, s->stream);
+    cudaEventRecord(e0, s->stream);
+    for (int w = 0; w < 5; ++w) avx::launch_rows(k, 0, s->stream);
+    cudaEventRecord(e1, s->stream);
+    cudaError_t ce = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+    if (ce == cudaSuccess) ce = cudaGetLastError();
+    if (ce != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return fail(AVX_E_CUDA, std::string("row-schedule tuning: ") + cudaGetErrorString(ce));
+    }
+    if (i == 0 || ms < best) {
+      best = ms;
+      s->rows_kc = cand[i][0];
+      s->rows_rt = cand[i][1];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return AVX_OK;
+}
+
+static int max_rows_per_frame(const avx_operator* op) {
+  int m = 0;
+  for (int t = 0; t + 1 < (int)op->row_off.size(); ++t) m = std::max(m, op->row_off[t + 1] - op->row_off[t]);
+  return m;
+}
+
+static avx_status autotune(avx_solver* s, const float2* b1) {
   int dev = 0;
   AVX_CK(cudaGetDevice(&dev));
-  const TuneKey key{dev, s->method, s->W, s->H, s->T};
+  const TuneKey key{dev, s->method, s->W, s->H, s->T, s->C, s->op->kind == 0 ? max_rows_per_frame(s->op) : -1};
   TuneEntry* ent;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -730,6 +785,8 @@ static avx_status autotune(avx_solver* s) {
   if (ent->done) {
     s->primal_tile = ent->primal_tile;
     s->dual_block = ent->dual_block;
+    s->rows_kc = ent->rows_kc;
+    s->rows_rt = ent->rows_rt;
     s->tuned = true;
     return AVX_OK;
   }
@@ -756,9 +813,15 @@ static avx_status autotune(avx_solver* s) {
       s->dual_block = i;
     }
   }
+  if (s->op->kind == 0 && s->op->R) {
+    avx_status r = tune_rows(s, b1);
+    if (r != AVX_OK) return r;
+  }
   s->tuned = true;
   ent->primal_tile = s->primal_tile;
   ent->dual_block = s->dual_block;
+  ent->rows_kc = s->rows_kc;
+  ent->rows_rt = s->rows_rt;
   ent->done = true;
   return AVX_OK;
 }
@@ -787,6 +850,8 @@ static KArgs make_kargs(avx_solver* s, const float2* b1, const float2* in, const
   k.partial = s->pk.p;
   set_tc(&k, s->op);
   k.b1t = s->b1t.p;
+  k.rows_kc = s->rows_kc;
+  k.rows_rt = s->rows_rt;
   return k;
 }
 
@@ -978,7 +1043,7 @@ static avx_status solver_begin(avx_solver* s, const float2* data, float2* x, con
   r = prepare_run(s, data, x);
   if (r != AVX_OK) return r;
   if (s->autotune && !s->tuned) {
-    r = autotune(s);
+    r = autotune(s, b1);
     if (r != AVX_OK) return r;
     r = prepare_run(s, data, x);  // the trial launches overwrote the fields
     if (r != AVX_OK) return r;
@@ -1006,6 +1071,7 @@ static avx_status solver_begin(avx_solver* s, const float2* data, float2* x, con
   pk.sigma = pk.tau = 0.f;
   const size_t key = (size_t)b1 ^ ((size_t)s->prim.p << 1) ^ ((size_t)s->op << 2) ^
                      ((size_t)s->op->dft_mode << 7) ^ ((size_t)(s->primal_tile * 8 + s->dual_block) << 9) ^
+                     ((size_t)(s->rows_kc * 2 + s->rows_rt) << 16) ^
                      std::hash<std::string>()(std::string((const char*)&pk, sizeof(pk)));
   if (key != s->graph_key) {
     s->drop_graphs();
@@ -1762,6 +1828,23 @@ avx_status avx_solver_get_tuning(const avx_solver* s, int* primal_tile, int* dua
   if (dual_block) *dual_block = s->dual_block;
   if (primal_name) *primal_name = avx::primal_tile_name(s->primal_tile);
   if (dual_threads) *dual_threads = avx::dual_block_threads(s->dual_block);
+  return AVX_OK;
+}
+
+avx_status avx_solver_set_kspace_schedule(avx_solver* s, int rows_per_pass, int runtime_plan) {
+  if (!s) return fail(AVX_E_ARG, "null solver");
+  if (rows_per_pass != 8 && rows_per_pass != 12 && rows_per_pass != 16)
+    return fail(AVX_E_ARG, "rows per pass must be 8, 12 or 16");
+  s->rows_kc = rows_per_pass;
+  s->rows_rt = runtime_plan ? 1 : 0;
+  s->drop_graphs();
+  return AVX_OK;
+}
+
+avx_status avx_solver_get_kspace_schedule(const avx_solver* s, int* rows_per_pass, int* runtime_plan) {
+  if (!s) return fail(AVX_E_ARG, "null solver");
+  if (rows_per_pass) *rows_per_pass = s->rows_kc;
+  if (runtime_plan) *runtime_plan = s->rows_rt;
   return AVX_OK;
 }
 

@@ -248,6 +248,14 @@ inline int fft_plan_id(int n, int nrad, const int* rad) {
   return 1;
 }
 
+// The run-time plan of a length (what fft_plan_id gives a length without a
+// compile-time plan): 1 when every radix is at most 5, else 0.
+inline int fft_plan_id_runtime(int nrad, const int* rad) {
+  for (int i = 0; i < nrad; ++i)
+    if (rad[i] > 5) return 0;
+  return 1;
+}
+
 // row_fft with a plan chosen at compile time; blockDim.x must be 256
 template <int KC, int PLAN, int SIGN>
 AVX_D float2* row_fft_planned(float2* src, float2* dst, const float2* tw, int W, int nrad, const int* rad) {

@@ -68,4 +68,8 @@ struct KArgs {
   const uint4* tc_ctab; // conjugate coefficient pieces, tc_dft.cuh
   int tc_kc;            // MMA K (2 x rows per frame, rounded up to 16)
   const float2* b1t;    // b1 in column-tile order for the tensor-core adjoint (tc_dft.cuh)
+  // row-FFT schedule of the row kernel (chosen by the autotuner): compact rows
+  // per pass (8, 12 or 16; 0 = 16) and the radix plan (0: the compile-time
+  // plan of the length when there is one, 1: the run-time plan)
+  int rows_kc, rows_rt;
 };

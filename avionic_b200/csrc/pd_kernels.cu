@@ -421,12 +421,12 @@ __global__ void __launch_bounds__(256, 4) rows_kernel(KArgs a, int mode) {
   }
 }
 
-size_t rows_smem_bytes(int W) {
-  const int KCP = AVX_FFT_PITCH(KSPACE_KC);
+size_t rows_smem_bytes(int W, int KC) {
+  const int KCP = AVX_FFT_PITCH(KC);
   return sizeof(float2) * (2 * (size_t)W * KCP + W) + sizeof(double) * 32 * 3;
 }
 
-size_t kspace_smem_bytes(int W, int H) { return std::max(ydft_smem_bytes(H), rows_smem_bytes(W)); }
+size_t kspace_smem_bytes(int W, int H) { return std::max(ydft_smem_bytes(H), rows_smem_bytes(W, KSPACE_KC)); }
 
 // ---------------------------------------------------------------------------
 // Column adjoint of the compact rows (completes K^H, cartesian_operator.cpp:65-111):
@@ -944,11 +944,21 @@ void launch_ydft(const KArgs& k, cudaStream_t s) {
   ydft_kernel<KSPACE_KC><<<gr, dim3(YD_XS, YD_CG), ydft_smem_bytes(k.g.H), s>>>(k);
 }
 
-void launch_rows(const KArgs& k, int mode, cudaStream_t s) {
+template <int KC>
+static void launch_rows_kc(const KArgs& k, int mode, cudaStream_t s) {
   // 256 threads, as the compile-time FFT plans assume
-#define CALL_R(ID) rows_kernel<KSPACE_KC, ID><<<k.g.C * k.g.T, 256, rows_smem_bytes(k.g.W), s>>>(k, mode)
-  AVX_FFT_PLAN_DISPATCH(fft_plan_id(k.g.W, k.g.nrad, k.g.rad), CALL_R)
+  const int id = k.rows_rt ? fft_plan_id_runtime(k.g.nrad, k.g.rad) : fft_plan_id(k.g.W, k.g.nrad, k.g.rad);
+#define CALL_R(ID) rows_kernel<KC, ID><<<k.g.C * k.g.T, 256, rows_smem_bytes(k.g.W, KC), s>>>(k, mode)
+  AVX_FFT_PLAN_DISPATCH(id, CALL_R)
 #undef CALL_R
+}
+
+void launch_rows(const KArgs& k, int mode, cudaStream_t s) {
+  switch (k.rows_kc) {
+    case 8: launch_rows_kc<8>(k, mode, s); break;
+    case 12: launch_rows_kc<12>(k, mode, s); break;
+    default: launch_rows_kc<KSPACE_KC>(k, mode, s); break;
+  }
 }
 
 void launch_kspace(const KArgs& k, int mode, cudaStream_t s) {
@@ -1049,8 +1059,12 @@ cudaError_t configure_kernels() {
   cudaError_t e = cudaFuncSetAttribute(ydft_kernel<KSPACE_KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
   if (e != cudaSuccess) return e;
   for (int id : {96, 128, 160, 192, 256, 320, 1, 0}) {
-#define SET_R(ID) \
-  e = cudaFuncSetAttribute(rows_kernel<KSPACE_KC, ID>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX)
+#define SET_R(ID)                                                                                                  \
+  e = cudaFuncSetAttribute(rows_kernel<8, ID>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);       \
+  if (e == cudaSuccess)                                                                                            \
+    e = cudaFuncSetAttribute(rows_kernel<12, ID>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);    \
+  if (e == cudaSuccess)                                                                                            \
+    e = cudaFuncSetAttribute(rows_kernel<KSPACE_KC, ID>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX)
     AVX_FFT_PLAN_DISPATCH(id, SET_R)
 #undef SET_R
     if (e != cudaSuccess) return e;

@@ -700,6 +700,7 @@ def main():
         solver.run(kd, x, b1)
     torch.cuda.synchronize()
     tuning = solver.tuning()
+    row_schedule = solver.kspace_schedule()
 
     clocks = ClockSampler(local)
     barrier()
@@ -851,7 +852,9 @@ def main():
         "recons_per_s": value / ITERS,
         "rel_l2_vs_oracle": err_oracle,
         "details": {"parallelism": "one independent reconstruction per GPU", "graphs": True,
-                    "tuning": {"primal_tile": tuning[2], "dual_block_threads": tuning[3]},
+                    "tuning": {"primal_tile": tuning[2], "dual_block_threads": tuning[3],
+                               "row_fft_rows_per_pass": row_schedule[0],
+                               "row_fft_plan": "run-time" if row_schedule[1] else "compile-time"},
                     "dft": args.dft, "other_dft_form": other,
                     "recon_latency_ms": {"p50": float(np.percentile(step_ms, 50)),
                                          "p99": float(np.percentile(step_ms, 99))}},

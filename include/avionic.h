@@ -206,6 +206,16 @@ avx_status avx_solver_set_tuning(avx_solver* s, int autotune, int primal_tile, i
 /* The shapes in use (chosen by the autotuner after the first run); any output may be NULL. */
 avx_status avx_solver_get_tuning(const avx_solver* s, int* primal_tile, int* dual_block, const char** primal_name,
                                  int* dual_threads);
+/* FFT schedule of the Cartesian operator's row kernel: compact rows per pass
+ * (8, 12 or 16; 16 by default) and the radix plan (0: the compile-time plan
+ * of the row length when it has one, leading with radix-8 passes; 1: the
+ * run-time plan).  With autotune set (avx_solver_set_tuning) the first run of
+ * a (device, method, W, H, T, C, sampled rows per frame) times the candidate
+ * schedules on the solver's own fields and keeps the fastest, replacing what
+ * is set here.  Rows per pass change the schedule only; the two radix plans
+ * round differently (results agree to fp32 rounding). */
+avx_status avx_solver_set_kspace_schedule(avx_solver* s, int rows_per_pass, int runtime_plan);
+avx_status avx_solver_get_kspace_schedule(const avx_solver* s, int* rows_per_pass, int* runtime_plan);
 
 /* IterativeReconstruction(data, x, b1) (pd_recon.h:134-135): d_data dense
  * k-space (W*H*C*T), d_x initial image in / result out (W*H*T), d_b1 coil maps

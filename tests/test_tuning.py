@@ -1,4 +1,6 @@
-"""Launch-shape autotuning of the dual and primal kernels (avx_solver_set_tuning).
+"""Autotuning of the dual and primal kernels' launch shapes
+(avx_solver_set_tuning) and of the row kernel's FFT schedule
+(avx_solver_set_kspace_schedule).
 
 Every shape runs the same per-pixel arithmetic; the compiler may still fuse
 multiply-adds differently in each instantiation, so the images are compared
@@ -33,6 +35,62 @@ def test_rejects_bad_arguments_without_a_device():
     import avionic_b200 as av
     assert av.lib.avx_solver_set_tuning(None, 1, 0, 0) == 1  # AVX_E_ARG
     assert av.lib.avx_solver_get_tuning(None, None, None, None, None) == 1
+    assert av.lib.avx_solver_set_kspace_schedule(None, 16, 0) == 1
+    assert av.lib.avx_solver_get_kspace_schedule(None, None, None) == 1
+
+
+def _run_rows(av, prob, kc, rt, autotune=False, iters=40):
+    import torch
+    T, C, H, W = prob["kdata"].shape
+    op = av.CartesianOperator(W, H, C, T, mask=av.to_device(prob["mask"]), centered=True)
+    s = av.Solver("TGV2", op)
+    p = s.params
+    p.maxIt = iters
+    s.params = p
+    s.set_tuning(autotune, 0, 0)
+    if not autotune:
+        s.set_kspace_schedule(kc, rt)
+    x = torch.zeros((T, H, W), dtype=torch.complex64, device="cuda")
+    s.run(av.to_device(prob["kdata"]), x, av.to_device(prob["b1"]))
+    return x.cpu().numpy(), s
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("W,H", [(64, 40), (36, 30)])
+def test_every_row_schedule_gives_the_same_image(W, H):
+    """Rows per pass change the schedule only: bit-identical images.  The
+    run-time radix plan rounds differently from the compile-time one (W = 64
+    has one; W = 36 has none, so both plans are the run-time plan)."""
+    import avionic_b200 as av
+    from avionic_b200 import synth
+    prob = synth.small(45, H=H, W=W, T=5, C=3)
+    ref, s = _run_rows(av, prob, 16, False)
+    assert s.kspace_schedule() == (16, False)
+    for kc in (12, 8):
+        x, s = _run_rows(av, prob, kc, False)
+        assert s.kspace_schedule() == (kc, False)
+        assert np.array_equal(x, ref), kc
+    x, s = _run_rows(av, prob, 16, True)
+    assert s.kspace_schedule() == (16, True)
+    assert rel(x, ref) < REL
+    if W == 36:
+        assert np.array_equal(x, ref)
+    with pytest.raises(RuntimeError):
+        s.set_kspace_schedule(10, False)
+
+
+@pytest.mark.gpu
+def test_row_schedule_is_tuned_and_reused():
+    import avionic_b200 as av
+    from avionic_b200 import synth
+    prob = synth.small(47, H=48, W=64, T=6, C=4)
+    ref, _ = _run_rows(av, prob, 16, False)
+    x, s = _run_rows(av, prob, 0, False, autotune=True)
+    kc, rt = s.kspace_schedule()
+    assert kc in (8, 12, 16)
+    assert rel(x, ref) < REL
+    _, s2 = _run_rows(av, prob, 0, False, autotune=True)
+    assert s2.kspace_schedule() == (kc, rt)
 
 
 @pytest.mark.gpu
