@@ -233,7 +233,7 @@ struct avx_operator {
   int S = 0, spf = 0;
   RadialGeomDev rg{};
   DevBuf<float> r_traj, r_sqrtw, r_ipx, r_ipy;
-  DevBuf<int> r_order, r_secstart;
+  DevBuf<int> r_order, r_secstart, r_spread_blocks;
   DevBuf<int2> r_win0;
   DevBuf<float> r_winw;
   DevBuf<float2> r_twgx, r_twgy, r_grid;
@@ -453,6 +453,29 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
     for (int s = 0; s < S; ++s) st[sec[s] + 1]++;
     for (int k = 0; k < nsec; ++k) st[k + 1] += st[k];
   }
+  // spreading CTAs in order of falling neighbourhood sample count (the 3x3
+  // sectors around each sector, as rad_spread_kernel stages them)
+  std::vector<int> blocks((size_t)T * nsec), blk_tot((size_t)T * nsec);
+  {
+    const int dxn = g.nsx >= 3 ? 3 : g.nsx, dyn = g.nsy >= 3 ? 3 : g.nsy;
+    for (int f = 0; f < T; ++f) {
+      const int* st = &start[(size_t)f * (nsec + 1)];
+      for (int sec = 0; sec < nsec; ++sec) {
+        const int sxi = sec % g.nsx, syi = sec / g.nsx;
+        int tot = 0;
+        for (int dy = 0; dy < dyn; ++dy)
+          for (int dx = 0; dx < dxn; ++dx) {
+            const int nx = ((sxi + (dxn == 3 ? dx - 1 : dx)) % g.nsx + g.nsx) % g.nsx;
+            const int ny = ((syi + (dyn == 3 ? dy - 1 : dy)) % g.nsy + g.nsy) % g.nsy;
+            const int ns = ny * g.nsx + nx;
+            tot += st[ns + 1] - st[ns];
+          }
+        blk_tot[(size_t)f * nsec + sec] = tot;
+      }
+    }
+    for (size_t i = 0; i < blocks.size(); ++i) blocks[i] = (int)i;
+    std::stable_sort(blocks.begin(), blocks.end(), [&](int a, int b) { return blk_tot[a] > blk_tot[b]; });
+  }
   const std::vector<int> rx = fft_radices(g.Gx), ry = fft_radices(g.Gy);
   if (rx.empty() || ry.empty()) return fail(AVX_E_UNSUPPORTED, "grid size has no FFT plan");
   g.nradx = (int)rx.size();
@@ -483,6 +506,8 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
   AVX_CK(cudaMemcpy(op->r_ipy.p, ipy.data(), H * sizeof(float), cudaMemcpyHostToDevice));
   AVX_CK(cudaMemcpy(op->r_order.p, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
   AVX_CK(cudaMemcpy(op->r_secstart.p, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+  AVX_CK(op->r_spread_blocks.alloc(blocks.size()));
+  AVX_CK(cudaMemcpy(op->r_spread_blocks.p, blocks.data(), blocks.size() * sizeof(int), cudaMemcpyHostToDevice));
   AVX_CK(cudaMemcpy(op->r_twgx.p, twx.data(), g.Gx * sizeof(float2), cudaMemcpyHostToDevice));
   AVX_CK(cudaMemcpy(op->r_twgy.p, twy.data(), g.Gy * sizeof(float2), cudaMemcpyHostToDevice));
   g.traj = op->r_traj.p;
@@ -491,6 +516,7 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
   g.inv_psi_y = op->r_ipy.p;
   g.order = op->r_order.p;
   g.sec_start = op->r_secstart.p;
+  g.spread_blocks = op->r_spread_blocks.p;
   g.twgx = op->r_twgx.p;
   g.twgy = op->r_twgy.p;
   // the samples' window starts and weights depend on the trajectory alone
@@ -2588,7 +2614,7 @@ size_t request_workspace(const avx_request& r, long long R_known, int max_rows_k
     const size_t Gx = (size_t)radial_grid_size((int)W, r.osf), Gy = (size_t)radial_grid_size((int)H, r.osf);
     const size_t sectors = T * ((Gx + isw - 1) / isw) * ((Gy + isw - 1) / isw) + 1;
     kspace = C * T * S;
-    b += T * S * (2 * 4 + 4 + 4) + (W + H) * 4 + sectors * 4 + (Gx + Gy) * c8 + T * C * Gx * Gy * c8 + N * c8;
+    b += T * S * (2 * 4 + 4 + 4) + (W + H) * 4 + sectors * 8 + (Gx + Gy) * c8 + T * C * Gx * Gy * c8 + N * c8;
     b += T * S * (8 + 2 * 8 * 4);  // window starts and Kaiser-Bessel weights
   }
   // solver: primal, extragradient and step scratch (3P), duals (D), z and d, reductions, history

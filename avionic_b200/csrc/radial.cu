@@ -267,7 +267,9 @@ __global__ void __launch_bounds__(256) rad_interp_kernel(RArgs a, int mode) {
 }
 
 // one CTA per (sector, frame); thread = grid cell of the sector; CC coils
-// accumulated per pass over the neighbouring sectors' samples
+// accumulated per pass over the neighbouring sectors' samples.  The CTAs are
+// numbered through g.spread_blocks, heaviest neighbourhood first, so that the
+// central sectors (which every spoke crosses) start in the first wave.
 template <int NW, int CC>
 __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
   if (a.st && a.st->stop) return;
@@ -279,14 +281,15 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
   // per sector row: the staged samples whose window covers that row (two
   // batches' worth, alternating), so that a cell visits only those
   __shared__ unsigned long long s_rowm[2][RAD_MAX_SW];
-  const int f = blockIdx.y;
-  const int sec = blockIdx.x;
+  const int nsec = g.nsx * g.nsy;
+  const int blk = g.spread_blocks[blockIdx.x];
+  const int f = blk / nsec;
+  const int sec = blk - f * nsec;
   const int sxi = sec % g.nsx, syi = sec / g.nsx;
   const int X0 = sxi * g.sw, Y0 = syi * g.sw;
   const int lx = threadIdx.x % g.sw, ly = threadIdx.x / g.sw;
   const int gx = X0 + lx, gy = Y0 + ly;
   const bool active = gx < g.Gx && gy < g.Gy;
-  const int nsec = g.nsx * g.nsy;
   const int* order = g.order + (long long)f * g.S;
   const int* start = g.sec_start + (long long)f * (nsec + 1);
   // The neighbourhood's samples, sector by sector in (dy, dx) order, as at
@@ -465,7 +468,7 @@ void launch_rad_windows(const RadialGeomDev& g, int2* win0, float* winw, cudaStr
 }
 
 void launch_rad_spread(const RArgs& a, const float2* samples, cudaStream_t s) {
-  dim3 grid(a.g.nsx * a.g.nsy, a.g.T);
+  const int grid = a.g.nsx * a.g.nsy * a.g.T;
   const int threads = a.g.sw * a.g.sw;
   // coils per pass: every pass re-reads the neighbouring sectors' samples
   if (a.g.C <= 4) {
