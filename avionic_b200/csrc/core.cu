@@ -233,7 +233,7 @@ struct avx_operator {
   int S = 0, spf = 0;
   RadialGeomDev rg{};
   DevBuf<float> r_traj, r_sqrtw, r_ipx, r_ipy;
-  DevBuf<int> r_order, r_secstart, r_spread_blocks;
+  DevBuf<int> r_order, r_secstart, r_spread_list, r_spread_off, r_spread_blocks;
   DevBuf<int2> r_win0;
   DevBuf<float> r_winw;
   DevBuf<float2> r_twgx, r_twgy, r_grid;
@@ -453,29 +453,6 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
     for (int s = 0; s < S; ++s) st[sec[s] + 1]++;
     for (int k = 0; k < nsec; ++k) st[k + 1] += st[k];
   }
-  // spreading CTAs in order of falling neighbourhood sample count (the 3x3
-  // sectors around each sector, as rad_spread_kernel stages them)
-  std::vector<int> blocks((size_t)T * nsec), blk_tot((size_t)T * nsec);
-  {
-    const int dxn = g.nsx >= 3 ? 3 : g.nsx, dyn = g.nsy >= 3 ? 3 : g.nsy;
-    for (int f = 0; f < T; ++f) {
-      const int* st = &start[(size_t)f * (nsec + 1)];
-      for (int sec = 0; sec < nsec; ++sec) {
-        const int sxi = sec % g.nsx, syi = sec / g.nsx;
-        int tot = 0;
-        for (int dy = 0; dy < dyn; ++dy)
-          for (int dx = 0; dx < dxn; ++dx) {
-            const int nx = ((sxi + (dxn == 3 ? dx - 1 : dx)) % g.nsx + g.nsx) % g.nsx;
-            const int ny = ((syi + (dyn == 3 ? dy - 1 : dy)) % g.nsy + g.nsy) % g.nsy;
-            const int ns = ny * g.nsx + nx;
-            tot += st[ns + 1] - st[ns];
-          }
-        blk_tot[(size_t)f * nsec + sec] = tot;
-      }
-    }
-    for (size_t i = 0; i < blocks.size(); ++i) blocks[i] = (int)i;
-    std::stable_sort(blocks.begin(), blocks.end(), [&](int a, int b) { return blk_tot[a] > blk_tot[b]; });
-  }
   const std::vector<int> rx = fft_radices(g.Gx), ry = fft_radices(g.Gy);
   if (rx.empty() || ry.empty()) return fail(AVX_E_UNSUPPORTED, "grid size has no FFT plan");
   g.nradx = (int)rx.size();
@@ -506,8 +483,6 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
   AVX_CK(cudaMemcpy(op->r_ipy.p, ipy.data(), H * sizeof(float), cudaMemcpyHostToDevice));
   AVX_CK(cudaMemcpy(op->r_order.p, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
   AVX_CK(cudaMemcpy(op->r_secstart.p, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
-  AVX_CK(op->r_spread_blocks.alloc(blocks.size()));
-  AVX_CK(cudaMemcpy(op->r_spread_blocks.p, blocks.data(), blocks.size() * sizeof(int), cudaMemcpyHostToDevice));
   AVX_CK(cudaMemcpy(op->r_twgx.p, twx.data(), g.Gx * sizeof(float2), cudaMemcpyHostToDevice));
   AVX_CK(cudaMemcpy(op->r_twgy.p, twy.data(), g.Gy * sizeof(float2), cudaMemcpyHostToDevice));
   g.traj = op->r_traj.p;
@@ -516,7 +491,6 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
   g.inv_psi_y = op->r_ipy.p;
   g.order = op->r_order.p;
   g.sec_start = op->r_secstart.p;
-  g.spread_blocks = op->r_spread_blocks.p;
   g.twgx = op->r_twgx.p;
   g.twgy = op->r_twgy.p;
   // the samples' window starts and weights depend on the trajectory alone
@@ -527,6 +501,56 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
   AVX_CK(cudaStreamSynchronize(0));
   g.win0 = op->r_win0.p;
   g.winw = op->r_winw.p;
+  // The spreading's work list.  Per (frame, sector), the samples whose window
+  // reaches the sector's cells, in the order the sector sums them: the 3x3
+  // neighbouring sectors in (dy, dx) order, each in sorted order (fewer than
+  // three sectors along an axis wrap onto themselves and are taken once).
+  // The CTAs are numbered heaviest list first, so that the central sectors,
+  // which every spoke crosses, start in the first wave.
+  {
+    std::vector<int2> w0((size_t)T * S);
+    AVX_CK(cudaMemcpy(w0.data(), op->r_win0.p, w0.size() * sizeof(int2), cudaMemcpyDeviceToHost));
+    auto wrap = [](int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); };
+    const int dxn = g.nsx >= 3 ? 3 : g.nsx, dyn = g.nsy >= 3 ? 3 : g.nsy;
+    std::vector<int> soff((size_t)T * nsec + 1, 0), slist;
+    slist.reserve((size_t)T * S * 4);
+    for (int f = 0; f < T; ++f) {
+      const int* st = &start[(size_t)f * (nsec + 1)];
+      const int* ord = &order[(size_t)f * S];
+      for (int sec = 0; sec < nsec; ++sec) {
+        const int sxi = sec % g.nsx, syi = sec / g.nsx;
+        const int X0 = sxi * g.sw, Y0 = syi * g.sw;
+        const int swx = std::min(g.sw, g.Gx - X0), swy = std::min(g.sw, g.Gy - Y0);
+        for (int dy = 0; dy < dyn; ++dy)
+          for (int dx = 0; dx < dxn; ++dx) {
+            const int nx = ((sxi + (dxn == 3 ? dx - 1 : dx)) % g.nsx + g.nsx) % g.nsx;
+            const int ny = ((syi + (dyn == 3 ? dy - 1 : dy)) % g.nsy + g.nsy) % g.nsy;
+            const int ns = ny * g.nsx + nx;
+            for (int q = st[ns]; q < st[ns + 1]; ++q) {
+              const int j = ord[q];
+              const int2 a0 = w0[(size_t)f * S + j];
+              const int dx0 = wrap(X0 - a0.x, g.Gx), dy0 = wrap(Y0 - a0.y, g.Gy);
+              if ((dx0 < g.nw || dx0 + swx > g.Gx) && (dy0 < g.nw || dy0 + swy > g.Gy)) slist.push_back(j);
+            }
+          }
+        soff[(size_t)f * nsec + sec + 1] = (int)slist.size();
+      }
+    }
+    std::vector<int> blocks((size_t)T * nsec);
+    for (size_t i = 0; i < blocks.size(); ++i) blocks[i] = (int)i;
+    std::stable_sort(blocks.begin(), blocks.end(),
+                     [&](int a, int b) { return soff[a + 1] - soff[a] > soff[b + 1] - soff[b]; });
+    AVX_CK(op->r_spread_list.alloc(std::max<size_t>(slist.size(), 1)));
+    AVX_CK(op->r_spread_off.alloc(soff.size()));
+    AVX_CK(op->r_spread_blocks.alloc(blocks.size()));
+    if (!slist.empty())
+      AVX_CK(cudaMemcpy(op->r_spread_list.p, slist.data(), slist.size() * sizeof(int), cudaMemcpyHostToDevice));
+    AVX_CK(cudaMemcpy(op->r_spread_off.p, soff.data(), soff.size() * sizeof(int), cudaMemcpyHostToDevice));
+    AVX_CK(cudaMemcpy(op->r_spread_blocks.p, blocks.data(), blocks.size() * sizeof(int), cudaMemcpyHostToDevice));
+    g.spread_list = op->r_spread_list.p;
+    g.spread_off = op->r_spread_off.p;
+    g.spread_blocks = op->r_spread_blocks.p;
+  }
   return AVX_OK;
 }
 
@@ -2614,8 +2638,9 @@ size_t request_workspace(const avx_request& r, long long R_known, int max_rows_k
     const size_t Gx = (size_t)radial_grid_size((int)W, r.osf), Gy = (size_t)radial_grid_size((int)H, r.osf);
     const size_t sectors = T * ((Gx + isw - 1) / isw) * ((Gy + isw - 1) / isw) + 1;
     kspace = C * T * S;
-    b += T * S * (2 * 4 + 4 + 4) + (W + H) * 4 + sectors * 8 + (Gx + Gy) * c8 + T * C * Gx * Gy * c8 + N * c8;
+    b += T * S * (2 * 4 + 4 + 4) + (W + H) * 4 + sectors * 4 + (Gx + Gy) * c8 + T * C * Gx * Gy * c8 + N * c8;
     b += T * S * (8 + 2 * 8 * 4);  // window starts and Kaiser-Bessel weights
+    b += T * S * 4 * 4 + 2 * sectors * 4;  // the spreading's work list, its offsets and order
   }
   // solver: primal, extragradient and step scratch (3P), duals (D), z and d, reductions, history
   b += (3 * P + D) * N * c8 + 2 * kspace * c8;

@@ -267,9 +267,11 @@ __global__ void __launch_bounds__(256) rad_interp_kernel(RArgs a, int mode) {
 }
 
 // one CTA per (sector, frame); thread = grid cell of the sector; CC coils
-// accumulated per pass over the neighbouring sectors' samples.  The CTAs are
-// numbered through g.spread_blocks, heaviest neighbourhood first, so that the
-// central sectors (which every spoke crosses) start in the first wave.
+// accumulated per pass over the sector's work list: the samples whose window
+// reaches the sector, in the order of the 3x3 neighbouring sectors and of the
+// sorted order within each (built with the operator).  The CTAs are numbered
+// through g.spread_blocks, longest list first, so that the central sectors
+// (which every spoke crosses) start in the first wave.
 template <int NW, int CC>
 __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
   if (a.st && a.st->stop) return;
@@ -290,42 +292,11 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
   const int lx = threadIdx.x % g.sw, ly = threadIdx.x / g.sw;
   const int gx = X0 + lx, gy = Y0 + ly;
   const bool active = gx < g.Gx && gy < g.Gy;
-  const int* order = g.order + (long long)f * g.S;
-  const int* start = g.sec_start + (long long)f * (nsec + 1);
-  // The neighbourhood's samples, sector by sector in (dy, dx) order, as at
-  // most nine ranges of the sorted order; neighbouring sectors of one row
-  // are adjacent there and merge into one range.  The batches run over the
-  // ranges' concatenation, so a sparse neighbourhood takes a single batch.
-  __shared__ int s_rb[9], s_rl[9], s_nr, s_tot;
-  if (threadIdx.x == 0) {
-    // distinct neighbouring sector offsets (fewer than three sectors along an axis wrap onto themselves)
-    const int dxn = g.nsx >= 3 ? 3 : g.nsx, dyn = g.nsy >= 3 ? 3 : g.nsy;
-    int nr = 0, tot = 0;
-    for (int dy = 0; dy < dyn; ++dy)
-      for (int dx = 0; dx < dxn; ++dx) {
-        const int nsxi = imod(sxi + (dxn == 3 ? dx - 1 : dx), g.nsx);
-        const int nsyi = imod(syi + (dyn == 3 ? dy - 1 : dy), g.nsy);
-        const int ns = nsyi * g.nsx + nsxi;
-        const int p0 = start[ns], p1 = start[ns + 1];
-        if (p1 <= p0) continue;
-        if (nr > 0 && s_rb[nr - 1] + s_rl[nr - 1] == p0) {
-          s_rl[nr - 1] += p1 - p0;
-        } else {
-          s_rb[nr] = p0;
-          s_rl[nr] = p1 - p0;
-          ++nr;
-        }
-        tot += p1 - p0;
-      }
-    s_nr = nr;
-    s_tot = tot;
-  }
+  const int* list = g.spread_list + g.spread_off[blk];
+  const int tot = g.spread_off[blk + 1] - g.spread_off[blk];
   for (int i = threadIdx.x; i < RAD_MAX_SW; i += blockDim.x) s_rowm[0][i] = s_rowm[1][i] = 0ull;
   __syncthreads();
-  const int nr = s_nr, tot = s_tot;
-  // the sector's cells, per axis: window offsets (cell - g0) mod G run over
-  // [d0, d0 + sw); the window reaches them when one of those is below NW
-  const int swx = min(g.sw, g.Gx - X0), swy = min(g.sw, g.Gy - Y0);
+  const int swy = min(g.sw, g.Gy - Y0);
   int bi = 0;  // batch counter over all coil passes (selects s_rowm)
   for (int c0 = 0; c0 < g.C; c0 += CC) {
     const int cc = min(CC, g.C - c0);
@@ -337,14 +308,9 @@ __global__ void rad_spread_kernel(RArgs a, const float2* __restrict__ samples) {
       unsigned long long* rowm = s_rowm[bi & 1];
       __syncthreads();
       for (int e = threadIdx.x; e < nb; e += blockDim.x) {
-        int q = b0 + e, k = 0;
-        while (k < nr - 1 && q >= s_rl[k]) q -= s_rl[k++];
-        const int j = order[s_rb[k] + q];
+        const int j = list[b0 + e];
         const long long fj = (long long)f * g.S + j;
         const int2 g0 = g.win0[fj];
-        const int dx0 = wrap1(X0 - g0.x, g.Gx), dy0 = wrap1(Y0 - g0.y, g.Gy);
-        const bool hit = (dx0 < NW || dx0 + swx > g.Gx) && (dy0 < NW || dy0 + swy > g.Gy);
-        if (!hit) continue;
         // the sector rows the window covers (bitwise OR: the result does not depend on the order)
 #pragma unroll
         for (int o = 0; o < NW; ++o) {

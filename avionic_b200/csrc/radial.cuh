@@ -21,7 +21,9 @@ struct RadialGeomDev {
   const float* inv_psi_y;   // [H]
   const int* order;         // [T][S] sample indices sorted by sector (stable)
   const int* sec_start;     // [T][nsx*nsy + 1] offsets into order
-  const int* spread_blocks; // [T*nsx*nsy] f*nsx*nsy + sector, by falling neighbourhood sample count
+  const int* spread_list;   // per (frame, sector): the samples whose window reaches the sector, in summation order
+  const int* spread_off;    // [T*nsx*nsy + 1] offsets into spread_list, index f*nsx*nsy + sector
+  const int* spread_blocks; // [T*nsx*nsy] f*nsx*nsy + sector, longest list first
   const int2* win0;         // [T][S] first grid cell (x, y) of each sample's window, unwrapped
   const float* winw;        // [T][S][2 nw] the window's weights, x then y
   const float2* twgx;       // [Gx] exp(+2 pi i j / Gx)
