@@ -328,6 +328,48 @@ __global__ void b1r_primal_kernel(CoilPD a, int coils) {
   a.ext1n[idx] = make_float2(2.f * n1.x - xo.x, 2.f * n1.y - xo.y);
 }
 
+// One B1Recon iteration in one kernel: the dual update of b1r_dual_kernel at
+// this pixel and at the neighbours the divergence reads (x - 1 for the x
+// component, x - W for the y component), recomputed from the old extragradient
+// and duals, then the primal update of b1r_primal_kernel.  The extragradient
+// and the duals are double-buffered (neighbouring threads read the old values
+// while the owner writes the new ones); x is updated in place (read and written
+// by its own thread only).  Same arithmetic as the two-kernel form.
+__global__ void b1r_fused_kernel(CoilPD a, int coils, B1Buffers b) {
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int HW = a.W * a.H;
+  if (idx >= (long long)coils * HW) return;
+  const int c = (int)(idx / HW);
+  const int pix = (int)(idx % HW);
+  const P2 p = p2_of(pix, a.W, a.H);
+  const long long cb = (long long)c * HW;
+  const float2* e = b.ext_in + cb;
+  const float sc = 1.f / (1.f + a.sigma / a.mu);
+  // dual component k at coil pixel q (the arithmetic of b1r_dual_kernel)
+  auto dual = [&](int k, int qx, int qy) {
+    const long long q = (long long)qy * a.W + qx;
+    const float2 g = k == 0 ? d_fwd(e, q, qx, a.W, 1) : d_fwd(e, q, qy, a.H, a.W);
+    const float2 v = (k == 0 ? b.y0_in : b.y1_in)[cb + q];
+    return cscale(make_float2(v.x + a.sigma * g.x, v.y + a.sigma * g.y), sc);
+  };
+  const float2 y0 = dual(0, p.x, p.y), y1 = dual(1, p.x, p.y);
+  b.y0_out[idx] = y0;
+  b.y1_out[idx] = y1;
+  // divergence (div2 of coils.cu) from the new duals
+  const float2 y0m = p.x > 0 ? dual(0, p.x - 1, p.y) : czero();
+  const float2 y1m = p.y > 0 ? dual(1, p.x, p.y - 1) : czero();
+  const float2 ax = csub(y0m, p.x < a.W - 1 ? y0 : czero());
+  const float2 ay = csub(y1m, p.y < a.H - 1 ? y1 : czero());
+  const float2 s2 = cadd(ax, ay);
+  const float2 dv = make_float2(-s2.x, -s2.y);
+  const float2 xo = a.x1[idx];
+  float2 n1 = make_float2(xo.x + a.tau * dv.x, xo.y + a.tau * dv.y);
+  const float2 lw = a.Lw[idx];
+  n1 = cmul(make_float2(n1.x + a.tau * lw.x, n1.y + a.tau * lw.y), a.Ib[idx]);
+  a.x1n[idx] = n1;
+  b.ext_out[idx] = make_float2(2.f * n1.x - xo.x, 2.f * n1.y - xo.y);
+}
+
 __global__ void b1r_normalize_kernel(const float2* x, float2* out, int HW, int coils) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= HW) return;
@@ -416,6 +458,10 @@ void launch_b1r_iter(const CoilPD& a, int coils, cudaStream_t s) {
   const long long n = (long long)coils * a.W * a.H;
   b1r_dual_kernel<<<nb256(n), 256, 0, s>>>(a, coils);
   b1r_primal_kernel<<<nb256(n), 256, 0, s>>>(a, coils);
+}
+void launch_b1r_fused(const CoilPD& a, int coils, const B1Buffers& b, cudaStream_t s) {
+  const long long n = (long long)coils * a.W * a.H;
+  b1r_fused_kernel<<<nb256(n), 256, 0, s>>>(a, coils, b);
 }
 void launch_b1r_normalize(const float2* x, float2* out, int HW, int coils, cudaStream_t s) {
   b1r_normalize_kernel<<<nb256(HW), 256, 0, s>>>(x, out, HW, coils);

@@ -22,6 +22,16 @@ struct CoilPD {
   const float2* Ib;
 };
 
+// double-buffered extragradient and duals of one fused B1Recon iteration
+struct B1Buffers {
+  const float2* ext_in;
+  float2* ext_out;
+  const float2* y0_in;
+  const float2* y1_in;
+  float2* y0_out;
+  float2* y1_out;
+};
+
 namespace avx {
 
 void launch_ta_sum(const float2* kdata, const float* mask, float2* out, int HW, int C, int T, cudaStream_t s);
@@ -36,6 +46,7 @@ void launch_absmax(const float2* v, int n, unsigned* out, cudaStream_t s);
 void launch_b1r_prep(const float2* u0, const unsigned* umax, const float2* crec, int coils, int HW, float tau,
                      float2* Lw, float2* Iu, cudaStream_t s);
 void launch_b1r_iter(const CoilPD& a, int coils, cudaStream_t s);
+void launch_b1r_fused(const CoilPD& a, int coils, const B1Buffers& b, cudaStream_t s);
 void launch_b1r_normalize(const float2* x, float2* out, int HW, int coils, cudaStream_t s);
 void launch_phase_apply(const float2* absb1, const float2* x1, float2* out, int HW, cudaStream_t s);
 void launch_weight_update(float2* w, const float2* b, int HW, cudaStream_t s);

@@ -1404,12 +1404,12 @@ avx_status coil_b1_recon(int W, int H, int coils, unsigned max_it, float mu, con
   CoilLoop local;
   CoilLoop& l = loop ? *loop : local;
   if (l.N != N || l.coils != coils) {
-    AVX_CK(l.buf.alloc(6 * CN));
+    AVX_CK(l.buf.alloc(9 * CN));
     AVX_CK(l.umax.alloc(1));
     l.N = N;
     l.coils = coils;
   }
-  AVX_CK(cudaMemsetAsync(l.buf.p, 0, 6 * CN * sizeof(float2), s));
+  AVX_CK(cudaMemsetAsync(l.buf.p, 0, 9 * CN * sizeof(float2), s));
   AVX_CK(cudaMemsetAsync(l.umax.p, 0, sizeof(unsigned), s));
   CoilPD a;
   memset(&a, 0, sizeof(a));
@@ -1428,7 +1428,22 @@ avx_status coil_b1_recon(int W, int H, int coils, unsigned max_it, float mu, con
   a.Ib = Iu;
   avx::launch_absmax(u0, N, l.umax.p, s);
   avx::launch_b1r_prep(u0, l.umax.p, crec, coils, N, p.b1Tau, Lw, Iu, s);
-  avx_status r = coil_iterate(l, max_it, s, [&] { avx::launch_b1r_iter(a, coils, s); });
+  // one kernel per iteration; the extragradient and the duals alternate
+  // between two buffers (the second set at 6 CN .. 9 CN), x stays in place
+  float2* ext2 = l.buf.p + 6 * CN;
+  float2* y2[2] = {l.buf.p + 7 * CN, l.buf.p + 8 * CN};
+  unsigned it = 0;
+  avx_status r = coil_iterate(l, max_it, s, [&] {
+    const bool odd = (it++ & 1u) != 0;
+    B1Buffers b;
+    b.ext_in = odd ? ext2 : a.ext1;
+    b.ext_out = odd ? a.ext1 : ext2;
+    b.y0_in = odd ? y2[0] : a.y1[0];
+    b.y1_in = odd ? y2[1] : a.y1[1];
+    b.y0_out = odd ? a.y1[0] : y2[0];
+    b.y1_out = odd ? a.y1[1] : y2[1];
+    avx::launch_b1r_fused(a, coils, b, s);
+  });
   if (r != AVX_OK) return r;
   avx::launch_b1r_normalize(a.x1, out, N, coils, s);
   AVX_CK(cudaGetLastError());
