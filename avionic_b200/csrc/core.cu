@@ -382,7 +382,11 @@ static int radial_grid_size(int d, double osf) {
   return n;
 }
 
-static avx_status build_radial(avx_operator* op, const float* h_traj, const float* h_dens, float J, float sw, float osf) {
+// The gridding operator's tables.  d_traj [T][2][S] and d_dens [T][S] are
+// device arrays; the per-sample tables (sector order, sqrt(w), windows,
+// spreading work lists) are built on the device, the per-axis ones (twiddles,
+// deapodisation) on the host.
+static avx_status build_radial(avx_operator* op, const float* d_traj, const float* d_dens, float J, float sw, float osf) {
   const int W = op->W, H = op->H, T = op->T, S = op->S;
   if (!(J > 0.f && J <= 7.f)) return fail(AVX_E_ARG, "kernelWidth must lie in (0, 7]");
   if (!(osf > 1.0f)) return fail(AVX_E_ARG, "osf must exceed 1");
@@ -402,8 +406,12 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
   // trajectory in [-1/2, 1/2] and a grid wider than the window plus two cells
   if ((float)std::min(g.Gx, g.Gy) <= J + 2.f)
     return fail(AVX_E_ARG, "oversampled grid too small for the kernel width");
-  for (size_t i = 0; i < (size_t)T * 2 * S; ++i)
-    if (!(std::fabs(h_traj[i]) <= 0.5f)) return fail(AVX_E_ARG, "trajectory values must lie in [-0.5, 0.5]");
+  {
+    int flags = 0;
+    AVX_CK(avx::rad_validate(d_traj, (long long)T * 2 * S, d_dens, (long long)T * S, &flags, 0));
+    if (flags & 1) return fail(AVX_E_ARG, "trajectory values must lie in [-0.5, 0.5]");
+    if (flags & 2) return fail(AVX_E_ARG, "density compensation must be non-negative");
+  }
   g.nw = (int)std::ceil(J) + 1;
   g.J = J;
   const double beta = M_PI * std::sqrt((J / osf) * (J / osf) * (osf - 0.5) * (osf - 0.5) - 0.8);
@@ -428,31 +436,7 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
   std::vector<float> ipx, ipy;
   deap(W, g.Gx, ipx);
   deap(H, g.Gy, ipy);
-  // sector of every sample in float32 arithmetic, then a stable sort by sector
   const int nsec = g.nsx * g.nsy;
-  std::vector<int> order((size_t)T * S), start((size_t)T * (nsec + 1));
-  std::vector<float> sqw((size_t)T * S);
-  for (int f = 0; f < T; ++f) {
-    std::vector<int> sec(S);
-    for (int s = 0; s < S; ++s) {
-      float px = h_traj[((size_t)f * 2 + 0) * S + s] * (float)g.Gx;
-      float py = h_traj[((size_t)f * 2 + 1) * S + s] * (float)g.Gy;
-      if (px < 0.f) px += (float)g.Gx;
-      if (py < 0.f) py += (float)g.Gy;
-      int sx = (int)std::floor(px / (float)isw), sy = (int)std::floor(py / (float)isw);
-      sx = std::min(std::max(sx, 0), g.nsx - 1);
-      sy = std::min(std::max(sy, 0), g.nsy - 1);
-      sec[s] = sy * g.nsx + sx;
-      sqw[(size_t)f * S + s] = (float)std::sqrt((double)h_dens[(size_t)f * S + s]);
-    }
-    int* ord = &order[(size_t)f * S];
-    for (int s = 0; s < S; ++s) ord[s] = s;
-    std::stable_sort(ord, ord + S, [&](int a, int b) { return sec[a] < sec[b]; });
-    int* st = &start[(size_t)f * (nsec + 1)];
-    std::fill(st, st + nsec + 1, 0);
-    for (int s = 0; s < S; ++s) st[sec[s] + 1]++;
-    for (int k = 0; k < nsec; ++k) st[k + 1] += st[k];
-  }
   const std::vector<int> rx = fft_radices(g.Gx), ry = fft_radices(g.Gy);
   if (rx.empty() || ry.empty()) return fail(AVX_E_UNSUPPORTED, "grid size has no FFT plan");
   g.nradx = (int)rx.size();
@@ -471,21 +455,20 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
   AVX_CK(op->r_sqrtw.alloc((size_t)T * S));
   AVX_CK(op->r_ipx.alloc(W));
   AVX_CK(op->r_ipy.alloc(H));
-  AVX_CK(op->r_order.alloc(order.size()));
-  AVX_CK(op->r_secstart.alloc(start.size()));
+  AVX_CK(op->r_order.alloc((size_t)T * S));
+  AVX_CK(op->r_secstart.alloc((size_t)T * (nsec + 1)));
   AVX_CK(op->r_twgx.alloc(g.Gx));
   AVX_CK(op->r_twgy.alloc(g.Gy));
   AVX_CK(op->r_grid.alloc((size_t)T * op->C * g.Gx * g.Gy));
   AVX_CK(op->r_khz.alloc((size_t)T * H * W));
-  AVX_CK(cudaMemcpy(op->r_traj.p, h_traj, (size_t)T * 2 * S * sizeof(float), cudaMemcpyHostToDevice));
-  AVX_CK(cudaMemcpy(op->r_sqrtw.p, sqw.data(), sqw.size() * sizeof(float), cudaMemcpyHostToDevice));
+  AVX_CK(cudaMemcpy(op->r_traj.p, d_traj, (size_t)T * 2 * S * sizeof(float), cudaMemcpyDeviceToDevice));
   AVX_CK(cudaMemcpy(op->r_ipx.p, ipx.data(), W * sizeof(float), cudaMemcpyHostToDevice));
   AVX_CK(cudaMemcpy(op->r_ipy.p, ipy.data(), H * sizeof(float), cudaMemcpyHostToDevice));
-  AVX_CK(cudaMemcpy(op->r_order.p, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
-  AVX_CK(cudaMemcpy(op->r_secstart.p, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
   AVX_CK(cudaMemcpy(op->r_twgx.p, twx.data(), g.Gx * sizeof(float2), cudaMemcpyHostToDevice));
   AVX_CK(cudaMemcpy(op->r_twgy.p, twy.data(), g.Gy * sizeof(float2), cudaMemcpyHostToDevice));
   g.traj = op->r_traj.p;
+  // sector of every sample in float32 arithmetic, then a stable sort by sector
+  AVX_CK(avx::rad_build_order(g, d_dens, op->r_sqrtw.p, op->r_order.p, op->r_secstart.p, 0));
   g.sqrt_w = op->r_sqrtw.p;
   g.inv_psi_x = op->r_ipx.p;
   g.inv_psi_y = op->r_ipy.p;
@@ -508,45 +491,13 @@ static avx_status build_radial(avx_operator* op, const float* h_traj, const floa
   // The CTAs are numbered heaviest list first, so that the central sectors,
   // which every spoke crosses, start in the first wave.
   {
-    std::vector<int2> w0((size_t)T * S);
-    AVX_CK(cudaMemcpy(w0.data(), op->r_win0.p, w0.size() * sizeof(int2), cudaMemcpyDeviceToHost));
-    auto wrap = [](int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); };
-    const int dxn = g.nsx >= 3 ? 3 : g.nsx, dyn = g.nsy >= 3 ? 3 : g.nsy;
-    std::vector<int> soff((size_t)T * nsec + 1, 0), slist;
-    slist.reserve((size_t)T * S * 4);
-    for (int f = 0; f < T; ++f) {
-      const int* st = &start[(size_t)f * (nsec + 1)];
-      const int* ord = &order[(size_t)f * S];
-      for (int sec = 0; sec < nsec; ++sec) {
-        const int sxi = sec % g.nsx, syi = sec / g.nsx;
-        const int X0 = sxi * g.sw, Y0 = syi * g.sw;
-        const int swx = std::min(g.sw, g.Gx - X0), swy = std::min(g.sw, g.Gy - Y0);
-        for (int dy = 0; dy < dyn; ++dy)
-          for (int dx = 0; dx < dxn; ++dx) {
-            const int nx = ((sxi + (dxn == 3 ? dx - 1 : dx)) % g.nsx + g.nsx) % g.nsx;
-            const int ny = ((syi + (dyn == 3 ? dy - 1 : dy)) % g.nsy + g.nsy) % g.nsy;
-            const int ns = ny * g.nsx + nx;
-            for (int q = st[ns]; q < st[ns + 1]; ++q) {
-              const int j = ord[q];
-              const int2 a0 = w0[(size_t)f * S + j];
-              const int dx0 = wrap(X0 - a0.x, g.Gx), dy0 = wrap(Y0 - a0.y, g.Gy);
-              if ((dx0 < g.nw || dx0 + swx > g.Gx) && (dy0 < g.nw || dy0 + swy > g.Gy)) slist.push_back(j);
-            }
-          }
-        soff[(size_t)f * nsec + sec + 1] = (int)slist.size();
-      }
-    }
-    std::vector<int> blocks((size_t)T * nsec);
-    for (size_t i = 0; i < blocks.size(); ++i) blocks[i] = (int)i;
-    std::stable_sort(blocks.begin(), blocks.end(),
-                     [&](int a, int b) { return soff[a + 1] - soff[a] > soff[b + 1] - soff[b]; });
-    AVX_CK(op->r_spread_list.alloc(std::max<size_t>(slist.size(), 1)));
-    AVX_CK(op->r_spread_off.alloc(soff.size()));
-    AVX_CK(op->r_spread_blocks.alloc(blocks.size()));
-    if (!slist.empty())
-      AVX_CK(cudaMemcpy(op->r_spread_list.p, slist.data(), slist.size() * sizeof(int), cudaMemcpyHostToDevice));
-    AVX_CK(cudaMemcpy(op->r_spread_off.p, soff.data(), soff.size() * sizeof(int), cudaMemcpyHostToDevice));
-    AVX_CK(cudaMemcpy(op->r_spread_blocks.p, blocks.data(), blocks.size() * sizeof(int), cudaMemcpyHostToDevice));
+    AVX_CK(op->r_spread_off.alloc((size_t)T * nsec + 1));
+    long long total = 0;
+    AVX_CK(avx::rad_count_lists(g, op->r_order.p, op->r_secstart.p, op->r_win0.p, op->r_spread_off.p, &total, 0));
+    AVX_CK(op->r_spread_list.alloc(std::max<size_t>((size_t)total, 1)));
+    AVX_CK(op->r_spread_blocks.alloc((size_t)T * nsec));
+    AVX_CK(avx::rad_fill_lists(g, op->r_order.p, op->r_secstart.p, op->r_win0.p, op->r_spread_off.p,
+                               op->r_spread_list.p, op->r_spread_blocks.p, 0));
     g.spread_list = op->r_spread_list.p;
     g.spread_off = op->r_spread_off.p;
     g.spread_blocks = op->r_spread_blocks.p;
@@ -1486,34 +1437,41 @@ __global__ void abs_inplace_kernel(float2* v, int n) {
 avx_status coil_time_averaged_radial(int W, int H, int C, int T, int S, const float* traj, const float* dens,
                                      const float2* kdata, float2* u, float2* crec, int apply_phase, cudaStream_t s) {
   const size_t TS = (size_t)T * S;
-  std::vector<float> ht((size_t)T * 2 * S), hd(TS), ht1(2 * TS);
-  AVX_CK(cudaMemcpy(ht.data(), traj, ht.size() * sizeof(float), cudaMemcpyDeviceToHost));
-  AVX_CK(cudaMemcpy(hd.data(), dens, hd.size() * sizeof(float), cudaMemcpyDeviceToHost));
-  for (int f = 0; f < T; ++f)
-    for (int j = 0; j < S; ++j) {
-      ht1[(size_t)f * S + j] = ht[((size_t)f * 2 + 0) * S + j];
-      ht1[TS + (size_t)f * S + j] = ht[((size_t)f * 2 + 1) * S + j];
-    }
+  // every frame's kx, then every frame's ky: [T][2][S] -> [1][2][T S] (the
+  // densities [T][S] already read as one frame)
+  DevBuf<float> t1;
+  AVX_CK(t1.alloc(2 * TS));
+  for (int a = 0; a < 2; ++a)
+    AVX_CK(cudaMemcpy2DAsync(t1.p + (size_t)a * TS, S * sizeof(float), traj + (size_t)a * S, 2 * S * sizeof(float),
+                             S * sizeof(float), T, cudaMemcpyDeviceToDevice, s));
+  AVX_CK(cudaStreamSynchronize(s));
+  // one frame holding every frame's samples; the spreading grid holds every
+  // coil (one pass over the samples for all coils), the adjoint grid
+  // transform and crop run per coil (no coil combination)
   avx_operator op;
   op.kind = 1;
-  op.W = W; op.H = H; op.C = 1; op.T = 1;
+  op.W = W; op.H = H; op.C = C; op.T = 1;
   op.S = (int)TS;
   op.spf = 1;
-  avx_status r = build_radial(&op, ht1.data(), hd.data(), 3.f, 8.f, 2.f);
+  avx_status r = build_radial(&op, t1.p, dens, 3.f, 8.f, 2.f);
   if (r != AVX_OK) return r;
   DevBuf<float2> ones, samp;
   AVX_CK(ones.alloc((size_t)W * H));
-  AVX_CK(samp.alloc(TS));
+  AVX_CK(samp.alloc((size_t)C * TS));
   std::vector<float2> h1((size_t)W * H, make_float2(1.f, 0.f));
   AVX_CK(cudaMemcpy(ones.p, h1.data(), h1.size() * sizeof(float2), cudaMemcpyHostToDevice));
+  // coil c's samples of all frames, frame after frame: [frame][coil][sample] -> [coil][frame][sample]
+  for (int c = 0; c < C; ++c)
+    AVX_CK(cudaMemcpy2DAsync(samp.p + (size_t)c * TS, S * sizeof(float2), kdata + (size_t)c * S,
+                             (size_t)C * S * sizeof(float2), S * sizeof(float2), T, cudaMemcpyDeviceToDevice, s));
   RArgs ra = make_rargs(&op, ones.p, nullptr, nullptr);
+  avx::launch_rad_spread(ra, samp.p, s);
+  const size_t G2 = (size_t)op.rg.Gx * op.rg.Gy;
   for (int c = 0; c < C; ++c) {
-    // gather coil c's samples of all frames ([frame][coil][sample] -> [frame][sample])
-    for (int f = 0; f < T; ++f)
-      AVX_CK(cudaMemcpyAsync(samp.p + (size_t)f * S, kdata + ((size_t)f * C + c) * S, S * sizeof(float2),
-                             cudaMemcpyDeviceToDevice, s));
-    avx::launch_rad_spread(ra, samp.p, s);
-    avx::launch_rad_adjoint_image(ra, crec + (size_t)c * W * H, s);
+    RArgs rc = ra;
+    rc.g.C = 1;
+    rc.grid = op.r_grid.p + (size_t)c * G2;
+    avx::launch_rad_adjoint_image(rc, crec + (size_t)c * W * H, s);
   }
   avx::launch_ta_combine(crec, u, W * H, C, 1.f, apply_phase, s);
   AVX_CK(cudaGetLastError());
@@ -1689,17 +1647,12 @@ avx_status avx_radial_operator_create(unsigned width, unsigned height, unsigned 
   avx_status r = configure_once();
   if (r != AVX_OK) return r;
   const size_t S = (size_t)nFE * spokesPerFrame;
-  std::vector<float> ht((size_t)frames * 2 * S), hd((size_t)frames * S);
-  AVX_CK(cudaMemcpy(ht.data(), d_traj, ht.size() * sizeof(float), cudaMemcpyDeviceToHost));
-  AVX_CK(cudaMemcpy(hd.data(), d_dens, hd.size() * sizeof(float), cudaMemcpyDeviceToHost));
-  for (float v : hd)
-    if (!(v >= 0.f)) return fail(AVX_E_ARG, "density compensation must be non-negative");
   avx_operator* op = new avx_operator();
   op->kind = 1;
   op->W = (int)width; op->H = (int)height; op->C = (int)coils; op->T = (int)frames;
   op->S = (int)S;
   op->spf = (int)spokesPerFrame;
-  r = build_radial(op, ht.data(), hd.data(), kernelWidth, sectorWidth, osf);
+  r = build_radial(op, d_traj, d_dens, kernelWidth, sectorWidth, osf);
   if (r != AVX_OK) {
     delete op;
     return r;

@@ -9,6 +9,9 @@
 // grid value is a fixed-order sum (no floating-point atomics, deterministic).
 #include <algorithm>
 
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
 #include "fft.cuh"
 #include "radial.cuh"
 
@@ -424,6 +427,200 @@ void launch_rad_interp(const RArgs& a, int mode, cudaStream_t s) {
 #define CALL_I(N) rad_interp_kernel<N><<<nb, 256, 0, s>>>(a, mode)
   RAD_NW_DISPATCH(a.g.nw, CALL_I)
 #undef CALL_I
+}
+
+// ---------------------------------------------------------------------------
+// Per-sample tables of an operator, built on the device.
+// ---------------------------------------------------------------------------
+
+__global__ void rad_validate_kernel(const float* traj, long long nt, const float* dens, long long nd, int* flags) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nt; i += (long long)gridDim.x * blockDim.x)
+    if (!(fabsf(traj[i]) <= 0.5f)) atomicOr(flags, 1);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nd; i += (long long)gridDim.x * blockDim.x)
+    if (!(dens[i] >= 0.f)) atomicOr(flags, 2);
+}
+
+// sector of every sample in float32 arithmetic (multiply, wrap, divide:
+// each rounded once), key f nsec + sector, value the sample index, the
+// per-key counts, and sqrt(w) per sample
+__global__ void rad_keys_kernel(RadialGeomDev g, const float* dens, float* sqrt_w, int* key, int* val, int* cnt) {
+  const int nsec = g.nsx * g.nsy;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)g.T * g.S;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)(i / g.S), s = (int)(i % g.S);
+    float px = __fmul_rn(g.traj[((long long)f * 2 + 0) * g.S + s], (float)g.Gx);
+    float py = __fmul_rn(g.traj[((long long)f * 2 + 1) * g.S + s], (float)g.Gy);
+    if (px < 0.f) px = __fadd_rn(px, (float)g.Gx);
+    if (py < 0.f) py = __fadd_rn(py, (float)g.Gy);
+    int sx = (int)floorf(__fdiv_rn(px, (float)g.sw)), sy = (int)floorf(__fdiv_rn(py, (float)g.sw));
+    sx = min(max(sx, 0), g.nsx - 1);
+    sy = min(max(sy, 0), g.nsy - 1);
+    const int k = f * nsec + sy * g.nsx + sx;
+    key[i] = k;
+    val[i] = s;
+    atomicAdd(cnt + k, 1);
+    sqrt_w[i] = (float)sqrt((double)dens[i]);
+  }
+}
+
+// sec_start[f][k] = offset of frame f's sector k within the frame's sorted order
+__global__ void rad_sec_start_kernel(RadialGeomDev g, const int* off, int* sec_start) {
+  const int nsec = g.nsx * g.nsy;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (long long)g.T * (nsec + 1);
+       i += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)(i / (nsec + 1)), k = (int)(i % (nsec + 1));
+    sec_start[i] = k < nsec ? off[(long long)f * nsec + k] - f * g.S : g.S;
+  }
+}
+
+// The spreading work list of (frame, sector) item `it`, one warp per item:
+// the samples of the distinct 3x3 neighbouring sectors in (dy, dx) order,
+// each sector's in sorted order, that pass the window test of
+// rad_spread_kernel.  Counts (list == nullptr) or writes them from off[it].
+__global__ void rad_lists_kernel(RadialGeomDev g, const int* order, const int* sec_start, const int2* win0,
+                                 int* count, const int* off, int* list) {
+  const int nsec = g.nsx * g.nsy;
+  const int lane = threadIdx.x & 31;
+  const long long it = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  if (it >= (long long)g.T * nsec) return;
+  const int f = (int)(it / nsec), sec = (int)(it % nsec);
+  const int sxi = sec % g.nsx, syi = sec / g.nsx;
+  const int X0 = sxi * g.sw, Y0 = syi * g.sw;
+  const int swx = min(g.sw, g.Gx - X0), swy = min(g.sw, g.Gy - Y0);
+  const int dxn = g.nsx >= 3 ? 3 : g.nsx, dyn = g.nsy >= 3 ? 3 : g.nsy;
+  const int* ord = order + (long long)f * g.S;
+  const int* st = sec_start + (long long)f * (nsec + 1);
+  int n = 0;
+  int* out = list ? list + off[it] : nullptr;
+  for (int dy = 0; dy < dyn; ++dy)
+    for (int dx = 0; dx < dxn; ++dx) {
+      const int nx = imod(sxi + (dxn == 3 ? dx - 1 : dx), g.nsx);
+      const int ny = imod(syi + (dyn == 3 ? dy - 1 : dy), g.nsy);
+      const int ns = ny * g.nsx + nx;
+      for (int q0 = st[ns]; q0 < st[ns + 1]; q0 += 32) {
+        const int q = q0 + lane;
+        bool hit = false;
+        int j = 0;
+        if (q < st[ns + 1]) {
+          j = ord[q];
+          const int2 a0 = win0[(long long)f * g.S + j];
+          const int dx0 = wrap1(X0 - a0.x, g.Gx), dy0 = wrap1(Y0 - a0.y, g.Gy);
+          hit = (dx0 < g.nw || dx0 + swx > g.Gx) && (dy0 < g.nw || dy0 + swy > g.Gy);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (out && hit) out[n + __popc(m & ((1u << lane) - 1u))] = j;
+        n += __popc(m);
+      }
+    }
+  if (!list && lane == 0) count[it] = n;
+}
+
+__global__ void rad_list_len_kernel(const int* off, int n, int* len) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) len[i] = off[i + 1] - off[i];
+}
+
+__global__ void rad_iota_kernel(int* v, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
+static int key_bits(long long n) {
+  int b = 1;
+  while ((1ll << b) < n) ++b;
+  return b;
+}
+
+cudaError_t rad_validate(const float* traj, long long nt, const float* dens, long long nd, int* flags_host,
+                         cudaStream_t s) {
+  int* d = nullptr;
+  cudaError_t e = cudaMallocAsync(&d, sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  cudaMemsetAsync(d, 0, sizeof(int), s);
+  rad_validate_kernel<<<148 * 8, 256, 0, s>>>(traj, nt, dens, nd, d);
+  cudaMemcpyAsync(flags_host, d, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(d, s);
+  e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e;
+}
+
+cudaError_t rad_build_order(const RadialGeomDev& g, const float* dens, float* sqrt_w, int* order, int* sec_start,
+                            cudaStream_t s) {
+  const long long n = (long long)g.T * g.S;
+  const long long nk = (long long)g.T * g.nsx * g.nsy;
+  int *key = nullptr, *key2 = nullptr, *val = nullptr, *cnt = nullptr, *off = nullptr;
+  void* tmp = nullptr;
+  size_t tb_sort = 0, tb_scan = 0;
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, tb_sort, key, key2, val, order, (int)n, 0, key_bits(nk), s);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb_scan, cnt, off, (int)nk, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&key, 2 * n * sizeof(int) + n * sizeof(int), s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&cnt, 2 * (nk + 1) * sizeof(int), s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&tmp, std::max(tb_sort, tb_scan) + 16, s);
+  if (e != cudaSuccess) return e;
+  key2 = key + n;
+  val = key + 2 * n;
+  off = cnt + nk + 1;
+  cudaMemsetAsync(cnt, 0, (nk + 1) * sizeof(int), s);
+  const int nb = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+  rad_keys_kernel<<<nb, 256, 0, s>>>(g, dens, sqrt_w, key, val, cnt);
+  // a stable sort: within a key, samples stay in index order
+  e = cub::DeviceRadixSort::SortPairs(tmp, tb_sort, key, key2, val, order, (int)n, 0, key_bits(nk), s);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tb_scan, cnt, off, (int)nk, s);
+  if (e == cudaSuccess) {
+    const long long ns = (long long)g.T * (g.nsx * g.nsy + 1);
+    rad_sec_start_kernel<<<(int)std::min<long long>((ns + 255) / 256, 148 * 16), 256, 0, s>>>(g, off, sec_start);
+    e = cudaGetLastError();
+  }
+  cudaFreeAsync(tmp, s);
+  cudaFreeAsync(cnt, s);
+  cudaFreeAsync(key, s);
+  return e;
+}
+
+cudaError_t rad_count_lists(const RadialGeomDev& g, const int* order, const int* sec_start, const int2* win0,
+                            int* off, long long* total, cudaStream_t s) {
+  const long long nk = (long long)g.T * g.nsx * g.nsy;
+  int* cnt = nullptr;
+  void* tmp = nullptr;
+  size_t tb = 0;
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, (int)(nk + 1), s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&cnt, (nk + 1) * sizeof(int), s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&tmp, tb + 16, s);
+  if (e != cudaSuccess) return e;
+  cudaMemsetAsync(cnt, 0, (nk + 1) * sizeof(int), s);
+  rad_lists_kernel<<<(int)((nk * 32 + 255) / 256), 256, 0, s>>>(g, order, sec_start, win0, cnt, nullptr, nullptr);
+  e = cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, off, (int)(nk + 1), s);
+  int h = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, off + nk, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(tmp, s);
+  cudaFreeAsync(cnt, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  *total = h;
+  return e;
+}
+
+cudaError_t rad_fill_lists(const RadialGeomDev& g, const int* order, const int* sec_start, const int2* win0,
+                           const int* off, int* list, int* blocks, cudaStream_t s) {
+  const long long nk = (long long)g.T * g.nsx * g.nsy;
+  rad_lists_kernel<<<(int)((nk * 32 + 255) / 256), 256, 0, s>>>(g, order, sec_start, win0, nullptr, off, list);
+  // CTAs longest list first (a stable sort: equal lengths keep item order)
+  int *len = nullptr, *len2 = nullptr, *ids = nullptr;
+  void* tmp = nullptr;
+  size_t tb = 0;
+  cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, len, len2, ids, blocks, (int)nk, 0, 32, s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&len, 3 * nk * sizeof(int), s);
+  if (e == cudaSuccess) e = cudaMallocAsync(&tmp, tb + 16, s);
+  if (e != cudaSuccess) return e;
+  len2 = len + nk;
+  ids = len + 2 * nk;
+  rad_list_len_kernel<<<(int)((nk + 255) / 256), 256, 0, s>>>(off, (int)nk, len);
+  rad_iota_kernel<<<(int)((nk + 255) / 256), 256, 0, s>>>(ids, (int)nk);
+  e = cub::DeviceRadixSort::SortPairsDescending(tmp, tb, len, len2, ids, blocks, (int)nk, 0, 32, s);
+  cudaFreeAsync(tmp, s);
+  cudaFreeAsync(len, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return e;
 }
 
 void launch_rad_windows(const RadialGeomDev& g, int2* win0, float* winw, cudaStream_t s) {

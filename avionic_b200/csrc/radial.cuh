@@ -55,6 +55,21 @@ cudaError_t configure_radial_kernels();
 
 // per-sample window starts and weights (g.win0, g.winw), once per operator
 void launch_rad_windows(const RadialGeomDev& g, int2* win0, float* winw, cudaStream_t s);
+// Per-sample tables of an operator, built on the device (stream-ordered, each
+// call returns after its stream work when it reads a result back):
+// flags bit 0: a trajectory value outside [-1/2, 1/2]; bit 1: a negative density
+cudaError_t rad_validate(const float* traj, long long nt, const float* dens, long long nd, int* flags_host,
+                         cudaStream_t s);
+// sqrt(w), and the samples of every frame stably sorted by sector (order,
+// [T][S]) with the sectors' offsets (sec_start, [T][nsx nsy + 1]); needs g.traj
+cudaError_t rad_build_order(const RadialGeomDev& g, const float* dens, float* sqrt_w, int* order, int* sec_start,
+                            cudaStream_t s);
+// the spreading work lists' offsets (off, [T nsx nsy + 1]) and total length
+cudaError_t rad_count_lists(const RadialGeomDev& g, const int* order, const int* sec_start, const int2* win0,
+                            int* off, long long* total, cudaStream_t s);
+// the work lists and the CTA order (longest list first)
+cudaError_t rad_fill_lists(const RadialGeomDev& g, const int* order, const int* sec_start, const int2* win0,
+                           const int* off, int* list, int* blocks, cudaStream_t s);
 // grid -> samples; mode 0 z prox, 1 sum |K u|^2, 2 gap sums, 3 write samples to a.out
 void launch_rad_interp(const RArgs& a, int mode, cudaStream_t s);
 // forward image -> grid: the zero-padded, deapodised b1 (in - in2) and its
