@@ -8,6 +8,8 @@
 // 664-684, 817-844, 1078-1117).
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "coils.cuh"
 #include "stencil.cuh"
 
@@ -179,6 +181,94 @@ __global__ void __launch_bounds__(1024) h1_cg_kernel(const float2* u, const floa
   __syncthreads();
   for (int i = threadIdx.x; i < N; i += blockDim.x) out[(size_t)c * N + i] = make_float2((float)x[i].x, (float)x[i].y);
   if (threadIdx.x == 0 && iters) iters[c] = it;
+}
+
+// The same CG with each coil's system spread over a cluster of H1_CLUSTER
+// CTAs (contiguous blocks of pixels per CTA).  The vectors stay in global
+// memory; the stencil reads its neighbours there after a cluster barrier
+// (release/acquire at cluster scope).  Every inner product is a block sum per
+// CTA, the CTA sums written into a slot of every CTA's shared memory, and one
+// cluster barrier, after which each CTA adds the slots in rank order: every
+// CTA holds the same value, so all take the same branch of the stopping test.
+#define H1_CLUSTER 8
+
+__global__ void __cluster_dims__(H1_CLUSTER, 1, 1) __launch_bounds__(1024)
+    h1_cg_cluster_kernel(const float2* u, const float2* crec, double mu, int W, int H, int max_it, double rel_tol,
+                         double2* work, double* muu_buf, float2* out, int* iters) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  __shared__ double red[32];
+  __shared__ double slots[2][H1_CLUSTER];  // the CTA sums of the two most recent reductions
+  const int rank = (int)cl.block_rank();
+  const int c = blockIdx.x / H1_CLUSTER;
+  const int N = W * H;
+  const int i0 = (int)((long long)N * rank / H1_CLUSTER), i1 = (int)((long long)N * (rank + 1) / H1_CLUSTER);
+  double2* x = work + (size_t)c * 4 * N;
+  double2* r = x + N;
+  double2* p = r + N;
+  double2* q = p + N;
+  double* muu = muu_buf + (size_t)c * N;
+  int nred = 0;
+  auto csum = [&](double v) {
+    v = block_dsum<1024>(v, red);
+    double* buf = slots[nred & 1];
+    if (threadIdx.x == 0)
+      for (int k = 0; k < H1_CLUSTER; ++k) cl.map_shared_rank(buf, k)[rank] = v;
+    cl.sync();
+    double t = 0.0;
+    for (int k = 0; k < H1_CLUSTER; ++k) t += buf[k];
+    ++nred;
+    return t;
+  };
+  double rr = 0.0;
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    const float2 uu = u[i];
+    const double au2 = (double)uu.x * uu.x + (double)uu.y * uu.y;
+    muu[i] = mu * au2;
+    const float2 cr = crec[(size_t)c * N + i];
+    const double ac = mu * sqrt((double)cr.x * cr.x + (double)cr.y * cr.y);
+    const double2 y = make_double2((double)uu.x * ac, -(double)uu.y * ac);
+    x[i] = make_double2(0.0, 0.0);
+    r[i] = y;
+    p[i] = y;
+    rr += y.x * y.x + y.y * y.y;
+  }
+  rr = csum(rr);  // the barrier also publishes p and muu to the cluster
+  const double rr0 = rr;
+  int it = 0;
+  for (; it < max_it && rr > rel_tol * rel_tol * rr0 && rr > 0.0; ++it) {
+    double pq = 0.0;
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+      const double2 a = h1_apply(p, muu, i % W, i / W, W, H);
+      q[i] = a;
+      const double2 pv = p[i];
+      pq += pv.x * a.x + pv.y * a.y;
+    }
+    pq = csum(pq);
+    const double alpha = rr / pq;
+    double rn = 0.0;
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+      const double2 pv = p[i], qv = q[i];
+      double2 xv = x[i], rv = r[i];
+      xv.x += alpha * pv.x;
+      xv.y += alpha * pv.y;
+      rv.x -= alpha * qv.x;
+      rv.y -= alpha * qv.y;
+      x[i] = xv;
+      r[i] = rv;
+      rn += rv.x * rv.x + rv.y * rv.y;
+    }
+    rn = csum(rn);
+    const double beta = rn / rr;
+    rr = rn;
+    for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+      const double2 rv = r[i], pv = p[i];
+      p[i] = make_double2(rv.x + beta * pv.x, rv.y + beta * pv.y);
+    }
+    cl.sync();  // the new p before any CTA applies the stencil to it
+  }
+  for (int i = i0 + threadIdx.x; i < i1; i += blockDim.x) out[(size_t)c * N + i] = make_float2((float)x[i].x, (float)x[i].y);
+  if (rank == 0 && threadIdx.x == 0 && iters) iters[c] = it;
 }
 
 // b1 <- |b1_c / sqrt(sum_c |b1_c|^2)| (coil_construction.cpp:428-444)
@@ -434,7 +524,7 @@ void launch_ta_combine(float2* crec, float2* u, int HW, int C, float scale, int 
 }
 void launch_h1_cg(const float2* u, const float2* crec, double mu, int W, int H, int C, int max_it, double rel_tol,
                   double2* work, double* muu, float2* out, int* iters, cudaStream_t s) {
-  h1_cg_kernel<<<C, 1024, 0, s>>>(u, crec, mu, W, H, max_it, rel_tol, work, muu, out, iters);
+  h1_cg_cluster_kernel<<<C * H1_CLUSTER, 1024, 0, s>>>(u, crec, mu, W, H, max_it, rel_tol, work, muu, out, iters);
 }
 void launch_h1_normalize(float2* b1, int HW, int C, cudaStream_t s) {
   h1_normalize_kernel<<<nb256(HW), 256, 0, s>>>(b1, HW, C);
