@@ -119,72 +119,8 @@ AVX_D double block_dsum(double v, double* red) {
   return r;
 }
 
-__global__ void __launch_bounds__(1024) h1_cg_kernel(const float2* u, const float2* crec, double mu, int W, int H,
-                                                     int max_it, double rel_tol, double2* work, double* muu_buf,
-                                                     float2* out, int* iters) {
-  __shared__ double red[32];
-  const int c = blockIdx.x;
-  const int N = W * H;
-  double2* x = work + (size_t)c * 4 * N;
-  double2* r = x + N;
-  double2* p = r + N;
-  double2* q = p + N;
-  double* muu = muu_buf + (size_t)c * N;
-  double rr = 0.0;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) {
-    const float2 uu = u[i];
-    const double au2 = (double)uu.x * uu.x + (double)uu.y * uu.y;
-    muu[i] = mu * au2;
-    const float2 cr = crec[(size_t)c * N + i];
-    const double ac = mu * sqrt((double)cr.x * cr.x + (double)cr.y * cr.y);
-    // conj(u) * mu |crec|
-    const double2 y = make_double2((double)uu.x * ac, -(double)uu.y * ac);
-    x[i] = make_double2(0.0, 0.0);
-    r[i] = y;
-    p[i] = y;
-    rr += y.x * y.x + y.y * y.y;
-  }
-  rr = block_dsum<1024>(rr, red);
-  const double rr0 = rr;
-  int it = 0;
-  for (; it < max_it && rr > rel_tol * rel_tol * rr0 && rr > 0.0; ++it) {
-    __syncthreads();
-    double pq = 0.0;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-      const double2 a = h1_apply(p, muu, i % W, i / W, W, H);
-      q[i] = a;
-      const double2 pv = p[i];
-      pq += pv.x * a.x + pv.y * a.y;
-    }
-    pq = block_dsum<1024>(pq, red);
-    const double alpha = rr / pq;
-    double rn = 0.0;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-      const double2 pv = p[i], qv = q[i];
-      double2 xv = x[i], rv = r[i];
-      xv.x += alpha * pv.x;
-      xv.y += alpha * pv.y;
-      rv.x -= alpha * qv.x;
-      rv.y -= alpha * qv.y;
-      x[i] = xv;
-      r[i] = rv;
-      rn += rv.x * rv.x + rv.y * rv.y;
-    }
-    rn = block_dsum<1024>(rn, red);
-    const double beta = rn / rr;
-    rr = rn;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
-      const double2 rv = r[i], pv = p[i];
-      p[i] = make_double2(rv.x + beta * pv.x, rv.y + beta * pv.y);
-    }
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < N; i += blockDim.x) out[(size_t)c * N + i] = make_float2((float)x[i].x, (float)x[i].y);
-  if (threadIdx.x == 0 && iters) iters[c] = it;
-}
-
-// The same CG with each coil's system spread over a cluster of H1_CLUSTER
-// CTAs (contiguous blocks of pixels per CTA).  The vectors stay in global
+// Each coil's system is solved by a cluster of H1_CLUSTER CTAs (contiguous
+// blocks of pixels per CTA).  The vectors stay in global
 // memory; the stencil reads its neighbours there after a cluster barrier
 // (release/acquire at cluster scope).  Every inner product is a block sum per
 // CTA, the CTA sums written into a slot of every CTA's shared memory, and one
