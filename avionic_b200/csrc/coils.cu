@@ -91,10 +91,8 @@ __global__ void ta_combine_kernel(float2* crec, float2* u, int HW, int C, float 
 
 // ---------------------------------------------------------------------------
 // H1 solve: (mu |u|^2 - Laplace_periodic) x = conj(u) mu |crec_c|, complex CG
-// in FP64, one CTA per coil (cg_forward_operation.h:47-70)
+// in FP64 (cg_forward_operation.h:47-70)
 // ---------------------------------------------------------------------------
-
-AVX_D double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 
 AVX_D double2 h1_apply(const double2* v, const double* muu, int x, int y, int W, int H) {
   const int i = y * W + x;
