@@ -62,6 +62,34 @@ avx_status fail(avx_status s, const std::string& msg) {
 // for the other requests' work (cudaFree would synchronise the device).
 thread_local cudaStream_t t_pool_stream = nullptr;
 
+// The library's own stream-ordered pool on the current device (created on
+// first use).  It keeps up to kPoolKeep bytes of freed memory for the next
+// allocations, so that repeated calls do not unmap and map memory; while a
+// batch engine lives it keeps everything (pool_hold).  The attributes of the
+// application's default pool are never changed.
+constexpr unsigned long long kPoolKeep = 4ull << 30;
+static cudaMemPool_t library_pool() {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = pools.find(dev);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props;
+  memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = dev;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+  unsigned long long keep = kPoolKeep;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools[dev] = pool;
+  return pool;
+}
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;
@@ -85,7 +113,9 @@ struct DevBuf {
     release();
     const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
     if (t_pool_stream) {
-      cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&p), bytes, t_pool_stream);
+      cudaMemPool_t pool = library_pool();
+      cudaError_t e = pool ? cudaMallocFromPoolAsync(reinterpret_cast<void**>(&p), bytes, pool, t_pool_stream)
+                           : cudaErrorMemoryAllocation;
       // the set-up code fills some buffers with synchronous copies on the
       // legacy stream: make the allocation visible to every stream first
       if (e == cudaSuccess) e = cudaStreamSynchronize(t_pool_stream);
@@ -100,6 +130,38 @@ struct DevBuf {
     cudaError_t e = cudaMalloc(&p, bytes);
     if (e == cudaSuccess) n = count;
     return e;
+  }
+};
+
+// A private stream for one synchronous entry point, ordered after the legacy
+// stream on entry; while it lives, DevBufs take their memory from the
+// stream-ordered pool on it (no device-wide synchronisation in cudaFree).
+// DevBufs declared after it release their memory on it before it syncs and
+// goes away.
+struct PoolScope {
+  cudaStream_t s = nullptr, prev = nullptr;
+  cudaError_t init() {
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      s = nullptr;
+      return e;
+    }
+    cudaEvent_t ev;
+    e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) {
+      e = cudaEventRecord(ev, 0);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
+      cudaEventDestroy(ev);
+    }
+    prev = t_pool_stream;
+    t_pool_stream = s;
+    return e;
+  }
+  ~PoolScope() {
+    if (!s) return;
+    cudaStreamSynchronize(s);
+    t_pool_stream = prev;
+    cudaStreamDestroy(s);
   }
 };
 
@@ -1559,23 +1621,6 @@ avx_status coil_estimate_on(int W, int H, int C, const avx_coil_params& p, float
 // (coil_construction.cpp:447-556): u0 (W*H, replaced by |u0|) and crec
 // (C*W*H).  Runs on a stream of its own (the loops' graphs need one), ordered
 // after s, and returns when it is done.
-avx_status coil_estimate(int W, int H, int C, const avx_coil_params& p, float2* u0p, float2* crecp, float2* u,
-                         float2* b1, cudaStream_t s) {
-  cudaStream_t cs;
-  cudaEvent_t ev;
-  AVX_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-  AVX_CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-  AVX_CK(cudaEventRecord(ev, s));
-  AVX_CK(cudaStreamWaitEvent(cs, ev, 0));
-  avx_status r = coil_estimate_on(W, H, C, p, u0p, crecp, u, b1, cs);
-  const cudaError_t e = cudaStreamSynchronize(cs);
-  cudaEventDestroy(ev);
-  cudaStreamDestroy(cs);
-  if (r != AVX_OK) return r;
-  AVX_CK(e);
-  return AVX_OK;
-}
-
 avx_status coil_construction(int W, int H, int C, int T, const avx_coil_params& p, const float2* kdata,
                              const float* mask, float2* u, float2* b1, cudaStream_t s) {
   DevBuf<float2> u0, crec;
@@ -1583,7 +1628,10 @@ avx_status coil_construction(int W, int H, int C, int T, const avx_coil_params& 
   AVX_CK(crec.alloc((size_t)C * W * H));
   avx_status r = coil_time_averaged(W, H, C, T, kdata, mask, u0.p, crec.p, 1, s);
   if (r != AVX_OK) return r;
-  return coil_estimate(W, H, C, p, u0.p, crec.p, u, b1, s);
+  r = coil_estimate_on(W, H, C, p, u0.p, crec.p, u, b1, s);
+  if (r != AVX_OK) return r;
+  AVX_CK(cudaStreamSynchronize(s));
+  return AVX_OK;
 }
 
 }  // namespace
@@ -2461,14 +2509,19 @@ avx_status avx_coil_construction_radial(unsigned W, unsigned H, unsigned C, unsi
   if (r != AVX_OK) return r;
   avx_coil_params dp;
   avx_coil_default_params(&dp);
+  PoolScope ps;
+  AVX_CK(ps.init());
   DevBuf<float2> u0, crec;
   AVX_CK(u0.alloc((size_t)W * H));
   AVX_CK(crec.alloc((size_t)C * W * H));
   r = coil_time_averaged_radial((int)W, (int)H, (int)C, (int)T, (int)S, d_traj, d_dens,
-                                reinterpret_cast<const float2*>(d_kdata), u0.p, crec.p, 1, 0);
+                                reinterpret_cast<const float2*>(d_kdata), u0.p, crec.p, 1, ps.s);
   if (r != AVX_OK) return r;
-  return coil_estimate((int)W, (int)H, (int)C, p ? *p : dp, u0.p, crec.p, reinterpret_cast<float2*>(d_u),
-                       reinterpret_cast<float2*>(d_b1), 0);
+  r = coil_estimate_on((int)W, (int)H, (int)C, p ? *p : dp, u0.p, crec.p, reinterpret_cast<float2*>(d_u),
+                       reinterpret_cast<float2*>(d_b1), ps.s);
+  if (r != AVX_OK) return r;
+  AVX_CK(cudaStreamSynchronize(ps.s));
+  return AVX_OK;
 }
 
 avx_status avx_coil_construction(unsigned W, unsigned H, unsigned C, unsigned T, const avx_coil_params* p,
@@ -2478,8 +2531,10 @@ avx_status avx_coil_construction(unsigned W, unsigned H, unsigned C, unsigned T,
   if (r != AVX_OK) return r;
   avx_coil_params dp;
   avx_coil_default_params(&dp);
+  PoolScope ps;
+  AVX_CK(ps.init());
   return coil_construction((int)W, (int)H, (int)C, (int)T, p ? *p : dp, reinterpret_cast<const float2*>(d_kdata),
-                           d_mask, reinterpret_cast<float2*>(d_u), reinterpret_cast<float2*>(d_b1), 0);
+                           d_mask, reinterpret_cast<float2*>(d_u), reinterpret_cast<float2*>(d_b1), ps.s);
 }
 
 // ---------------------------------------------------------------------------
@@ -2888,6 +2943,36 @@ avx_status avx_query_workspace(const avx_request* r, size_t* bytes) {
   return AVX_OK;
 }
 
+// The device's default memory pool keeps freed memory (release threshold
+// unlimited) while at least one engine lives on the device; when the last one
+// goes, the previous threshold comes back and the unused memory is returned,
+// so that later synchronous allocations of the process find it free.
+static avx_status pool_hold(int device, bool acquire) {
+  static std::mutex mu;
+  static std::map<int, int> held;  // device -> live engines
+  std::lock_guard<std::mutex> lk(mu);
+  int cur = 0;
+  AVX_CK(cudaGetDevice(&cur));
+  AVX_CK(cudaSetDevice(device));
+  cudaMemPool_t pool = library_pool();
+  cudaSetDevice(cur);
+  if (!pool) return fail(AVX_E_CUDA, "cannot create the library's memory pool");
+  int& h = held[device];
+  if (acquire) {
+    if (h++ == 0) {
+      unsigned long long keep = ~0ull;
+      AVX_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
+    return AVX_OK;
+  }
+  if (h > 0 && --h == 0) {
+    unsigned long long keep = kPoolKeep;
+    AVX_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    AVX_CK(cudaMemPoolTrimTo(pool, kPoolKeep));
+  }
+  return AVX_OK;
+}
+
 avx_status avx_batch_create(int device, size_t hbm_budget, int workers, avx_batch** out) {
   if (!out || workers < 1 || hbm_budget == 0) return fail(AVX_E_ARG, "invalid batch engine arguments");
   int n = 0;
@@ -2896,11 +2981,10 @@ avx_status avx_batch_create(int device, size_t hbm_budget, int workers, avx_batc
   AVX_CK(cudaSetDevice(device));
   avx_status r = configure_once();
   if (r != AVX_OK) return r;
-  // keep freed pool memory for the next requests instead of returning it to the driver
-  cudaMemPool_t pool;
-  AVX_CK(cudaDeviceGetDefaultMemPool(&pool, device));
-  unsigned long long keep = ~0ull;
-  AVX_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  // keep freed pool memory for the next requests instead of returning it to
+  // the driver while an engine lives on the device (pool_hold)
+  r = pool_hold(device, true);
+  if (r != AVX_OK) return r;
   avx_batch* b = new avx_batch();
   b->device = device;
   b->budget = hbm_budget;
@@ -2927,6 +3011,7 @@ avx_status avx_batch_create(int device, size_t hbm_budget, int workers, avx_batc
     for (cudaStream_t s : b->streams) cudaStreamDestroy(s);
     for (cudaEvent_t e : b->events) cudaEventDestroy(e);
     delete b;
+    pool_hold(device, false);
     return st;
   }
   memset(b->h_states, 0, sizeof(DevState) * 2 * slots);
@@ -3002,7 +3087,9 @@ void avx_batch_destroy(avx_batch* b) {
   }
   for (cudaEvent_t e : b->events) cudaEventDestroy(e);
   cudaFreeHost(b->h_states);
+  const int dev = b->device;
   delete b;
+  pool_hold(dev, false);
 }
 
 }  // extern "C"
