@@ -856,6 +856,7 @@ static avx_status autotune(avx_solver* s, const float2* b1) {
   PDArgs a = make_pdargs(s);
   float best = 0.f;
   for (int i = 0; i < AVX_PRIMAL_TILES; ++i) {
+    if (i >= 5 && !avx::dual_pairs(s->method, s->W)) break;
     a.primal_tile = i;
     float ms;
     avx_status r = time_launches(s, avx::launch_primal, a, &ms);
@@ -867,6 +868,7 @@ static avx_status autotune(avx_solver* s, const float2* b1) {
   }
   a.primal_tile = s->primal_tile;
   for (int i = 0; i < AVX_DUAL_BLOCKS; ++i) {
+    if (i >= 3 && !avx::dual_pairs(s->method, s->W)) break;
     a.dual_block = i;
     float ms;
     avx_status r = time_launches(s, avx::launch_dual, a, &ms);

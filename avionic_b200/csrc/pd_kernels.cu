@@ -136,6 +136,353 @@ __global__ void __launch_bounds__(NT) dual_kernel(PDArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// dual update, two pixels per thread (x0, x0 + 1 with x0 even; W even) for
+// TGV2 / ICTGV2: every field is read and written as 128-bit pairs, the
+// stencil neighbours along y and t as pairs too, along x the one value past
+// each end.  Per pixel the arithmetic of dual_kernel (results agree to
+// rounding: the compiler may fuse multiply-adds differently).
+// ---------------------------------------------------------------------------
+
+struct V2 {
+  float2 a, b;  // pixel x0, x0 + 1
+};
+AVX_D V2 ld4(const float2* p, long long i) {
+  const float4 v = __ldg(reinterpret_cast<const float4*>(p + i));
+  return V2{make_float2(v.x, v.y), make_float2(v.z, v.w)};
+}
+AVX_D void st4(float2* p, long long i, float2 a, float2 b) {
+  *reinterpret_cast<float4*>(p + i) = make_float4(a.x, a.y, b.x, b.y);
+}
+
+// neighbourhood of one field at a pixel pair
+struct Nb {
+  V2 c, yp, ym, tp, tm;
+  float2 xp, xm;  // x0 + 2, x0 - 1
+};
+
+template <bool FWD, bool BWD>
+AVX_D Nb load_nb(const float2* u, long long i, int x0, int y, int t, int W, int H, int T, long long sW, long long sWH) {
+  Nb n;
+  n.c = ld4(u, i);
+  if (FWD) {
+    n.xp = (x0 + 2 < W) ? __ldg(u + i + 2) : czero();
+    n.yp = (y < H - 1) ? ld4(u, i + sW) : V2{czero(), czero()};
+    n.tp = (t < T - 1) ? ld4(u, i + sWH) : V2{czero(), czero()};
+  }
+  if (BWD) {
+    n.xm = (x0 > 0) ? __ldg(u + i - 1) : czero();
+    n.ym = (y > 0) ? ld4(u, i - sW) : V2{czero(), czero()};
+    n.tm = (t > 0) ? ld4(u, i - sWH) : V2{czero(), czero()};
+  }
+  return n;
+}
+
+// per pixel k (0, 1) of the pair: the values stencil.cuh reads
+AVX_D float2 pick(const V2& v, int k) { return k ? v.b : v.a; }
+AVX_D float2 nb_xp(const Nb& n, int k) { return k ? n.xp : n.c.b; }  // u(i + 1)
+AVX_D float2 nb_xm(const Nb& n, int k) { return k ? n.c.a : n.xm; }  // u(i - 1)
+
+// d_fwd of stencil.cuh along x / y / t for pixel k
+AVX_D float2 fx(const Nb& n, int k, int x, int W) { return (x < W - 1) ? csub(nb_xp(n, k), pick(n.c, k)) : czero(); }
+AVX_D float2 fy(const Nb& n, int k, int y, int H) { return (y < H - 1) ? csub(pick(n.yp, k), pick(n.c, k)) : czero(); }
+AVX_D float2 ft(const Nb& n, int k, int t, int T) { return (t < T - 1) ? csub(pick(n.tp, k), pick(n.c, k)) : czero(); }
+// d_fwd2: D+ of (u - v), the difference formed first
+AVX_D float2 fx2(const Nb& u, const Nb& v, int k, int x, int W) {
+  if (x >= W - 1) return czero();
+  return csub(csub(nb_xp(u, k), nb_xp(v, k)), csub(pick(u.c, k), pick(v.c, k)));
+}
+AVX_D float2 fy2(const Nb& u, const Nb& v, int k, int y, int H) {
+  if (y >= H - 1) return czero();
+  return csub(csub(pick(u.yp, k), pick(v.yp, k)), csub(pick(u.c, k), pick(v.c, k)));
+}
+AVX_D float2 ft2(const Nb& u, const Nb& v, int k, int t, int T) {
+  if (t >= T - 1) return czero();
+  return csub(csub(pick(u.tp, k), pick(v.tp, k)), csub(pick(u.c, k), pick(v.c, k)));
+}
+// d_bwd
+AVX_D float2 bx(const Nb& n, int k, int x, int W) {
+  const float2 a = (x < W - 1) ? pick(n.c, k) : czero();
+  const float2 b = (x > 0) ? nb_xm(n, k) : czero();
+  return csub(a, b);
+}
+AVX_D float2 by(const Nb& n, int k, int y, int H) {
+  const float2 a = (y < H - 1) ? pick(n.c, k) : czero();
+  const float2 b = (y > 0) ? pick(n.ym, k) : czero();
+  return csub(a, b);
+}
+AVX_D float2 bt(const Nb& n, int k, int t, int T) {
+  const float2 a = (t < T - 1) ? pick(n.c, k) : czero();
+  const float2 b = (t > 0) ? pick(n.tm, k) : czero();
+  return csub(a, b);
+}
+
+template <int M, int NT>
+__global__ void __launch_bounds__(NT) dual_vec_kernel(PDArgs a) {
+  if (a.st->stop) return;
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) a.st->iters += 1;
+  const int HW2 = (a.W >> 1) * a.H;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= HW2) return;
+  const int t = blockIdx.y;
+  const int y = j / (a.W >> 1);
+  const int x0 = 2 * (j - y * (a.W >> 1));
+  const long long sW = a.W, sWH = (long long)a.W * a.H;
+  const long long i = x0 + sW * y + sWH * t;
+  const float sig = (float)a.st->sigma;
+  // branch 1
+  {
+    V2 y1v[3], y2v[6];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) y1v[k] = ld4(a.y[k], i);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) y2v[k] = ld4(a.y[3 + k], i);
+    const Nb u = load_nb<true, false>(a.xb[0], i, x0, y, t, a.W, a.H, a.T, sW, sWH);
+    Nb w;
+    if (M == AVX_M_ICTGV2) w = load_nb<true, false>(a.xb[4], i, x0, y, t, a.W, a.H, a.T, sW, sWH);
+    const Nb v0 = load_nb<false, true>(a.xb[1], i, x0, y, t, a.W, a.H, a.T, sW, sWH);
+    const Nb v1 = load_nb<false, true>(a.xb[2], i, x0, y, t, a.W, a.H, a.T, sW, sWH);
+    const Nb v2 = load_nb<false, true>(a.xb[3], i, x0, y, t, a.W, a.H, a.T, sW, sWH);
+    float2 o1[2][3], o2[2][6];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int x = x0 + k;
+      float2 g[3], e[6], y1[3], y2[6];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) y1[c] = pick(y1v[c], k);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) y2[c] = pick(y2v[c], k);
+      if (M == AVX_M_TGV2) {
+        g[0] = cscale(fx(u, k, x, a.W), a.w1.ix);
+        g[1] = cscale(fy(u, k, y, a.H), a.w1.iy);
+        g[2] = cscale(ft(u, k, t, a.T), a.w1.it);
+      } else {
+        g[0] = cscale(fx2(u, w, k, x, a.W), a.w1.ix);
+        g[1] = cscale(fy2(u, w, k, y, a.H), a.w1.iy);
+        g[2] = cscale(ft2(u, w, k, t, a.T), a.w1.it);
+      }
+      e[0] = cscale(bx(v0, k, x, a.W), a.w1.ix);
+      e[1] = cscale(by(v1, k, y, a.H), a.w1.iy);
+      e[2] = cscale(bt(v2, k, t, a.T), a.w1.it);
+      e[3] = cadd(cscale(by(v0, k, y, a.H), a.w1.hy), cscale(bx(v1, k, x, a.W), a.w1.hx));
+      e[4] = cadd(cscale(bt(v0, k, t, a.T), a.w1.ht), cscale(bx(v2, k, x, a.W), a.w1.hx));
+      e[5] = cadd(cscale(bt(v1, k, t, a.T), a.w1.ht), cscale(by(v2, k, y, a.H), a.w1.hx));
+      const Nb* vv[3] = {&v0, &v1, &v2};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float2 d = csub(g[c], pick(vv[c]->c, k));
+        y1[c] = make_float2(y1[c].x + sig * d.x, y1[c].y + sig * d.y);
+      }
+      prox_div<3>(y1, nrm3(y1), a.r1);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) y2[c] = make_float2(y2[c].x + sig * e[c].x, y2[c].y + sig * e[c].y);
+      prox_div<6>(y2, nrm6(y2), a.r2);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) o1[k][c] = y1[c];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) o2[k][c] = y2[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) st4(a.y[c], i, o1[0][c], o1[1][c]);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) st4(a.y[3 + c], i, o2[0][c], o2[1][c]);
+  }
+  if (M == AVX_M_ICTGV2) {
+    V2 y3v[3], y4v[6];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) y3v[k] = ld4(a.y[9 + k], i);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) y4v[k] = ld4(a.y[12 + k], i);
+    const Nb w = load_nb<true, false>(a.xb[4], i, x0, y, t, a.W, a.H, a.T, sW, sWH);
+    const Nb v0 = load_nb<false, true>(a.xb[5], i, x0, y, t, a.W, a.H, a.T, sW, sWH);
+    const Nb v1 = load_nb<false, true>(a.xb[6], i, x0, y, t, a.W, a.H, a.T, sW, sWH);
+    const Nb v2 = load_nb<false, true>(a.xb[7], i, x0, y, t, a.W, a.H, a.T, sW, sWH);
+    float2 o1[2][3], o2[2][6];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int x = x0 + k;
+      float2 g[3], e[6], y3[3], y4[6];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) y3[c] = pick(y3v[c], k);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) y4[c] = pick(y4v[c], k);
+      g[0] = cscale(fx(w, k, x, a.W), a.w2.ix);
+      g[1] = cscale(fy(w, k, y, a.H), a.w2.iy);
+      g[2] = cscale(ft(w, k, t, a.T), a.w2.it);
+      e[0] = cscale(bx(v0, k, x, a.W), a.w2.ix);
+      e[1] = cscale(by(v1, k, y, a.H), a.w2.iy);
+      e[2] = cscale(bt(v2, k, t, a.T), a.w2.it);
+      e[3] = cadd(cscale(by(v0, k, y, a.H), a.w2.hy), cscale(bx(v1, k, x, a.W), a.w2.hx));
+      e[4] = cadd(cscale(bt(v0, k, t, a.T), a.w2.ht), cscale(bx(v2, k, x, a.W), a.w2.hx));
+      e[5] = cadd(cscale(bt(v1, k, t, a.T), a.w2.ht), cscale(by(v2, k, y, a.H), a.w2.hx));
+      const Nb* vv[3] = {&v0, &v1, &v2};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float2 d = csub(g[c], pick(vv[c]->c, k));
+        y3[c] = make_float2(y3[c].x + sig * d.x, y3[c].y + sig * d.y);
+      }
+      prox_div<3>(y3, nrm3(y3), a.r3);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) y4[c] = make_float2(y4[c].x + sig * e[c].x, y4[c].y + sig * e[c].y);
+      prox_div<6>(y4, nrm6(y4), a.r4);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) o1[k][c] = y3[c];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) o2[k][c] = y4[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) st4(a.y[9 + c], i, o1[0][c], o1[1][c]);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) st4(a.y[12 + c], i, o2[0][c], o2[1][c]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// primal update, two pixels per thread (W even) for TGV2 / ICTGV2, with
+// 128-bit accesses as in dual_vec_kernel; per pixel the arithmetic of
+// primal_kernel
+// ---------------------------------------------------------------------------
+
+// d_fwd_t / d_bwd_t of stencil.cuh for pixel k of a pair
+AVX_D float2 tfx(const Nb& n, int k, int x, int W) {
+  const float2 a = (x > 0) ? nb_xm(n, k) : czero();
+  const float2 b = (x < W - 1) ? pick(n.c, k) : czero();
+  return csub(a, b);
+}
+AVX_D float2 tfy(const Nb& n, int k, int y, int H) {
+  const float2 a = (y > 0) ? pick(n.ym, k) : czero();
+  const float2 b = (y < H - 1) ? pick(n.c, k) : czero();
+  return csub(a, b);
+}
+AVX_D float2 tft(const Nb& n, int k, int t, int T) {
+  const float2 a = (t > 0) ? pick(n.tm, k) : czero();
+  const float2 b = (t < T - 1) ? pick(n.c, k) : czero();
+  return csub(a, b);
+}
+AVX_D float2 tbx(const Nb& n, int k, int x, int W) { return (x < W - 1) ? csub(pick(n.c, k), nb_xp(n, k)) : czero(); }
+AVX_D float2 tby(const Nb& n, int k, int y, int H) { return (y < H - 1) ? csub(pick(n.c, k), pick(n.yp, k)) : czero(); }
+AVX_D float2 tbt(const Nb& n, int k, int t, int T) { return (t < T - 1) ? csub(pick(n.c, k), pick(n.tp, k)) : czero(); }
+
+// the pair's neighbours that one field needs: bit 0 x+1, 1 y+1, 2 t+1, 3 x-1, 4 y-1, 5 t-1
+template <int F>
+AVX_D Nb load_sel(const float2* u, long long i, int x0, int y, int t, int W, int H, int T, long long sW,
+                  long long sWH) {
+  Nb n;
+  const V2 z{czero(), czero()};
+  n.c = ld4(u, i);
+  n.xp = (F & 1) && x0 + 2 < W ? __ldg(u + i + 2) : czero();
+  n.yp = (F & 2) && y < H - 1 ? ld4(u, i + sW) : z;
+  n.tp = (F & 4) && t < T - 1 ? ld4(u, i + sWH) : z;
+  n.xm = (F & 8) && x0 > 0 ? __ldg(u + i - 1) : czero();
+  n.ym = (F & 16) && y > 0 ? ld4(u, i - sW) : z;
+  n.tm = (F & 32) && t > 0 ? ld4(u, i - sWH) : z;
+  return n;
+}
+
+// div3 (D- transposed of the gradient, negated) and symdiv of one branch for pixel k
+struct DivBranch {
+  Nb y0, y1, y2, w0, w1, w2, w3, w4, w5;
+};
+AVX_D DivBranch load_branch(float2* const* yv, long long i, int x0, int y, int t, int W, int H, int T, long long sW,
+                            long long sWH, bool sym) {
+  DivBranch b;
+  b.y0 = load_sel<8>(yv[0], i, x0, y, t, W, H, T, sW, sWH);
+  b.y1 = load_sel<16>(yv[1], i, x0, y, t, W, H, T, sW, sWH);
+  b.y2 = load_sel<32>(yv[2], i, x0, y, t, W, H, T, sW, sWH);
+  if (sym) {
+    b.w0 = load_sel<1>(yv[3], i, x0, y, t, W, H, T, sW, sWH);
+    b.w1 = load_sel<2>(yv[4], i, x0, y, t, W, H, T, sW, sWH);
+    b.w2 = load_sel<4>(yv[5], i, x0, y, t, W, H, T, sW, sWH);
+    b.w3 = load_sel<3>(yv[6], i, x0, y, t, W, H, T, sW, sWH);
+    b.w4 = load_sel<5>(yv[7], i, x0, y, t, W, H, T, sW, sWH);
+    b.w5 = load_sel<6>(yv[8], i, x0, y, t, W, H, T, sW, sWH);
+  }
+  return b;
+}
+AVX_D float2 pair_div3(const DivBranch& b, int k, int x, int y, int t, int W, int H, int T, const Wts& w) {
+  float2 a = cscale(tfx(b.y0, k, x, W), w.ix);
+  a = cadd(a, cscale(tfy(b.y1, k, y, H), w.iy));
+  a = cadd(a, cscale(tft(b.y2, k, t, T), w.it));
+  return make_float2(-a.x, -a.y);
+}
+AVX_D void pair_symdiv(const DivBranch& b, int k, int x, int y, int t, int W, int H, int T, const Wts& w,
+                       float2 (&d)[3]) {
+  float2 a = cscale(tbx(b.w0, k, x, W), w.ix);
+  a = cadd(a, cscale(tby(b.w3, k, y, H), w.iy));
+  a = cadd(a, cscale(tbt(b.w4, k, t, T), w.it));
+  d[0] = make_float2(-a.x, -a.y);
+  a = cscale(tbx(b.w3, k, x, W), w.ix);
+  a = cadd(a, cscale(tby(b.w1, k, y, H), w.iy));
+  a = cadd(a, cscale(tbt(b.w5, k, t, T), w.it));
+  d[1] = make_float2(-a.x, -a.y);
+  a = cscale(tbx(b.w4, k, x, W), w.ix);
+  a = cadd(a, cscale(tby(b.w5, k, y, H), w.iy));
+  a = cadd(a, cscale(tbt(b.w2, k, t, T), w.it));
+  d[2] = make_float2(-a.x, -a.y);
+}
+
+template <int M, int NT>
+__global__ void __launch_bounds__(NT) primal_vec_kernel(PDArgs a) {
+  if (a.st->stop) return;
+  constexpr int P = MethodDims<M>::P;
+  const int HW2 = (a.W >> 1) * a.H;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= HW2) return;
+  const int t = blockIdx.y;
+  const int y = j / (a.W >> 1);
+  const int x0 = 2 * (j - y * (a.W >> 1));
+  const long long sW = a.W, sWH = (long long)a.W * a.H;
+  const long long i = x0 + sW * y + sWH * t;
+  const float tau = (float)a.st->tau;
+  const V2 kh = ld4(a.khz, i);
+  const DivBranch b1 = load_branch(a.y, i, x0, y, t, a.W, a.H, a.T, sW, sWH, true);
+  DivBranch b2;
+  if (M == AVX_M_ICTGV2) b2 = load_branch(a.y + 9, i, x0, y, t, a.W, a.H, a.T, sW, sWH, true);
+  V2 xo[8];
+#pragma unroll
+  for (int c = 0; c < P; ++c) xo[c] = ld4(a.x[c], i);
+  float2 xn[2][8], xbv[2][8];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int x = x0 + k;
+    const float2 dv1 = pair_div3(b1, k, x, y, t, a.W, a.H, a.T, a.w1);
+    float2 sd1[3], y1[3], sd2[3], y3[3];
+    float2 dv3 = czero();
+    pair_symdiv(b1, k, x, y, t, a.W, a.H, a.T, a.w1, sd1);
+    y1[0] = pick(b1.y0.c, k);
+    y1[1] = pick(b1.y1.c, k);
+    y1[2] = pick(b1.y2.c, k);
+    if (M == AVX_M_ICTGV2) {
+      dv3 = pair_div3(b2, k, x, y, t, a.W, a.H, a.T, a.w2);
+      pair_symdiv(b2, k, x, y, t, a.W, a.H, a.T, a.w2, sd2);
+      y3[0] = pick(b2.y0.c, k);
+      y3[1] = pick(b2.y1.c, k);
+      y3[2] = pick(b2.y2.c, k);
+    }
+    float2 r[8];
+    r[0] = csub(dv1, pick(kh, k));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) r[1 + c] = cadd(y1[c], sd1[c]);
+    if (M == AVX_M_ICTGV2) {
+      r[4] = csub(dv3, dv1);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) r[5 + c] = cadd(y3[c], sd2[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < P; ++c) {
+      const float2 o = pick(xo[c], k);
+      const float2 n = make_float2(o.x + tau * r[c].x, o.y + tau * r[c].y);
+      xn[k][c] = n;
+      xbv[k][c] = make_float2(2.f * n.x - o.x, 2.f * n.y - o.y);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < P; ++c) {
+    st4(a.x[c], i, xn[0][c], xn[1][c]);
+    st4(a.xb[c], i, xbv[0][c], xbv[1][c]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // y-transform: frame t, a strip of YD_XS image columns, every coil.
 //   P[t,c,k,x] = 1/sqrt(H) sum_y e^{+2 pi i (ky_k-sy)(y-sy)/H} b1[c,y,x] u[t,y,x]
 // (u = in - in2 when in2 is given), written into k.qp in the compact layout
@@ -890,8 +1237,9 @@ static void rec(cudaEvent_t* ev, int i, cudaStream_t s) {
 // tuning tables (AVX_PRIMAL_TILES, AVX_DUAL_BLOCKS entries, in the order of
 // the switches below); 32 x 8 x 1 and 256 threads measured fastest at
 // 192 x 192 x 30 ICTGV2 (primal 68 us against 90 us for 32 x 4 x 4)
-static const char* kPrimalTileNames[AVX_PRIMAL_TILES] = {"32x8x1", "32x4x2", "64x4x1", "32x4x4", "32x16x1"};
-static const int kDualBlocks[AVX_DUAL_BLOCKS] = {256, 128, 512};
+static const char* kPrimalTileNames[AVX_PRIMAL_TILES] = {"32x8x1", "32x4x2", "64x4x1", "32x4x4", "32x16x1",
+                                                          "128x1 pairs", "256x1 pairs"};
+static const int kDualBlocks[AVX_DUAL_BLOCKS] = {256, 128, 512, 256, 128, 512};
 
 const char* primal_tile_name(int i) { return kPrimalTileNames[(i >= 0 && i < AVX_PRIMAL_TILES) ? i : 0]; }
 int dual_block_threads(int i) { return kDualBlocks[(i >= 0 && i < AVX_DUAL_BLOCKS) ? i : 0]; }
@@ -906,7 +1254,24 @@ static void launch_dual_nt(int method, const PDArgs& a, cudaStream_t s) {
   else dual_kernel<AVX_M_ICTGV2, NT><<<gd, NT, 0, s>>>(a);
 }
 
+bool dual_pairs(int method, int W) { return (method == AVX_M_TGV2 || method == AVX_M_ICTGV2) && W % 2 == 0; }
+
+template <int NT>
+static void launch_dual_vec(int method, const PDArgs& a, cudaStream_t s) {
+  dim3 gd(((a.W / 2) * a.H + NT - 1) / NT, a.T);
+  if (method == AVX_M_TGV2) dual_vec_kernel<AVX_M_TGV2, NT><<<gd, NT, 0, s>>>(a);
+  else dual_vec_kernel<AVX_M_ICTGV2, NT><<<gd, NT, 0, s>>>(a);
+}
+
 void launch_dual(int method, const PDArgs& a, cudaStream_t s) {
+  if (a.dual_block >= 3 && dual_pairs(method, a.W)) {
+    switch (dual_block_threads(a.dual_block)) {
+      case 128: launch_dual_vec<128>(method, a, s); break;
+      case 512: launch_dual_vec<512>(method, a, s); break;
+      default: launch_dual_vec<256>(method, a, s); break;
+    }
+    return;
+  }
   switch (dual_block_threads(a.dual_block)) {
     case 128: launch_dual_nt<128>(method, a, s); break;
     case 512: launch_dual_nt<512>(method, a, s); break;
@@ -925,7 +1290,21 @@ static void launch_primal_tile(int method, const PDArgs& a, cudaStream_t s) {
   else primal_kernel<AVX_M_ICTGV2, TX, TY, YP><<<gp, bl, 0, s>>>(a);
 }
 
+template <int NT>
+static void launch_primal_vec(int method, const PDArgs& a, cudaStream_t s) {
+  dim3 gd(((a.W / 2) * a.H + NT - 1) / NT, a.T);
+  if (method == AVX_M_TGV2) primal_vec_kernel<AVX_M_TGV2, NT><<<gd, NT, 0, s>>>(a);
+  else primal_vec_kernel<AVX_M_ICTGV2, NT><<<gd, NT, 0, s>>>(a);
+}
+
 void launch_primal(int method, const PDArgs& a, cudaStream_t s) {
+  if (a.primal_tile >= 5 && dual_pairs(method, a.W)) {
+    if (a.primal_tile == 5)
+      launch_primal_vec<128>(method, a, s);
+    else
+      launch_primal_vec<256>(method, a, s);
+    return;
+  }
   switch (a.primal_tile) {
     case 1: launch_primal_tile<32, 4, 2>(method, a, s); break;
     case 2: launch_primal_tile<64, 4, 1>(method, a, s); break;

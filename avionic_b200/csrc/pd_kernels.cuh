@@ -20,8 +20,8 @@
 // Launch shapes the autotuner chooses from (PDArgs::primal_tile, dual_block):
 // primal tiles (threads along x, threads along y, pixels per thread along y)
 // and dual-kernel block sizes; index 0 of each is the untuned default.
-#define AVX_PRIMAL_TILES 5
-#define AVX_DUAL_BLOCKS 3
+#define AVX_PRIMAL_TILES 7  // 0-4: one pixel per thread; 5-6: pairs (TGV2 / ICTGV2 with even W)
+#define AVX_DUAL_BLOCKS 6  // 0-2: one pixel per thread; 3-5: two (TGV2 / ICTGV2 with even W)
 
 // timed stages of one iteration (avx_solver_kernel_times)
 #define AVX_NSTAGE 5
@@ -50,6 +50,7 @@ void launch_dual(int method, const PDArgs& a, cudaStream_t s);
 void launch_primal(int method, const PDArgs& a, cudaStream_t s);
 // the shape behind a tuning index: primal tile "TXxTYxYP", dual block "N threads"
 const char* primal_tile_name(int i);
+bool dual_pairs(int method, int W);  // the two-pixel dual and primal kernels apply
 int dual_block_threads(int i);
 void launch_ydft(const KArgs& k, cudaStream_t s);
 void launch_rows(const KArgs& k, int mode, cudaStream_t s);

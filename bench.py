@@ -856,6 +856,7 @@ def main():
         "rel_l2_vs_oracle": err_oracle,
         "details": {"parallelism": "one independent reconstruction per GPU", "graphs": True,
                     "tuning": {"primal_tile": tuning[2], "dual_block_threads": tuning[3],
+                               "dual_pixels_per_thread": 2 if tuning[1] >= 3 else 1,
                                "row_fft_rows_per_pass": row_schedule[0],
                                "row_fft_plan": "run-time" if row_schedule[1] else "compile-time"},
                     "dft": args.dft, "other_dft_form": other,

@@ -196,10 +196,13 @@ avx_status avx_solver_set_stream(avx_solver* s, void* cuda_stream);          /* 
  * (the default) the first run of a (device, method, W, H, T) times each
  * candidate on the solver's own fields, keeps the fastest and reuses it for
  * later runs and solvers of that shape in the process; with autotune clear
- * the given indices are used.  primal_tile in [0, 5): 32x8x1, 32x4x2, 64x4x1,
+ * the given indices are used.  primal_tile in [0, 7): 32x8x1, 32x4x2, 64x4x1,
  * 32x4x4, 32x16x1 (threads along x, threads along y, pixels per thread along
- * y); dual_block in [0, 3): 256, 128, 512 threads.  Index 0 is the default
- * shape.  The shapes change the schedule only: every pixel's arithmetic is
+ * y), then 128 and 256 threads with two pixels per thread and 128-bit
+ * accesses (TGV2 and ICTGV2 with an even width; otherwise tile 0); dual_block in [0, 6): 256, 128, 512 threads with one pixel per thread,
+ * then 256, 128, 512 threads with two pixels per thread and 128-bit
+ * accesses (TGV2 and ICTGV2 with an even width; otherwise the one-pixel
+ * kernel of that block size).  Index 0 is the default shape.  The shapes change the schedule only: every pixel's arithmetic is
  * the same in all of them (results agree to rounding; the compiler may fuse
  * multiply-adds differently in each). */
 avx_status avx_solver_set_tuning(avx_solver* s, int autotune, int primal_tile, int dual_block);
