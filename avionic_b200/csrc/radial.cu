@@ -523,6 +523,21 @@ __global__ void rad_iota_kernel(int* v, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
 }
 
+// stream-ordered scratch memory, returned on its stream when it goes out of scope
+struct AsyncScratch {
+  void* p = nullptr;
+  cudaStream_t s;
+  explicit AsyncScratch(cudaStream_t st) : s(st) {}
+  ~AsyncScratch() {
+    if (p) cudaFreeAsync(p, s);
+  }
+  cudaError_t alloc(size_t bytes) { return cudaMallocAsync(&p, bytes, s); }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
 static int key_bits(long long n) {
   int b = 1;
   while ((1ll << b) < n) ++b;
@@ -531,14 +546,13 @@ static int key_bits(long long n) {
 
 cudaError_t rad_validate(const float* traj, long long nt, const float* dens, long long nd, int* flags_host,
                          cudaStream_t s) {
-  int* d = nullptr;
-  cudaError_t e = cudaMallocAsync(&d, sizeof(int), s);
+  AsyncScratch d(s);
+  cudaError_t e = d.alloc(sizeof(int));
+  if (e == cudaSuccess) e = cudaMemsetAsync(d.p, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
-  cudaMemsetAsync(d, 0, sizeof(int), s);
-  rad_validate_kernel<<<148 * 8, 256, 0, s>>>(traj, nt, dens, nd, d);
-  cudaMemcpyAsync(flags_host, d, sizeof(int), cudaMemcpyDeviceToHost, s);
-  cudaFreeAsync(d, s);
-  e = cudaStreamSynchronize(s);
+  rad_validate_kernel<<<148 * 8, 256, 0, s>>>(traj, nt, dens, nd, d.as<int>());
+  e = cudaMemcpyAsync(flags_host, d.p, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e == cudaSuccess) e = cudaGetLastError();
   return e;
 }
@@ -547,52 +561,46 @@ cudaError_t rad_build_order(const RadialGeomDev& g, const float* dens, float* sq
                             cudaStream_t s) {
   const long long n = (long long)g.T * g.S;
   const long long nk = (long long)g.T * g.nsx * g.nsy;
-  int *key = nullptr, *key2 = nullptr, *val = nullptr, *cnt = nullptr, *off = nullptr;
-  void* tmp = nullptr;
   size_t tb_sort = 0, tb_scan = 0;
-  cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, tb_sort, key, key2, val, order, (int)n, 0, key_bits(nk), s);
-  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb_scan, cnt, off, (int)nk, s);
-  if (e == cudaSuccess) e = cudaMallocAsync(&key, 2 * n * sizeof(int) + n * sizeof(int), s);
-  if (e == cudaSuccess) e = cudaMallocAsync(&cnt, 2 * (nk + 1) * sizeof(int), s);
-  if (e == cudaSuccess) e = cudaMallocAsync(&tmp, std::max(tb_sort, tb_scan) + 16, s);
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, tb_sort, (int*)nullptr, (int*)nullptr, (int*)nullptr,
+                                                  order, (int)n, 0, key_bits(nk), s);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb_scan, (int*)nullptr, (int*)nullptr, (int)nk, s);
+  AsyncScratch keys(s), counts(s), tmp(s);
+  if (e == cudaSuccess) e = keys.alloc(3 * n * sizeof(int));
+  if (e == cudaSuccess) e = counts.alloc(2 * (nk + 1) * sizeof(int));
+  if (e == cudaSuccess) e = tmp.alloc(std::max(tb_sort, tb_scan) + 16);
+  if (e == cudaSuccess) e = cudaMemsetAsync(counts.p, 0, (nk + 1) * sizeof(int), s);
   if (e != cudaSuccess) return e;
-  key2 = key + n;
-  val = key + 2 * n;
-  off = cnt + nk + 1;
-  cudaMemsetAsync(cnt, 0, (nk + 1) * sizeof(int), s);
+  int *key = keys.as<int>(), *key2 = key + n, *val = key + 2 * n;
+  int *cnt = counts.as<int>(), *off = cnt + nk + 1;
   const int nb = (int)std::min<long long>((n + 255) / 256, 148 * 16);
   rad_keys_kernel<<<nb, 256, 0, s>>>(g, dens, sqrt_w, key, val, cnt);
   // a stable sort: within a key, samples stay in index order
-  e = cub::DeviceRadixSort::SortPairs(tmp, tb_sort, key, key2, val, order, (int)n, 0, key_bits(nk), s);
-  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp, tb_scan, cnt, off, (int)nk, s);
+  e = cub::DeviceRadixSort::SortPairs(tmp.p, tb_sort, key, key2, val, order, (int)n, 0, key_bits(nk), s);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(tmp.p, tb_scan, cnt, off, (int)nk, s);
   if (e == cudaSuccess) {
     const long long ns = (long long)g.T * (g.nsx * g.nsy + 1);
     rad_sec_start_kernel<<<(int)std::min<long long>((ns + 255) / 256, 148 * 16), 256, 0, s>>>(g, off, sec_start);
     e = cudaGetLastError();
   }
-  cudaFreeAsync(tmp, s);
-  cudaFreeAsync(cnt, s);
-  cudaFreeAsync(key, s);
   return e;
 }
 
 cudaError_t rad_count_lists(const RadialGeomDev& g, const int* order, const int* sec_start, const int2* win0,
                             int* off, long long* total, cudaStream_t s) {
   const long long nk = (long long)g.T * g.nsx * g.nsy;
-  int* cnt = nullptr;
-  void* tmp = nullptr;
   size_t tb = 0;
-  cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, off, (int)(nk + 1), s);
-  if (e == cudaSuccess) e = cudaMallocAsync(&cnt, (nk + 1) * sizeof(int), s);
-  if (e == cudaSuccess) e = cudaMallocAsync(&tmp, tb + 16, s);
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, tb, (int*)nullptr, off, (int)(nk + 1), s);
+  AsyncScratch counts(s), tmp(s);
+  if (e == cudaSuccess) e = counts.alloc((nk + 1) * sizeof(int));
+  if (e == cudaSuccess) e = tmp.alloc(tb + 16);
+  if (e == cudaSuccess) e = cudaMemsetAsync(counts.p, 0, (nk + 1) * sizeof(int), s);
   if (e != cudaSuccess) return e;
-  cudaMemsetAsync(cnt, 0, (nk + 1) * sizeof(int), s);
-  rad_lists_kernel<<<(int)((nk * 32 + 255) / 256), 256, 0, s>>>(g, order, sec_start, win0, cnt, nullptr, nullptr);
-  e = cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, off, (int)(nk + 1), s);
+  rad_lists_kernel<<<(int)((nk * 32 + 255) / 256), 256, 0, s>>>(g, order, sec_start, win0, counts.as<int>(), nullptr,
+                                                                   nullptr);
+  e = cub::DeviceScan::ExclusiveSum(tmp.p, tb, counts.as<int>(), off, (int)(nk + 1), s);
   int h = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h, off + nk, sizeof(int), cudaMemcpyDeviceToHost, s);
-  cudaFreeAsync(tmp, s);
-  cudaFreeAsync(cnt, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e == cudaSuccess) e = cudaGetLastError();
   *total = h;
@@ -604,20 +612,17 @@ cudaError_t rad_fill_lists(const RadialGeomDev& g, const int* order, const int* 
   const long long nk = (long long)g.T * g.nsx * g.nsy;
   rad_lists_kernel<<<(int)((nk * 32 + 255) / 256), 256, 0, s>>>(g, order, sec_start, win0, nullptr, off, list);
   // CTAs longest list first (a stable sort: equal lengths keep item order)
-  int *len = nullptr, *len2 = nullptr, *ids = nullptr;
-  void* tmp = nullptr;
   size_t tb = 0;
-  cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, len, len2, ids, blocks, (int)nk, 0, 32, s);
-  if (e == cudaSuccess) e = cudaMallocAsync(&len, 3 * nk * sizeof(int), s);
-  if (e == cudaSuccess) e = cudaMallocAsync(&tmp, tb + 16, s);
+  cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, (int*)nullptr, (int*)nullptr, (int*)nullptr,
+                                                            blocks, (int)nk, 0, 32, s);
+  AsyncScratch lens(s), tmp(s);
+  if (e == cudaSuccess) e = lens.alloc(3 * nk * sizeof(int));
+  if (e == cudaSuccess) e = tmp.alloc(tb + 16);
   if (e != cudaSuccess) return e;
-  len2 = len + nk;
-  ids = len + 2 * nk;
+  int *len = lens.as<int>(), *len2 = len + nk, *ids = len + 2 * nk;
   rad_list_len_kernel<<<(int)((nk + 255) / 256), 256, 0, s>>>(off, (int)nk, len);
   rad_iota_kernel<<<(int)((nk + 255) / 256), 256, 0, s>>>(ids, (int)nk);
-  e = cub::DeviceRadixSort::SortPairsDescending(tmp, tb, len, len2, ids, blocks, (int)nk, 0, 32, s);
-  cudaFreeAsync(tmp, s);
-  cudaFreeAsync(len, s);
+  e = cub::DeviceRadixSort::SortPairsDescending(tmp.p, tb, len, len2, ids, blocks, (int)nk, 0, 32, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e == cudaSuccess) e = cudaGetLastError();
   return e;
