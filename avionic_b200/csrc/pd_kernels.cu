@@ -420,10 +420,13 @@ AVX_D void pair_symdiv(const DivBranch& b, int k, int x, int y, int t, int W, in
   d[2] = make_float2(-a.x, -a.y);
 }
 
+// Two phases per pair, to keep fewer values live: branch 1 (div and symdiv
+// of y1, y2: components 0-3) is loaded, updated and stored before branch 2
+// (ICTGV2: y3, y4, components 4-7) is loaded; component 4 needs branch 1's
+// divergence, which is all that crosses the phases.
 template <int M, int NT>
 __global__ void __launch_bounds__(NT) primal_vec_kernel(PDArgs a) {
   if (a.st->stop) return;
-  constexpr int P = MethodDims<M>::P;
   const int HW2 = (a.W >> 1) * a.H;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= HW2) return;
@@ -433,52 +436,69 @@ __global__ void __launch_bounds__(NT) primal_vec_kernel(PDArgs a) {
   const long long sW = a.W, sWH = (long long)a.W * a.H;
   const long long i = x0 + sW * y + sWH * t;
   const float tau = (float)a.st->tau;
-  const V2 kh = ld4(a.khz, i);
-  const DivBranch b1 = load_branch(a.y, i, x0, y, t, a.W, a.H, a.T, sW, sWH, true);
-  DivBranch b2;
-  if (M == AVX_M_ICTGV2) b2 = load_branch(a.y + 9, i, x0, y, t, a.W, a.H, a.T, sW, sWH, true);
-  V2 xo[8];
+  float2 dv1[2];
+  {
+    const V2 kh = ld4(a.khz, i);
+    const DivBranch b1 = load_branch(a.y, i, x0, y, t, a.W, a.H, a.T, sW, sWH, true);
+    V2 xo[4];
 #pragma unroll
-  for (int c = 0; c < P; ++c) xo[c] = ld4(a.x[c], i);
-  float2 xn[2][8], xbv[2][8];
+    for (int c = 0; c < 4; ++c) xo[c] = ld4(a.x[c], i);
+    float2 xn[2][4], xbv[2][4];
 #pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const int x = x0 + k;
-    const float2 dv1 = pair_div3(b1, k, x, y, t, a.W, a.H, a.T, a.w1);
-    float2 sd1[3], y1[3], sd2[3], y3[3];
-    float2 dv3 = czero();
-    pair_symdiv(b1, k, x, y, t, a.W, a.H, a.T, a.w1, sd1);
-    y1[0] = pick(b1.y0.c, k);
-    y1[1] = pick(b1.y1.c, k);
-    y1[2] = pick(b1.y2.c, k);
-    if (M == AVX_M_ICTGV2) {
-      dv3 = pair_div3(b2, k, x, y, t, a.W, a.H, a.T, a.w2);
-      pair_symdiv(b2, k, x, y, t, a.W, a.H, a.T, a.w2, sd2);
-      y3[0] = pick(b2.y0.c, k);
-      y3[1] = pick(b2.y1.c, k);
-      y3[2] = pick(b2.y2.c, k);
-    }
-    float2 r[8];
-    r[0] = csub(dv1, pick(kh, k));
+    for (int k = 0; k < 2; ++k) {
+      const int x = x0 + k;
+      dv1[k] = pair_div3(b1, k, x, y, t, a.W, a.H, a.T, a.w1);
+      float2 sd1[3];
+      pair_symdiv(b1, k, x, y, t, a.W, a.H, a.T, a.w1, sd1);
+      const float2 y1[3] = {pick(b1.y0.c, k), pick(b1.y1.c, k), pick(b1.y2.c, k)};
+      float2 r[4];
+      r[0] = csub(dv1[k], pick(kh, k));
 #pragma unroll
-    for (int c = 0; c < 3; ++c) r[1 + c] = cadd(y1[c], sd1[c]);
-    if (M == AVX_M_ICTGV2) {
-      r[4] = csub(dv3, dv1);
+      for (int c = 0; c < 3; ++c) r[1 + c] = cadd(y1[c], sd1[c]);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) r[5 + c] = cadd(y3[c], sd2[c]);
+      for (int c = 0; c < 4; ++c) {
+        const float2 o = pick(xo[c], k);
+        const float2 n = make_float2(o.x + tau * r[c].x, o.y + tau * r[c].y);
+        xn[k][c] = n;
+        xbv[k][c] = make_float2(2.f * n.x - o.x, 2.f * n.y - o.y);
+      }
     }
 #pragma unroll
-    for (int c = 0; c < P; ++c) {
-      const float2 o = pick(xo[c], k);
-      const float2 n = make_float2(o.x + tau * r[c].x, o.y + tau * r[c].y);
-      xn[k][c] = n;
-      xbv[k][c] = make_float2(2.f * n.x - o.x, 2.f * n.y - o.y);
+    for (int c = 0; c < 4; ++c) {
+      st4(a.x[c], i, xn[0][c], xn[1][c]);
+      st4(a.xb[c], i, xbv[0][c], xbv[1][c]);
     }
   }
+  if (M == AVX_M_ICTGV2) {
+    const DivBranch b2 = load_branch(a.y + 9, i, x0, y, t, a.W, a.H, a.T, sW, sWH, true);
+    V2 xo[4];
 #pragma unroll
-  for (int c = 0; c < P; ++c) {
-    st4(a.x[c], i, xn[0][c], xn[1][c]);
-    st4(a.xb[c], i, xbv[0][c], xbv[1][c]);
+    for (int c = 0; c < 4; ++c) xo[c] = ld4(a.x[4 + c], i);
+    float2 xn[2][4], xbv[2][4];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int x = x0 + k;
+      const float2 dv3 = pair_div3(b2, k, x, y, t, a.W, a.H, a.T, a.w2);
+      float2 sd2[3];
+      pair_symdiv(b2, k, x, y, t, a.W, a.H, a.T, a.w2, sd2);
+      const float2 y3[3] = {pick(b2.y0.c, k), pick(b2.y1.c, k), pick(b2.y2.c, k)};
+      float2 r[4];
+      r[0] = csub(dv3, dv1[k]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) r[1 + c] = cadd(y3[c], sd2[c]);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const float2 o = pick(xo[c], k);
+        const float2 n = make_float2(o.x + tau * r[c].x, o.y + tau * r[c].y);
+        xn[k][c] = n;
+        xbv[k][c] = make_float2(2.f * n.x - o.x, 2.f * n.y - o.y);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      st4(a.x[4 + c], i, xn[0][c], xn[1][c]);
+      st4(a.xb[4 + c], i, xbv[0][c], xbv[1][c]);
+    }
   }
 }
 
