@@ -638,6 +638,8 @@ def main():
                     help="requests per rate (bounded sample of the 2000-request stream)")
     ap.add_argument("--serve-rates", default="20,200",
                     help="comma list of arrival rates in requests/s (the configuration sweeps 20-200)")
+    ap.add_argument("--serve-stop-gap", type=float, default=1e-4,
+                    help="normalised primal-dual gap (gap / pixels) at which a served request stops")
     args = ap.parse_args()
     parts = set(args.parts.split(","))
 
@@ -668,7 +670,8 @@ def main():
         extra["radial"] = run_radial(av, torch)
     if world == 1 and "serving" in parts:
         extra["serving"] = run_serving(av, torch, args.serve_workers, args.serve_requests,
-                                       [float(r) for r in args.serve_rates.split(",")])
+                                       [float(r) for r in args.serve_rates.split(",")],
+                                       rel_gap=args.serve_stop_gap)
     if "headline" not in parts:
         if dist is not None:
             dist.destroy_process_group()

@@ -153,6 +153,26 @@ def test_encoding_opnorm_radial_matches_oracle(av):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("method", ["TV", "TGV2", "ICTGV2"])
+def test_solver_opnorm_radial_matches_oracle(av, method):
+    """The whole primal-dual operator with the gridding operator as its
+    encoding part."""
+    W, H, C, T, nfe, spf, osf = 24, 20, 3, 3, 48, 9, 1.5
+    rng = np.random.default_rng(8)
+    traj, dens = rd.golden_angle_radial(nfe, spf, T)
+    traj, dens = traj.astype(np.float32), dens.astype(np.float32)
+    b1 = cplx(rng, (C, H, W)).astype(np.complex64)
+    x0 = cplx(rng, (T, H, W)).astype(np.complex64)
+    g = av.RadialOperator(W, H, C, T, av.to_device(traj), av.to_device(dens), spf, 3.0, 8.0, osf)
+    o = rd.RadialOperator(W, H, C, T, traj.astype(float), dens.astype(float), 3.0, 8.0, osf)
+    s = av.Solver(method, g)
+    est = s.opnorm(av.to_device(x0), av.to_device(b1), 10)
+    p = so.init_params(method)
+    ref = on.getopnorm(on.method_normal(method, o, b1.astype(complex), p), on.method_start(method, x0), 10)
+    assert _rel(est, ref) < REL_EST, (est, ref)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("dft", [0, 1])
 @pytest.mark.parametrize("method", METHODS)
 def test_solver_opnorm_matches_oracle(av, method, dft):
