@@ -172,6 +172,34 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+def tensor_roofline(mask, W, H, T, C, ydft_ms, coladj_ms):
+    """Tensor-pipe roofline of the two split-BF16x3 kernels: the bf16 MMA FLOPs
+    they issue per launch (six piece products; tiles as tc_dft.cu launches
+    them: M = 128 (coil, column) pairs x N = 2 x rows per frame (padded to 16)
+    x K = 2H for the y-transform, M = 128 image rows x N = 16 coils x 8
+    columns x 2 x K = N' for the column adjoint) over the stage means, against
+    the sustained bf16 figure of MEASURED_PEAKS.json (kernels timed inside a
+    long reconstruction)."""
+    rows = max(int(np.count_nonzero(np.any(mask[t] != 0, axis=1))) for t in range(T))
+    npad = max(16, (2 * rows + 15) // 16 * 16)
+    ceil = lambda a, b: -(-a // b)  # noqa: E731
+    mma = lambda m, n, k: 2 * m * n * k  # noqa: E731
+    ydft = T * ceil(C * W, 128) * ceil(2 * H, 32) * 2 * 6 * mma(128, npad, 16)
+    coladj = T * ceil(H, 128) * ceil(W, 8) * sum(
+        (npad // 16) * 6 * mma(128, ceil(2 * 8 * min(16, C - c0), 16) * 16, 16) for c0 in range(0, C, 16))
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, src = float(json.load(f)["bf16_tflops_sustained"]), "measured sustained"
+    except Exception:
+        peak, src = 1400.0, "fallback sustained"
+    out = {"peak_tflops": peak, "peak_source": src + " (MEASURED_PEAKS.json bf16_tflops_sustained)",
+           "n_per_mma_y_transform": npad}
+    for name, fl, ms in (("ydft_tc", ydft, ydft_ms), ("coladj_tc", coladj, coladj_ms)):
+        t = fl / (ms / 1000.0) / 1e12
+        out[name] = {"bf16_mma_gflop_per_launch": fl / 1e9, "achieved_tflops": t, "frac": t / peak}
+    return out
+
+
 def load_traffic():
     """DRAM bytes per launch by kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "kernel_traffic.txt")
@@ -798,6 +826,8 @@ def main():
                                 "after the timed region" % n_timed,
             "iteration_algorithmic_bytes": ab["iteration"],
             "iteration_frac": ab["iteration"] / (iter_ms / 1000.0) / 1e9 / peak}
+    if args.dft == "split":
+        roof["tensor_kernels"] = tensor_roofline(prob["mask"], W, H, T, C, kmean[1], kmean[3])
 
     # end-to-end through the host-buffer entry point (pinned host buffers)
     pk = torch.from_numpy(prob["kdata"]).pin_memory()
