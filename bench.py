@@ -109,6 +109,9 @@ def algorithmic_bytes(W, H, T, C, R):
         # the whole iteration: fields read and written once, z and d at the
         # sampled values, b1 once, the kept rows' mask: 8 [4PN + 2DN + 3CS] + 8 C W H + 4 R W
         "iteration": 8 * (4 * P * N + 2 * D * N + 3 * S) + 8 * C * W * H + 4 * R * W,
+        # the same with the reference's dense layout (z and d at all C N
+        # k-space points, the mask as 4 N bytes), for comparison only
+        "iteration_dense_layout": 8 * (4 * P * N + 2 * D * N + 3 * C * N) + 8 * C * W * H + 4 * N,
     }
 
 
@@ -825,7 +828,8 @@ def main():
             "kernel_ms_source": "CUDA events around each stage, %d iterations of one extra reconstruction "
                                 "after the timed region" % n_timed,
             "iteration_algorithmic_bytes": ab["iteration"],
-            "iteration_frac": ab["iteration"] / (iter_ms / 1000.0) / 1e9 / peak}
+            "iteration_frac": ab["iteration"] / (iter_ms / 1000.0) / 1e9 / peak,
+            "iteration_bytes_dense_layout": ab["iteration_dense_layout"]}
     if args.dft == "split":
         roof["tensor_kernels"] = tensor_roofline(prob["mask"], W, H, T, C, kmean[1], kmean[3])
 
