@@ -659,7 +659,7 @@ def main():
     ap.add_argument("--parts", default="headline,tv128,radial,batched,serving",
                     help="comma list: headline (the 192x192x30 cine ICTGV2 line), tv128, radial, batched, serving "
                          "(added to the line at N=1; batched at every N)")
-    ap.add_argument("--batch-workers", type=int, default=64,
+    ap.add_argument("--batch-workers", type=int, default=8,
                     help="requests the engine advances together in the batched form")
     ap.add_argument("--serve-workers", type=int, default=16,
                     help="requests the engine advances together in the served form (fewer finish in arrival order "
