@@ -661,7 +661,7 @@ def main():
                          "(added to the line at N=1; batched at every N)")
     ap.add_argument("--batch-workers", type=int, default=8,
                     help="requests the engine advances together in the batched form")
-    ap.add_argument("--serve-workers", type=int, default=16,
+    ap.add_argument("--serve-workers", type=int, default=4,
                     help="requests the engine advances together in the served form (fewer finish in arrival order "
                          "sooner; more overlap small requests)")
     ap.add_argument("--batch-size", type=int, default=64)
