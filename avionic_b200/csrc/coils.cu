@@ -241,54 +241,101 @@ __global__ void utgv_prep_kernel(const float2* b10, const float2* crec0, const i
   Ib[p] = make_float2(den.x / dd, -den.y / dd);
 }
 
-__global__ void utgv_dual_kernel(CoilPD a) {
+// One UTGV2Recon iteration (coil_construction.cpp:75-215) in one kernel: the
+// dual update (y1 += sigma (grad x1bar - x2bar), y2 += sigma E x2bar, each
+// projected onto its ball) at this pixel and at the neighbours the primal
+// update reads (the divergence: x - 1, y - W; the symmetrised divergence:
+// x + 1, y + W), recomputed from the old extragradients and duals, then the
+// primal update (x1 <- (x1 + tau (div y1 + Lw)) Ib, x2 += tau (y1 + div_sym
+// y2), extragradients 2 new - old).  The extragradients and the duals are
+// double-buffered; x1 and x2 are updated in place by their own thread.
+__global__ void utgv_fused_kernel(CoilPD a, UtgvBuffers b) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= a.W * a.H) return;
   const P2 p = p2_of(idx, a.W, a.H);
-  float2 g[2], e[3], y1[2], y2[3];
-  grad2(a.ext1, p, g);
+  // the dual update at pixel (qx, qy)
+  auto dual = [&](int qx, int qy, float2 (&y1)[2], float2 (&y2)[3]) {
+    P2 q;
+    q.x = qx;
+    q.y = qy;
+    q.W = a.W;
+    q.H = a.H;
+    q.i = (long long)qy * a.W + qx;
+    float2 g[2], e[3];
+    grad2(b.ext1_in, q, g);
 #pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const float2 d = csub(g[k], ldc(a.ext2[k], p.i));
-    const float2 v = a.y1[k][p.i];
-    y1[k] = make_float2(v.x + a.sigma * d.x, v.y + a.sigma * d.y);
+    for (int k = 0; k < 2; ++k) {
+      const float2 d = csub(g[k], ldc(b.ext2_in[k], q.i));
+      const float2 v = ldc(b.y1_in[k], q.i);
+      y1[k] = make_float2(v.x + a.sigma * d.x, v.y + a.sigma * d.y);
+    }
+    symgrad2(b.ext2_in[0], b.ext2_in[1], q, e);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const float2 v = ldc(b.y2_in[k], q.i);
+      y2[k] = make_float2(v.x + a.sigma * e[k].x, v.y + a.sigma * e[k].y);
+    }
+    const float n1 = sqrtf(cabs2(y1[0]) + cabs2(y1[1]));
+    const float n2 = sqrtf(cabs2(y2[0]) + cabs2(y2[1]) + 2.f * cabs2(y2[2]));
+    const float d1 = fmaxf(1.f, a.s1 * n1), d2 = fmaxf(1.f, a.s2 * n2);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) y1[k] = make_float2(y1[k].x / d1, y1[k].y / d1);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) y2[k] = make_float2(y2[k].x / d2, y2[k].y / d2);
+  };
+  float2 y1[2], y2[3];
+  dual(p.x, p.y, y1, y2);
+#pragma unroll
+  for (int k = 0; k < 2; ++k) b.y1_out[k][idx] = y1[k];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) b.y2_out[k][idx] = y2[k];
+  float2 n1[2], n2[3];
+  // div2 (d_fwd_t along x of y1_0, along y of y1_1), negated
+  float2 xm = czero(), ym = czero();
+  if (p.x > 0) {
+    dual(p.x - 1, p.y, n1, n2);
+    xm = n1[0];
   }
-  symgrad2(a.ext2[0], a.ext2[1], p, e);
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const float2 v = a.y2[k][p.i];
-    y2[k] = make_float2(v.x + a.sigma * e[k].x, v.y + a.sigma * e[k].y);
+  if (p.y > 0) {
+    dual(p.x, p.y - 1, n1, n2);
+    ym = n1[1];
   }
-  const float n1 = sqrtf(cabs2(y1[0]) + cabs2(y1[1]));
-  const float n2 = sqrtf(cabs2(y2[0]) + cabs2(y2[1]) + 2.f * cabs2(y2[2]));
-  const float d1 = fmaxf(1.f, a.s1 * n1), d2 = fmaxf(1.f, a.s2 * n2);
-#pragma unroll
-  for (int k = 0; k < 2; ++k) a.y1[k][p.i] = make_float2(y1[k].x / d1, y1[k].y / d1);
-#pragma unroll
-  for (int k = 0; k < 3; ++k) a.y2[k][p.i] = make_float2(y2[k].x / d2, y2[k].y / d2);
-}
-
-__global__ void utgv_primal_kernel(CoilPD a) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= a.W * a.H) return;
-  const P2 p = p2_of(idx, a.W, a.H);
-  const float2 dv = div2(a.y1[0], a.y1[1], p);
-  const float2 xo = a.x1[p.i];
-  float2 n1 = make_float2(xo.x + a.tau * dv.x, xo.y + a.tau * dv.y);
-  const float2 lw = a.Lw[p.i];
-  n1 = make_float2(n1.x + a.tau * lw.x, n1.y + a.tau * lw.y);
-  n1 = cmul(n1, a.Ib[p.i]);
-  a.x1n[p.i] = n1;
-  a.ext1n[p.i] = make_float2(2.f * n1.x - xo.x, 2.f * n1.y - xo.y);
+  const float2 ax = csub(xm, p.x < a.W - 1 ? y1[0] : czero());
+  const float2 ay = csub(ym, p.y < a.H - 1 ? y1[1] : czero());
+  const float2 s2 = cadd(ax, ay);
+  const float2 dv = make_float2(-s2.x, -s2.y);
+  const float2 xo = a.x1[idx];
+  float2 x1n = make_float2(xo.x + a.tau * dv.x, xo.y + a.tau * dv.y);
+  const float2 lw = a.Lw[idx];
+  x1n = make_float2(x1n.x + a.tau * lw.x, x1n.y + a.tau * lw.y);
+  x1n = cmul(x1n, a.Ib[idx]);
+  a.x1[idx] = x1n;
+  b.ext1_out[idx] = make_float2(2.f * x1n.x - xo.x, 2.f * x1n.y - xo.y);
+  // symdiv2 (d_bwd_t: w0 and w2 along x, w2 and w1 along y), negated
+  float2 w0p = czero(), w2x = czero(), w2y = czero(), w1p = czero();
+  if (p.x < a.W - 1) {
+    dual(p.x + 1, p.y, n1, n2);
+    w0p = n2[0];
+    w2x = n2[2];
+  }
+  if (p.y < a.H - 1) {
+    dual(p.x, p.y + 1, n1, n2);
+    w1p = n2[1];
+    w2y = n2[2];
+  }
+  const float2 z = czero();
   float2 sd[2];
-  symdiv2(a.y2[0], a.y2[1], a.y2[2], p, sd);
+  float2 t0 = cadd(p.x < a.W - 1 ? csub(y2[0], w0p) : z, p.y < a.H - 1 ? csub(y2[2], w2y) : z);
+  sd[0] = make_float2(-t0.x, -t0.y);
+  t0 = cadd(p.x < a.W - 1 ? csub(y2[2], w2x) : z, p.y < a.H - 1 ? csub(y2[1], w1p) : z);
+  sd[1] = make_float2(-t0.x, -t0.y);
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
-    const float2 r = cadd(ldc(a.y1[k], p.i), sd[k]);
-    const float2 x2 = a.x2[k][p.i];
-    const float2 n2 = make_float2(x2.x + a.tau * r.x, x2.y + a.tau * r.y);
-    a.x2[k][p.i] = n2;
-    a.ext2n[k][p.i] = make_float2(2.f * n2.x - x2.x, 2.f * n2.y - x2.y);
+    const float2 r = cadd(y1[k], sd[k]);
+    const float2 x2 = a.x2[k][idx];
+    const float2 m = make_float2(x2.x + a.tau * r.x, x2.y + a.tau * r.y);
+    a.x2[k][idx] = m;
+    b.ext2_out[k][idx] = make_float2(2.f * m.x - x2.x, 2.f * m.y - x2.y);
   }
 }
 
@@ -320,45 +367,14 @@ __global__ void b1r_prep_kernel(const float2* u0, const unsigned* umax, const fl
   }
 }
 
-__global__ void b1r_dual_kernel(CoilPD a, int coils) {
-  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int HW = a.W * a.H;
-  if (idx >= (long long)coils * HW) return;
-  const int c = (int)(idx / HW);
-  const P2 p = p2_of((int)(idx % HW), a.W, a.H);
-  const float2* e = a.ext1 + (long long)c * HW;
-  float2 g[2];
-  grad2(e, p, g);
-  const float sc = 1.f / (1.f + a.sigma / a.mu);
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const float2 v = a.y1[k][idx];
-    a.y1[k][idx] = cscale(make_float2(v.x + a.sigma * g[k].x, v.y + a.sigma * g[k].y), sc);
-  }
-}
-
-__global__ void b1r_primal_kernel(CoilPD a, int coils) {
-  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const int HW = a.W * a.H;
-  if (idx >= (long long)coils * HW) return;
-  const int c = (int)(idx / HW);
-  const P2 p = p2_of((int)(idx % HW), a.W, a.H);
-  const float2 dv = div2(a.y1[0] + (long long)c * HW, a.y1[1] + (long long)c * HW, p);
-  const float2 xo = a.x1[idx];
-  float2 n1 = make_float2(xo.x + a.tau * dv.x, xo.y + a.tau * dv.y);
-  const float2 lw = a.Lw[idx];
-  n1 = cmul(make_float2(n1.x + a.tau * lw.x, n1.y + a.tau * lw.y), a.Ib[idx]);
-  a.x1n[idx] = n1;
-  a.ext1n[idx] = make_float2(2.f * n1.x - xo.x, 2.f * n1.y - xo.y);
-}
-
-// One B1Recon iteration in one kernel: the dual update of b1r_dual_kernel at
-// this pixel and at the neighbours the divergence reads (x - 1 for the x
-// component, x - W for the y component), recomputed from the old extragradient
-// and duals, then the primal update of b1r_primal_kernel.  The extragradient
-// and the duals are double-buffered (neighbouring threads read the old values
-// while the owner writes the new ones); x is updated in place (read and written
-// by its own thread only).  Same arithmetic as the two-kernel form.
+// One B1Recon iteration (coil_construction.cpp:217-361) in one kernel: the
+// dual update (y = (y + sigma grad xbar) / (1 + sigma / mu)) at this pixel and
+// at the neighbours the divergence reads (x - 1 for the x component, x - W for
+// the y component), recomputed from the old extragradient and duals, then the
+// primal update (x <- (x + tau (div y + Lw)) Iu, extragradient 2 new - old).
+// The extragradient and the duals are double-buffered (neighbouring threads
+// read the old values while the owner writes the new ones); x is updated in
+// place (read and written by its own thread only).
 __global__ void b1r_fused_kernel(CoilPD a, int coils, B1Buffers b) {
   const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const int HW = a.W * a.H;
@@ -369,7 +385,7 @@ __global__ void b1r_fused_kernel(CoilPD a, int coils, B1Buffers b) {
   const long long cb = (long long)c * HW;
   const float2* e = b.ext_in + cb;
   const float sc = 1.f / (1.f + a.sigma / a.mu);
-  // dual component k at coil pixel q (the arithmetic of b1r_dual_kernel)
+  // dual component k at coil pixel q
   auto dual = [&](int k, int qx, int qy) {
     const long long q = (long long)qy * a.W + qx;
     const float2 g = k == 0 ? d_fwd(e, q, qx, a.W, 1) : d_fwd(e, q, qy, a.H, a.W);
@@ -467,9 +483,8 @@ void launch_utgv_prep(const float2* b10, const float2* crec0, const int* inds, i
                       float2* Lw, float2* Ib, cudaStream_t s) {
   utgv_prep_kernel<<<nb256(HW), 256, 0, s>>>(b10, crec0, inds, ninds, tau, HW, Lw, Ib);
 }
-void launch_utgv_iter(const CoilPD& a, cudaStream_t s) {
-  utgv_dual_kernel<<<nb256((long long)a.W * a.H), 256, 0, s>>>(a);
-  utgv_primal_kernel<<<nb256((long long)a.W * a.H), 256, 0, s>>>(a);
+void launch_utgv_fused(const CoilPD& a, const UtgvBuffers& b, cudaStream_t s) {
+  utgv_fused_kernel<<<nb256((long long)a.W * a.H), 256, 0, s>>>(a, b);
 }
 void launch_absmax(const float2* v, int n, unsigned* out, cudaStream_t s) {
   absmax_kernel<<<nb256(n), 256, 0, s>>>(v, n, out);
@@ -477,11 +492,6 @@ void launch_absmax(const float2* v, int n, unsigned* out, cudaStream_t s) {
 void launch_b1r_prep(const float2* u0, const unsigned* umax, const float2* crec, int coils, int HW, float tau,
                      float2* Lw, float2* Iu, cudaStream_t s) {
   b1r_prep_kernel<<<nb256(HW), 256, 0, s>>>(u0, umax, crec, coils, HW, tau, Lw, Iu);
-}
-void launch_b1r_iter(const CoilPD& a, int coils, cudaStream_t s) {
-  const long long n = (long long)coils * a.W * a.H;
-  b1r_dual_kernel<<<nb256(n), 256, 0, s>>>(a, coils);
-  b1r_primal_kernel<<<nb256(n), 256, 0, s>>>(a, coils);
 }
 void launch_b1r_fused(const CoilPD& a, int coils, const B1Buffers& b, cudaStream_t s) {
   const long long n = (long long)coils * a.W * a.H;

@@ -32,6 +32,18 @@ struct B1Buffers {
   float2* y1_out;
 };
 
+// double-buffered extragradients and duals of one fused UTGV2Recon iteration
+struct UtgvBuffers {
+  const float2* ext1_in;
+  float2* ext1_out;
+  const float2* ext2_in[2];
+  float2* ext2_out[2];
+  const float2* y1_in[2];
+  float2* y1_out[2];
+  const float2* y2_in[3];
+  float2* y2_out[3];
+};
+
 namespace avx {
 
 void launch_ta_sum(const float2* kdata, const float* mask, float2* out, int HW, int C, int T, cudaStream_t s);
@@ -41,11 +53,10 @@ void launch_h1_cg(const float2* u, const float2* crec, double mu, int W, int H, 
 void launch_h1_normalize(float2* b1, int HW, int C, cudaStream_t s);
 void launch_utgv_prep(const float2* b10, const float2* crec0, const int* inds, int ninds, float tau, int HW,
                       float2* Lw, float2* Ib, cudaStream_t s);
-void launch_utgv_iter(const CoilPD& a, cudaStream_t s);
+void launch_utgv_fused(const CoilPD& a, const UtgvBuffers& b, cudaStream_t s);
 void launch_absmax(const float2* v, int n, unsigned* out, cudaStream_t s);
 void launch_b1r_prep(const float2* u0, const unsigned* umax, const float2* crec, int coils, int HW, float tau,
                      float2* Lw, float2* Iu, cudaStream_t s);
-void launch_b1r_iter(const CoilPD& a, int coils, cudaStream_t s);
 void launch_b1r_fused(const CoilPD& a, int coils, const B1Buffers& b, cudaStream_t s);
 void launch_b1r_normalize(const float2* x, float2* out, int HW, int coils, cudaStream_t s);
 void launch_phase_apply(const float2* absb1, const float2* x1, float2* out, int HW, cudaStream_t s);

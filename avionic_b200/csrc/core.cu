@@ -1369,15 +1369,17 @@ avx_status coil_utgv2(int W, int H, const avx_coil_params& p, const float2* b10,
   const int N = W * H;
   CoilLoop local;
   CoilLoop& l = loop ? *loop : local;
+  // 11 N: ext1, x2 (2), ext2 (2), y1 (2), y2 (3), Lw; 8 N more: the second
+  // set of the double-buffered ext1, ext2, y1, y2
   if (l.N != N) {
-    AVX_CK(l.buf.alloc((size_t)11 * N));
+    AVX_CK(l.buf.alloc((size_t)19 * N));
     AVX_CK(l.xw.alloc(N));
     AVX_CK(l.Ib.alloc(N));
     l.N = N;
   }
   AVX_CK(l.dind.alloc(std::max<size_t>(inds.size(), 1)));
   AVX_CK(cudaMemcpyAsync(l.dind.p, inds.data(), inds.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-  AVX_CK(cudaMemsetAsync(l.buf.p, 0, (size_t)11 * N * sizeof(float2), s));
+  AVX_CK(cudaMemsetAsync(l.buf.p, 0, (size_t)19 * N * sizeof(float2), s));
   CoilPD a;
   memset(&a, 0, sizeof(a));
   a.W = W;
@@ -1403,7 +1405,29 @@ avx_status coil_utgv2(int W, int H, const avx_coil_params& p, const float2* b10,
   AVX_CK(cudaMemcpyAsync(l.xw.p, x1, N * sizeof(float2), cudaMemcpyDeviceToDevice, s));
   AVX_CK(cudaMemcpyAsync(a.ext1, x1, N * sizeof(float2), cudaMemcpyDeviceToDevice, s));
   avx::launch_utgv_prep(b10, crec0, l.dind.p, (int)inds.size(), p.uTau, N, Lw, l.Ib.p, s);
-  avx_status r = coil_iterate(l, p.uNrIt, s, [&] { avx::launch_utgv_iter(a, s); });
+  // one kernel per iteration; ext1, ext2, y1, y2 alternate between the two
+  // sets (the second at 11 N .. 19 N), x1 and x2 stay in place
+  UtgvBuffers ub[2];
+  float2* second = l.buf.p + (size_t)11 * N;
+  for (int q = 0; q < 2; ++q) {
+    const bool odd = q == 1;
+    auto pick = [&](float2* first, int j) { return odd ? second + (size_t)j * N : first; };
+    auto other = [&](float2* first, int j) { return odd ? first : second + (size_t)j * N; };
+    ub[q].ext1_in = pick(a.ext1, 0);
+    ub[q].ext1_out = other(a.ext1, 0);
+    for (int k = 0; k < 2; ++k) {
+      ub[q].ext2_in[k] = pick(a.ext2[k], 1 + k);
+      ub[q].ext2_out[k] = other(a.ext2[k], 1 + k);
+      ub[q].y1_in[k] = pick(a.y1[k], 3 + k);
+      ub[q].y1_out[k] = other(a.y1[k], 3 + k);
+    }
+    for (int k = 0; k < 3; ++k) {
+      ub[q].y2_in[k] = pick(a.y2[k], 5 + k);
+      ub[q].y2_out[k] = other(a.y2[k], 5 + k);
+    }
+  }
+  unsigned it = 0;
+  avx_status r = coil_iterate(l, p.uNrIt, s, [&] { avx::launch_utgv_fused(a, ub[it++ & 1u], s); });
   if (r != AVX_OK) return r;
   AVX_CK(cudaMemcpyAsync(x1, l.xw.p, N * sizeof(float2), cudaMemcpyDeviceToDevice, s));
   AVX_CK(cudaGetLastError());
