@@ -23,7 +23,7 @@ struct CartGeomDev {
   int rad[12];            // radices, first pass first
 };
 
-AVX_HD long long kbase(const CartGeomDev& g, int t, int c, int r0, int r1) {
+AVX_HD long long kbase(const CartGeomDev& g, int /* frame: implied by r0, r1 */, int c, int r0, int r1) {
   return ((long long)r0 * g.C + (long long)c * (r1 - r0)) * g.W;
 }
 
