@@ -6,10 +6,11 @@
 // k = 2 y + {re, im}, n = 2 kk + {re, im}; A is produced by the CTA's threads
 // from b1 and u and split into three bf16 pieces, B is the precomputed
 // coefficient table (tc_dft.cuh).  K runs in stages of 16 image rows through
-// two shared-memory buffers; one thread issues the 12 MMAs of a stage (2 K
-// steps x 6 piece products) and commits them to the buffer's mbarrier, which
-// the producers wait on before refilling that buffer.  The fp32 accumulator
-// lives in tensor memory and is read back with tcgen05.ld.
+// two A buffers in tensor memory and a three-slot coefficient ring in shared
+// memory; one thread issues the 12 MMAs of a stage (2 K steps x 6 piece
+// products) and commits them to the buffer's mbarrier, which the producers
+// wait on before refilling that buffer.  The fp32 accumulator lives in tensor
+// memory and is read back with tcgen05.ld.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -171,10 +172,11 @@ void tc_build_ytab(int W, int H, int T, int sx, int sy, const int* rows, const i
 // shared memory, and the MMAs read it from TMEM.  TMEM columns: the fp32
 // accumulator [0, np), then per A buffer b, K step ks and piece p the 8
 // columns (16 bf16 per lane) at np_al + ((2 b + ks) 3 + p) 8.  The
-// coefficient pieces (B) run through a three-stage shared-memory ring filled
-// one stage ahead by cp.async.  The MMAs of stage s are committed to
+// coefficient pieces (B) run through a three-slot shared-memory ring filled
+// one stage ahead by a bulk copy.  The MMAs of stage s are committed to
 // bar[s % 2]; stage s + 2 waits on that barrier (one lane per warp polls it)
-// before it overwrites the A buffer and the coefficient buffer of stage s + 3.
+// before it overwrites the A buffer, and thread 0 before it loads the
+// coefficients of stage s + 3 into the slot stage s used.
 AVX_D void tmem_st8(uint32_t taddr, const uint32_t (&v)[8]) {
   asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
                "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
@@ -191,7 +193,31 @@ AVX_D void mma_bf16_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t id
       : "memory");
 }
 
-template <bool U2>
+AVX_D void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+AVX_D void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// one contiguous global -> shared copy on the bulk-copy engine, completion
+// counted in bytes on bar (this GPU's memory, no multicast)
+AVX_D void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Stage hand-off on mbarriers, no CTA barrier in the loop: every thread
+// arrives on afull[b] once its tcgen05.st of A buffer b completed; thread 0
+// waits for the 256 arrivals and for the stage's coefficients, issues the
+// stage's MMAs and commits them to bar[b], while the other warps go on to the
+// next stage.  The coefficient stages come by one bulk copy each (thread 0,
+// completion on bfull[s % 3]), so the producing threads only load, multiply,
+// split and store A.  FULL: every tile row exists (C W a multiple of 128) and
+// every stage lies inside the image (H a multiple of 16), so the loads carry
+// no range tests.
+template <bool U2, bool FULL>
 __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   if (a.st && a.st->stop) return;
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -205,12 +231,14 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   const int pieceB = tc_piece_bytes(np);
   const int stageB = 3 * pieceB;
   unsigned char* sB = smem;  // 3 stages
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sB + 3 * stageB);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sB + 3 * stageB);  // [2] MMAs of A buffer b done
+  uint64_t* bfull = bar + 2;                                     // [3] coefficient stage landed
+  uint64_t* afull = bar + 5;                                     // [2] A buffer b written
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 7);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int q = warp & 3, kh = warp >> 2;
-  const int m = 32 * q + lane;              // tile row of this thread
-  const int mg = blockIdx.x * TC_M + m;     // global (c, x) row index
+  const int m = 32 * q + lane;
+  const int mg = blockIdx.x * TC_M + m;
   const int CW = C * W;
   const bool valid = mg < CW;
   const int c = valid ? mg / W : 0, x = valid ? mg - c * W : 0;
@@ -227,6 +255,9 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   if (tid == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
+    for (int i = 0; i < 3; ++i) mbar_init(&bfull[i], 1);
+    mbar_init(&afull[0], TC_THREADS);
+    mbar_init(&afull[1], TC_THREADS);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc_fence_before();
@@ -239,50 +270,57 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   const float2* __restrict__ pb = a.b1 + (long long)c * HW + x;
   const float2* __restrict__ pu = a.in + (long long)t * HW + x;
   const float2* __restrict__ pw = U2 ? a.in2 + (long long)t * HW + x : nullptr;
-  const uint4* __restrict__ btab = a.tc_ytab + (size_t)t * tc_nstage(H) * 3 * (pieceB / 16);
   const int nst = tc_nstage(H);
-  const int nbt = stageB / 16;
+  const unsigned char* __restrict__ btab =
+      reinterpret_cast<const unsigned char*>(a.tc_ytab) + (size_t)t * nst * stageB;
   bool ok = true;
 
-  auto issue_b = [&](int st) {
-    const uint4* src = btab + (size_t)st * nbt;
-    unsigned char* dst = sB + (st % 3) * stageB;
-    for (int e = tid; e < nbt; e += TC_THREADS)
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst + 16 * e)), "l"(src + e) : "memory");
-    asm volatile("cp.async.commit_group;" ::: "memory");
+  auto issue_b = [&](int st) {  // thread 0
+    uint64_t* fb = &bfull[st % 3];
+    mbar_expect_tx(fb, (uint32_t)stageB);
+    bulk_g2s(sB + (st % 3) * stageB, btab + (size_t)st * stageB, (uint32_t)stageB, fb);
   };
 
-  // register prefetch of one stage: b1 and u (, u2) at this thread's 8 image rows
   float2 rb[8], ru[8], rw[U2 ? 8 : 1];
   auto load_stage = [&](int st) {
+    const int y0 = st * (TC_KS / 2) + 8 * kh;
+    if (FULL) {
+      const long long o = (long long)y0 * W;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int y = st * (TC_KS / 2) + 8 * kh + i;
-      const bool in = valid && y < H;
-      const int off = y * W;
-      rb[i] = in ? __ldg(pb + off) : czero();
-      ru[i] = in ? pu[off] : czero();
-      if (U2) rw[i] = in ? pw[off] : czero();
+      for (int i = 0; i < 8; ++i) {
+        rb[i] = __ldg(pb + o + i * W);
+        ru[i] = pu[o + i * W];
+        if (U2) rw[i] = pw[o + i * W];
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int y = y0 + i;
+        const bool in = valid && y < H;
+        const int off = y * W;
+        rb[i] = in ? __ldg(pb + off) : czero();
+        ru[i] = in ? pu[off] : czero();
+        if (U2) rw[i] = in ? pw[off] : czero();
+      }
     }
   };
 
-  issue_b(0);
+  if (tid == 0) issue_b(0);
   load_stage(0);
   for (int s = 0; s < nst; ++s) {
     const int buf = s & 1;
-    unsigned char* sb = sB + (s % 3) * stageB;
     if (s >= 2) {
-      // MMAs of stage s - 2 done: its A buffer and the coefficient buffer of stage s + 1 are free
+      // MMAs of stage s - 2 done: A buffer buf is free (and, for thread 0, the
+      // coefficient slot of stage s + 1)
       bool w = true;
       if (lane == 0) w = mbar_wait(&bar[buf], (uint32_t)((s - 2) >> 1) & 1u);
       ok = __shfl_sync(0xffffffffu, w ? 1 : 0, 0) && ok;
     }
-    if (s + 1 < nst) issue_b(s + 1);
+    if (tid == 0 && s + 1 < nst) issue_b(s + 1);
     float2 v[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) v[i] = cmul(rb[i], U2 ? csub(ru[i], rw[i]) : ru[i]);
     if (s + 1 < nst) load_stage(s + 1);
-    // split: word i of piece p holds (re, im) of image row 8 kh + i, i.e. K = 16 kh + 2 i, + 1
     uint32_t pw3[3][8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
@@ -296,20 +334,16 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
 #pragma unroll
     for (int p = 0; p < 3; ++p) tmem_st8(tmem + lane_base + acol + (uint32_t)(p * 8), pw3[p]);
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-    // this stage's coefficients have landed (the next stage's may be in flight)
-    if (s + 1 < nst)
-      asm volatile("cp.async.wait_group 1;" ::: "memory");
-    else
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
-    __syncthreads();
+    mbar_arrive(&afull[buf]);
     if (tid == 0) {
+      bool w = mbar_wait(&afull[buf], (uint32_t)(s >> 1) & 1u);
+      w = mbar_wait(&bfull[s % 3], (uint32_t)(s / 3) & 1u) && w;
+      ok = ok && w;
       tc_fence_after();
-      const uint32_t b0 = smem_u32(sb);
+      const uint32_t b0 = smem_u32(sB + (s % 3) * stageB);
 #pragma unroll
       for (int ks = 0; ks < TC_KS / 16; ++ks) {
-        // piece products (pa, pb) with pa + pb <= 2
         const int pa[6] = {0, 0, 1, 0, 1, 2};
         const int pbk[6] = {0, 1, 0, 2, 1, 0};
 #pragma unroll
@@ -321,6 +355,7 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
       }
       mma_commit(&bar[buf]);
     }
+    __syncwarp();
   }
   const int last = nst - 1;
   ok = mbar_wait(&bar[last & 1], (uint32_t)(last >> 1) & 1u) && ok;
@@ -329,7 +364,6 @@ __global__ void __launch_bounds__(TC_THREADS, 3) ydft_tc_kernel(KArgs a) {
   if (!__all_sync(0xffffffffu, ok)) {
     if (a.st && lane == 0) atomicExch(&a.st->err, 2);
   } else {
-    // epilogue: this thread's row m, columns of its half (kh) of the accumulator
     const int ncol_half = np / 2;
     float2* out = a.qp + kbase(g, t, c, r0, r1) + x;
     for (int cc = kh * ncol_half; cc < (kh + 1) * ncol_half; cc += 8) {
@@ -620,10 +654,11 @@ void launch_b1_tile_transpose(const float2* b1, float2* b1t, int W, int H, int C
 }
 
 cudaError_t configure_tc_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(ydft_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       AVX_DYN_SMEM_MAX);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(ydft_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
+  const cudaFuncAttribute smem = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  cudaError_t e = cudaFuncSetAttribute(ydft_tc_kernel<false, false>, smem, AVX_DYN_SMEM_MAX);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(ydft_tc_kernel<true, false>, smem, AVX_DYN_SMEM_MAX);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(ydft_tc_kernel<false, true>, smem, AVX_DYN_SMEM_MAX);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(ydft_tc_kernel<true, true>, smem, AVX_DYN_SMEM_MAX);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(coladj_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, AVX_DYN_SMEM_MAX);
 }
@@ -636,10 +671,19 @@ void launch_coladj_tc(const KArgs& k, float2* img, cudaStream_t s) {
 void launch_ydft_tc(const KArgs& k, cudaStream_t s) {
   dim3 gr((k.g.C * k.g.W + TC_M - 1) / TC_M, k.g.T);
   const size_t sm = tc_ydft_smem_bytes(k.tc_np);
-  if (k.in2)
-    ydft_tc_kernel<true><<<gr, TC_THREADS, sm, s>>>(k);
-  else
-    ydft_tc_kernel<false><<<gr, TC_THREADS, sm, s>>>(k);
+  // every thread's tile row exists and every stage lies inside the image
+  const bool full = (k.g.C * k.g.W) % TC_M == 0 && k.g.H % (TC_KS / 2) == 0;
+  if (k.in2) {
+    if (full)
+      ydft_tc_kernel<true, true><<<gr, TC_THREADS, sm, s>>>(k);
+    else
+      ydft_tc_kernel<true, false><<<gr, TC_THREADS, sm, s>>>(k);
+  } else {
+    if (full)
+      ydft_tc_kernel<false, true><<<gr, TC_THREADS, sm, s>>>(k);
+    else
+      ydft_tc_kernel<false, false><<<gr, TC_THREADS, sm, s>>>(k);
+  }
 }
 
 }  // namespace avx
