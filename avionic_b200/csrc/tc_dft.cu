@@ -200,7 +200,7 @@ AVX_D void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 // one contiguous global -> shared copy on the bulk-copy engine, completion
-// counted in bytes on bar (this GPU's memory, no multicast)
+// counted in bytes on bar; source in this GPU's memory, destination this CTA
 AVX_D void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    smem_u32(dst)),
