@@ -41,6 +41,9 @@ CASES = [
     (32, 24, 4, 5, "weights", False),
     (20, 20, 3, 2, None, True),
     (96, 64, 2, 3, "lines", False),
+    # whole tensor-core tiles: C W a multiple of 128 and H of 16 (two stages, one stage)
+    (64, 32, 2, 3, "lines", False),
+    (32, 16, 4, 2, "random", True),
 ]
 
 
